@@ -1,0 +1,343 @@
+"""Benchmark of the B200 IISPH step: particle-updates/s on the 1,000,000-particle dam break.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one full IISPH time step (neighbor build, density, non-pressure, source/diagonal,
+relaxed-Jacobi loop to the density-error target, pressure acceleration, integration) of the
+100^3 dam break (dx = 0.01 m, 5 x 2 x 2 m tank, 2 wall layers, dt = 5e-4 s, omega = 0.5,
+2..100 iterations, average positive density error <= 0.1 %), seeded +-0.01 dx jitter. The
+working set (~0.3 GB) is larger than L2, so no flush is needed between steps.
+
+value: fluid particles x steps / device time (CUDA events on the backend stream, timed region
+bracketed by a barrier and device synchronisation, max over ranks). Multi-GPU: independent
+replicas (one scene per GPU, no inter-GPU traffic) -> weak scaling.
+e2e: the same metric through the C ABI with pinned host buffers: per step pull_state (H2D of
+the step's particle state) + step + push_state (D2H of positions, velocities, pressure,
+density).
+--impl reference: the CPU restatement of the reference step (oracle/, OpenMP over all host
+threads) on the same workload; the reference's own CPU backend cannot be built here.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-updates/s @1M (plain vs served batch, same B200); p50/p99 step ms"
+UNIT = "particle-updates/s"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(dist, v, device=None):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        import torch
+        if device is not None:
+            dist.all_reduce(torch.zeros(1, device=device))
+        else:
+            dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    p = os.path.join(ROOT, "profiles", "jacobi_dam_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def build_workload():
+    from turbospharticles_b200 import scene as S
+    st, dmin, dmax, p = S.dam_1m(seed=42)
+    return st, dmin, dmax, p
+
+
+def pinned_state(st):
+    """Copy of a UniversalSimState whose arrays live in pinned (page-locked) host memory."""
+    import torch
+    out = st.copy()
+    for k, v in st.arrays().items():
+        t = torch.empty(v.shape, dtype=getattr(torch, str(v.dtype)) if v.dtype != np.uint64 else torch.int64,
+                        pin_memory=True)
+        a = t.numpy().view(v.dtype)
+        a[...] = v
+        setattr(out, k, a)
+        out.__dict__.setdefault("_pins", []).append(t)
+    return out
+
+
+def run_b200(args):
+    import torch
+    from turbospharticles_b200 import abi
+    from turbospharticles_b200.backend import SimBackendB200
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = init_dist(ws, "nccl")
+    dev = torch.device("cuda", local)
+    st, dmin, dmax, p = build_workload()
+    be = SimBackendB200(p, device=local)
+    be.set_sim_domain_bounds(dmin, dmax)
+    be.pull(st, p)
+    be.run_stage(abi.STAGE_BOUNDARY_VOLUMES, p)
+    stream = torch.cuda.ExternalStream(be.stream_handle(), device=dev)
+    for _ in range(args.warmup):
+        be.step(p)
+    # ---- device-timed region
+    barrier(dist, dev)
+    torch.cuda.synchronize(dev)
+    l0 = be.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    step_ms, iters = [], []
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            be.step(p)
+            s = be.stats()
+            step_ms.append(s.lastStepMs)
+            iters.append(s.solverIters - 1)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(dist, dev)
+    elapsed_ms = max_over_ranks(dist, e0.elapsed_time(e1), dev)
+    launches = be.launch_count() - l0
+    nF = st.N_F
+    total_updates = nF * args.steps * ws
+    value = total_updates / (elapsed_ms / 1e3)
+    sweeps = int(np.sum(iters))
+    # ---- roofline of the dominant kernel: the relaxed-Jacobi sweep (KJacobi)
+    s = be.stats()
+    L = s.sellPackedBytes / nF + 6.0
+    bytes_per_particle = 32.0 + L + 4.0
+    jac_ms = be.time_stage(abi.STAGE_JACOBI_UPDATE, reps=20, params=p)
+    pacc_ms = be.time_stage(abi.STAGE_PRESSURE_ACC, reps=20, params=p)
+    achieved = bytes_per_particle * nF / (jac_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = profiled_traffic()
+    roof = {"kernel": "KJacobi (relaxed Jacobi sweep + FP64 residual reduction)", "bound": "hbm",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_source": peak_kind, "traffic": (traffic or {}).get("bytes_per_launch_scaled"),
+            "algorithmic_bytes_per_launch": int(bytes_per_particle * nF), "ms_per_launch": round(jac_ms, 4),
+            "pressure_acc_ms_per_launch": round(pacc_ms, 4),
+            "bytes_per_particle": round(bytes_per_particle, 2), "list_bytes_per_particle": round(L, 2)}
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = pinned_state(be.push())
+        out = pinned_state(be.push())
+        for n in ("xVelPredF", "yVelPredF", "zVelPredF", "xAccPressF", "yAccPressF", "zAccPressF",
+                  "sourceTermF", "diagElemF"):
+            setattr(out, n, np.zeros(0, np.float32))
+            setattr(host, n, np.zeros(0, np.float32))
+        h2d = host.N_F * (8 + 12 + 12 + 4 + 4) + host.N_B * (8 + 12 + 4 + 4)
+        d2h = host.N_F * (8 + 12 + 12 + 4 + 4) + host.N_B * (8 + 12 + 4 + 4)
+        barrier(dist, dev)
+        torch.cuda.synchronize(dev)
+        k_e2e = max(1, min(args.steps, 10))
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(k_e2e):
+            be.pull(host, p)
+            be.step(p)
+            be.push(out)
+            host, out = out, host
+        e3.record(stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms = max_over_ranks(dist, e2.elapsed_time(e3), dev)
+        e2e = {"value": round(nF * k_e2e * ws / (e2e_ms / 1e3), 1), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": k_e2e,
+               "path": "tsp_b200_pull_state + tsp_b200_step + tsp_b200_push_state, pinned host SoA"}
+    # ---- CPU baseline: the oracle port on this host, one step from the current GPU state
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cpu = cpu_baseline_from(be, p, dmin, dmax)
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    q = np.percentile(step_ms, [50, 99])
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 residual and rigid sums)",
+        "data": "synthetic (seeded dam-break scene restated from the reference builder)",
+        "config": {"workload": "iisph_dam_1M", "n_fluid": nF, "n_boundary": st.N_B, "dx_m": 0.01, "dt_s": 5e-4,
+                   "tank_m": [5, 2, 2], "omega": 0.5, "iters": "2..100, avg positive density error <= 0.001",
+                   "parallelism": f"replicas x{ws}", "l2": "working set > L2 (126 MB), no flush"},
+        "p50_step_ms": round(float(q[0]), 4), "p99_step_ms": round(float(q[1]), 4),
+        "jacobi_sweeps": sweeps, "jacobi_iters_per_s": round(sweeps * ws / (elapsed_ms / 1e3), 1),
+        "neighbor_ms_last": round(s.lastNeighborMs, 4), "jacobi_ms_last": round(s.lastJacobiMs, 4),
+        "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
+        "clocks": clk.summary(), "impl": "b200",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_from(be, p, dmin, dmax):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import OracleBackend
+    st = be.push()
+    threads = os.cpu_count() or 1
+    o = OracleBackend(p, threads=threads)
+    o.set_sim_domain_bounds(dmin, dmax)
+    o.pull(st, p)
+    t0 = time.perf_counter()
+    o.step(p)
+    dt = time.perf_counter() - t0
+    iters = o.stats().solverIters - 1
+    return {"value": round(st.N_F / dt, 1), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"1 IISPH step of the 1M dam from the GPU state after warm-up ({iters} Jacobi sweeps, "
+                      f"{dt:.2f} s, oracle/ CPU restatement, OpenMP)"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if ws > 1 and rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import OracleBackend
+    st, dmin, dmax, p = build_workload()
+    threads = os.cpu_count() or 1
+    o = OracleBackend(p, threads=threads)
+    o.set_sim_domain_bounds(dmin, dmax)
+    o.pull(st, p)
+    from turbospharticles_b200 import abi
+    o.run_stage(abi.STAGE_BOUNDARY_VOLUMES, p)
+    budget_s = 150.0
+    t_start = time.perf_counter()
+    for _ in range(args.warmup):
+        o.step(p)
+        if time.perf_counter() - t_start > budget_s / 2:
+            break
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.step(p)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget_s:
+            break
+    value = st.N_F * len(times) / sum(times)
+    q = np.percentile(np.array(times) * 1e3, [50, 99])
+    line = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": ws, "steps": len(times),
+            "warmup": args.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 residual sums)",
+            "data": "synthetic (seeded dam-break scene restated from the reference builder)",
+            "config": {"workload": "iisph_dam_1M", "n_fluid": st.N_F, "n_boundary": st.N_B,
+                       "parallelism": f"{threads} host threads"},
+            "p50_step_ms": round(float(q[0]), 2), "p99_step_ms": round(float(q[1]), 2), "impl": "reference",
+            "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{len(times)} IISPH steps of the 1M dam after {args.warmup} warm-up steps "
+                                       "(oracle/ CPU restatement; the reference CPU backend needs oneTBB/xsimd/"
+                                       "glm/Boost which are not installed)"},
+            "e2e": {"value": round(value, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

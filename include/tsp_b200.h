@@ -1,0 +1,248 @@
+/*
+ * tsp_b200.h -- C ABI of the B200-native IISPH solver backend.
+ *
+ * One handle = one solver backend instance (one scene) resident on one GPU. The entry points
+ * are the C-level replacement of the reference's solver-backend interface
+ * `Sim::I_SimBackend` (source/simulation/core/backend_sim.h:194-261); each declaration below
+ * cites the method it replaces. All functions return TSP_OK (0) or a negative status; no C++
+ * exception crosses this boundary. `tsp_b200_last_error()` gives the message of the last
+ * failure on that handle (thread-local message when the handle is NULL).
+ *
+ * Particle order: like the reference backends, the backend keeps its own (Morton-sorted)
+ * particle order. Pushed fluid/boundary arrays come out in that order together with their
+ * particle IDs; rigid particles keep their storage order (source/simulation/CPU/backend/
+ * neighbor_search.cpp:747-774).
+ *
+ * Threading: a handle must be used by one host thread at a time (the reference calls its
+ * backend from the single simulation-controller thread, source/simulation/core/simulation.h:150).
+ */
+#ifndef TSP_B200_H
+#define TSP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define TSP_OK                  0
+#define TSP_ERR_INVALID        -1  /* bad argument / state (std::invalid_argument analogue)   */
+#define TSP_ERR_CUDA           -2  /* CUDA runtime error (GPU::Check, gpu_utils.h:24-45)       */
+#define TSP_ERR_OVERFLOW       -3  /* count/size overflow (particle_types.h:393-497)            */
+#define TSP_ERR_FRAME          -4  /* cell frame exceeds 2^21 cells per axis (cell_frame.h:29)  */
+#define TSP_ERR_NEIGHBOR_LIST  -5  /* SELL32 fill overflow / delta range (common.cuh:24-26)     */
+#define TSP_ERR_RIGID          -6  /* degenerate rigid orientation (cpu_backend.cpp:46-58)      */
+#define TSP_ERR_UNSUPPORTED    -7  /* configuration outside what this backend implements        */
+#define TSP_ERR_NO_DEVICE      -8  /* no CUDA device / extension not usable                     */
+
+/* Sim::SolverTerminationCond (source/base/enum_hub.h:212-218) */
+#define TSP_TERM_FIXED_ITERS    0u
+#define TSP_TERM_REL_ERR_RAW    1u
+#define TSP_TERM_REL_ERR_POS    2u
+#define TSP_TERM_REL_ERR_ABS    3u
+
+/*
+ * Subset of Sim::SimParams (source/simulation/core/parameters_sim.h:25-175) that the step
+ * reads. Derived values follow the reference setters (parameters_sim.cpp:1478-1483):
+ * massF = restDensity * h^3, kernelRadius = 2h, kernelRadiusSqu = kernelRadius^2.
+ * `cubicSplineAlphaOverride` > 0 replaces alpha = 1/(4*pi*h^3) (solver_constants.h:20-36);
+ * the reference's own kernel unit tests pass alpha directly (tests/unit/sph_pressure.cpp).
+ */
+typedef struct tsp_params {
+    float timeStep;
+    float particleSizeF;
+    float particleSizeB;
+    float kernelRadius;
+    float kernelRadiusSqu;
+    float restDensity;
+    float massF;
+    float massB;
+    float viscosityF;
+    float viscosityB;
+    float gravity[3];
+    float pressGamma;
+    float jacobiOmega;
+    float jacobiWarmStart;
+    float densityDevTarget;
+    uint32_t fixedIters;
+    uint32_t minSolverIters;
+    uint32_t maxSolverIters;
+    uint32_t solverTerminationCond;   /* TSP_TERM_* */
+    float gridCellSizeRatio;
+    uint32_t boundaryLayers;
+    float cubicSplineAlphaOverride;   /* <= 0: derive from particleSizeF */
+    uint32_t reserved[4];
+} tsp_params;
+
+/*
+ * Host view of Sync::UniversalSimState (source/simulation/sync/state_sim.h): plain SoA
+ * pointers and counts. For pull, NULL optional fluid fields mean "zero" (density: rest density),
+ * NULL boundary/rigid coefficients take the reference defaults psi = massB,
+ * vol = massB / restDensity (state_sim.h:347-362, 461-475). For push, every non-NULL pointer
+ * receives N_* values.
+ */
+typedef struct tsp_state_view {
+    uint32_t N_F, N_B, N_R, N_RB;
+    uint64_t step;
+    double time;
+    /* fluid */
+    uint64_t* idF;
+    float *xPosF, *yPosF, *zPosF;
+    float *xVelF, *yVelF, *zVelF;
+    float *xVelPredF, *yVelPredF, *zVelPredF;
+    float *xAccPressF, *yAccPressF, *zAccPressF;
+    float *sourceTermF, *diagElemF, *pressureF, *densityF;
+    /* boundary */
+    uint64_t* idB;
+    float *xPosB, *yPosB, *zPosB;
+    float *volB, *psiB;
+    /* rigid particles (storage order is preserved) */
+    uint64_t* idR;
+    uint32_t* bodyIdR;
+    float *xPosRelR, *yPosRelR, *zPosRelR;
+    float *volR, *psiR;
+    float *xPosR, *yPosR, *zPosR;         /* push only: world positions */
+    /* rigid bodies */
+    uint64_t* idRB;
+    uint32_t* rigidParticleCountRB;
+    float *xCM, *yCM, *zCM;
+    float *xVelRB, *yVelRB, *zVelRB;
+    float *xOmegaRB, *yOmegaRB, *zOmegaRB;
+    float *xAngMomRB, *yAngMomRB, *zAngMomRB;
+    float *a00, *a01, *a02, *a10, *a11, *a12, *a20, *a21, *a22;
+    float *massRB, *massInvRB;
+    float *iBodyInv00, *iBodyInv01, *iBodyInv02;
+    float *iBodyInv10, *iBodyInv11, *iBodyInv12;
+    float *iBodyInv20, *iBodyInv21, *iBodyInv22;
+} tsp_state_view;
+
+/* Sim::PressureSolveErrorSums (backend_sim.h:62-67) + solver iteration state of the last step */
+typedef struct tsp_step_stats {
+    uint64_t step;
+    double time;
+    uint32_t solverIters;          /* N_solverIters_ (sph_solver.cpp:208,229)            */
+    uint32_t reserved0;
+    double errSumRaw, errSumPos, errSumAbs;  /* FP64 sums of the last evaluated sweep    */
+    float avgRelDensityErrRaw, avgRelDensityErrPos, avgRelDensityErrAbs;
+    uint32_t frameRebuilds;        /* cell-frame rebuilds since pull                    */
+    int32_t cellOrig[3];
+    uint32_t cellDims[3];
+    uint32_t keyBits;              /* CellIdKeyBits (neighbor_search.cpp:403-413)       */
+    uint32_t nCellsF, nCellsB, nCellsR;
+    uint64_t nNbrFF, nNbrFB, nNbrFR, nNbrRF, nNbrRB, nNbrRR;
+    uint64_t sellPackedBytes;      /* FF+FB+FR Delta16x2 + Abs32 storage                */
+    float lastStepMs;              /* device time of the last step (CUDA events)        */
+    float lastNeighborMs;          /* of which neighbor search                          */
+    float lastJacobiMs;            /* of which Jacobi loop                              */
+    uint32_t reserved1;
+} tsp_step_stats;
+
+typedef struct tsp_backend tsp_backend;
+
+/* ---- lifecycle: MakeSimBackend (backend_sim.cpp:18-38) -------------------------------- */
+/* creates a backend on CUDA device `device` (current device when < 0) */
+int tsp_b200_create(const tsp_params* params, int device, tsp_backend** out);
+/* ~I_SimBackend (backend_sim.h:198) */
+int tsp_b200_destroy(tsp_backend* h);
+/* I_SimBackend::Name (backend_sim.h:200) */
+const char* tsp_b200_name(const tsp_backend* h);
+/* last error message of h (or of this thread when h is NULL) */
+const char* tsp_b200_last_error(const tsp_backend* h);
+
+/* ---- state boundary ------------------------------------------------------------------ */
+/* I_SimBackend::SetSimDomainBounds (backend_sim.h:204); an empty extent leaves it unbounded */
+int tsp_b200_set_domain(tsp_backend* h, const float min_xyz[3], const float max_xyz[3]);
+/* I_SimBackend::PullFromUniversalSimState (backend_sim.h:207) */
+int tsp_b200_pull_state(tsp_backend* h, const tsp_state_view* src, const tsp_params* params);
+/* I_SimBackend::PushToUniversalSimState (backend_sim.h:211): copies into caller arrays */
+int tsp_b200_push_state(tsp_backend* h, tsp_state_view* dst);
+/* I_SimBackend::GetNumFluidParticles / Boundary / Rigid (backend_sim.h:258-260) */
+int tsp_b200_get_counts(const tsp_backend* h, uint32_t* nF, uint32_t* nB, uint32_t* nR, uint32_t* nRB);
+
+/* ---- hot path -------------------------------------------------------------------------- */
+/* I_SimBackend::ExecuteNeighborSearch (backend_sim.h:249; CPU cpu_backend.cpp:1593-1624):
+ * reorders ALL fluid fields, rebuilds cell tables and the SELL32 / CSR neighbor lists */
+int tsp_b200_neighbor_search(tsp_backend* h, const tsp_params* params);
+/* I_SimBackend::ExecuteFullSimStep (backend_sim.h:252; CPU Step_IISPH sph_solver.cpp:34-319):
+ * runs n_steps IISPH steps (the step counters advance by n_steps) */
+int tsp_b200_step(tsp_backend* h, const tsp_params* params, uint32_t n_steps);
+/* solver statistics of the last step (FillStatisticsRecord analogue, backend_sim.h:243) */
+int tsp_b200_get_stats(const tsp_backend* h, tsp_step_stats* out);
+
+/* ---- inspection (test access, like the reference's NeighborSearchTestAccess) ----------- */
+#define TSP_SPECIES_F 0u
+#define TSP_SPECIES_B 1u
+#define TSP_SPECIES_R 2u
+/* per-particle cell IDs in current (sorted) order; rigid: in storage order */
+int tsp_b200_read_cell_ids(const tsp_backend* h, uint32_t species, uint64_t* out, uint32_t n);
+/* last sort permutation: oldIdx of newIdx (fluid, boundary); rigid: sorted-slot -> rigid idx */
+int tsp_b200_read_permutation(const tsp_backend* h, uint32_t species, uint32_t* out, uint32_t n);
+/* compact cell table: returns count in *n_cells; fills when buffers are non-NULL (capacity cap) */
+int tsp_b200_read_cell_table(const tsp_backend* h, uint32_t species, uint64_t* unique_ids,
+                             uint32_t* cell_start /* n_cells + 1 */, uint32_t cap, uint32_t* n_cells);
+
+#define TSP_LIST_FF 0u
+#define TSP_LIST_FB 1u
+#define TSP_LIST_FR 2u
+#define TSP_LIST_RF 3u
+#define TSP_LIST_RB 4u
+#define TSP_LIST_RR 5u
+/* SELL32 meta of FF/FB/FR (GPU layout of the reference, neighbor_search_kernels.cu:86-250):
+ * counts[N_F], chunk pitch/format/base/base2/offset [n_chunks]; sizes of the packed buffers */
+int tsp_b200_read_sell32_meta(const tsp_backend* h, uint32_t list, uint16_t* counts,
+                              uint16_t* chunk_pitch, uint8_t* chunk_format, uint32_t* chunk_base,
+                              uint32_t* chunk_base2, uint64_t* chunk_offset, uint32_t n_chunks,
+                              uint64_t* n_delta16, uint64_t* n_abs32);
+int tsp_b200_read_sell32_words(const tsp_backend* h, uint32_t list, uint16_t* delta16, uint64_t n16,
+                               uint32_t* abs32, uint64_t n32);
+/* decoded neighbor rows as CSR: offsets[n_src+1], indices[total] (any list) */
+int tsp_b200_read_rows(const tsp_backend* h, uint32_t list, uint64_t* offsets, uint32_t n_src,
+                       uint32_t* indices, uint64_t cap, uint64_t* total);
+
+/* ---- stage access (test access to single solver stages on the resident state) --------- */
+#define TSP_STAGE_DENSITY            1u  /* Density_ChunkedSELL            sph_solver.cpp:734  */
+#define TSP_STAGE_NON_PRESSURE       2u  /* NonPressureAcceleration        sph_solver.cpp:892  */
+#define TSP_STAGE_SOURCE_DIAG_INIT   3u  /* SourceTermAndDiagonal...Init   sph_solver.cpp:1225 */
+#define TSP_STAGE_PRESSURE_ACC       4u  /* PressureAcceleration           sph_solver.cpp:1507 */
+#define TSP_STAGE_JACOBI_UPDATE      5u  /* PressureRelaxedJacobiSolver    sph_solver.cpp:1781 */
+#define TSP_STAGE_INTEGRATION        6u  /* Integration                    sph_solver.cpp:2051 */
+#define TSP_STAGE_BOUNDARY_VOLUMES   7u  /* ComputeParticleCoefficients    builder.cpp:174     */
+/* runs one stage; for TSP_STAGE_JACOBI_UPDATE `err_sums` (3 doubles) receives the FP64 sums */
+int tsp_b200_run_stage(tsp_backend* h, const tsp_params* params, uint32_t stage, double* err_sums);
+
+#define TSP_FIELD_POS        0u  /* 3 floats per fluid particle */
+#define TSP_FIELD_VEL        1u  /* 3 */
+#define TSP_FIELD_VEL_PRED   2u  /* 3 */
+#define TSP_FIELD_ACC_PRESS  3u  /* 3 */
+#define TSP_FIELD_SOURCE     4u  /* 1 */
+#define TSP_FIELD_DIAG       5u  /* 1 */
+#define TSP_FIELD_PRESSURE   6u  /* 1 */
+#define TSP_FIELD_DENSITY    7u  /* 1 */
+#define TSP_FIELD_VOL_B      8u  /* 1 per boundary particle */
+#define TSP_FIELD_PSI_B      9u  /* 1 per boundary particle */
+#define TSP_FIELD_VOL_R     10u  /* 1 per rigid particle */
+#define TSP_FIELD_PSI_R     11u  /* 1 per rigid particle */
+#define TSP_FIELD_FORCE_R   12u  /* 3 per rigid particle */
+#define TSP_FIELD_BODY_FT   13u  /* 6 doubles per body: force xyz, torque xyz (FP64) */
+/* reads (write_field: overwrites) one field as an interleaved (n x comps) float array;
+ * TSP_FIELD_BODY_FT uses double */
+int tsp_b200_read_field(const tsp_backend* h, uint32_t field, void* out, uint32_t n);
+int tsp_b200_write_field(tsp_backend* h, uint32_t field, const void* in, uint32_t n);
+
+/* ---- measurement (the reference's BenchmarksTracker role, eval/bench/benchmarks.h) ------ */
+/* launches `stage` `reps` times back to back on the backend's stream between two CUDA
+ * events and returns the average device time per launch (the stage must be runnable, see
+ * tsp_b200_run_stage; TSP_STAGE_JACOBI_UPDATE modifies the pressure field) */
+int tsp_b200_time_stage(tsp_backend* h, const tsp_params* params, uint32_t stage, uint32_t reps,
+                        float* ms_per_launch);
+/* the cudaStream_t all work of this backend runs on (for events / ordering by the caller) */
+int tsp_b200_get_stream(const tsp_backend* h, void** stream);
+/* number of CUDA kernels this backend launched since creation (graph nodes included) */
+int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TSP_B200_H */

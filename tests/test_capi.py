@@ -1,0 +1,59 @@
+"""The C-ABI library loads and exports every entry point include/tsp_b200.h declares (no GPU)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from turbospharticles_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_entry_points():
+    names = []
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if h.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", h)).read()
+            names += re.findall(r"^\s*(?:int|const char\*)\s+(tsp_b200_\w+)\s*\(", text, re.M)
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared_entry_points()
+    assert "tsp_b200_step" in names and "tsp_b200_pull_state" in names
+    assert len(names) == len(set(names))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(abi.LIB_PATH):
+        from turbospharticles_b200 import build
+        build.build()
+    return C.CDLL(abi.LIB_PATH)
+
+
+def test_library_exports_every_declared_symbol(lib):
+    for name in declared_entry_points():
+        assert hasattr(lib, name), name
+
+
+def test_python_signatures_cover_header():
+    assert set(declared_entry_points()) <= set(abi.EXPORTS)
+
+
+def test_struct_layouts_match_header():
+    # tsp_params: 25 four-byte fields + 4 reserved words
+    assert C.sizeof(abi.TspParams) == 4 * (3 + 2 + 3 + 2 + 3 + 4 + 4 + 1 + 1 + 1 + 4)
+    # tsp_state_view: 4 counts, step, time, then only pointers
+    n_ptr = len(abi.TspStateView._fields_) - 6
+    assert C.sizeof(abi.TspStateView) == 16 + 8 + 8 + 8 * n_ptr
+
+
+def test_null_handle_is_rejected_without_gpu(lib):
+    lib.tsp_b200_step.restype = C.c_int
+    lib.tsp_b200_step.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+    assert lib.tsp_b200_step(None, None, 1) == -1
+    lib.tsp_b200_last_error.restype = C.c_char_p
+    lib.tsp_b200_last_error.argtypes = [C.c_void_p]
+    assert b"NULL" in lib.tsp_b200_last_error(None)

@@ -1,0 +1,254 @@
+"""Parity of the B200 backend with the CPU oracle and the reference's known answers.
+
+Neighbor structures (Morton cell IDs, sort permutation, cell tables, neighbor rows, SELL32
+chunk metadata and packed words) must be bit-exact. FP32 solver fields compare with
+|gpu - oracle| <= rtol * (|oracle| + max|oracle|), rtol stated per test.
+"""
+import numpy as np
+import pytest
+
+import kat_cases as K
+from oracle import OracleBackend
+from turbospharticles_b200 import abi, scene as S
+from turbospharticles_b200.backend import SimBackendB200
+
+pytestmark = pytest.mark.gpu
+
+
+def pair(p, fp64=False):
+    return SimBackendB200(p), OracleBackend(p, fp64=fp64)
+
+
+def load(bes, st, p, dmin=None, dmax=None):
+    for be in bes:
+        if dmin is not None:
+            be.set_sim_domain_bounds(dmin, dmax)
+        be.pull(st, p)
+
+
+def assert_close(a, b, rtol, what=""):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = np.max(np.abs(b)) if b.size else 0.0
+    err = np.abs(a - b)
+    lim = rtol * (np.abs(b) + scale) + 1e-30
+    bad = err > lim
+    assert not bad.any(), f"{what}: {bad.sum()} of {bad.size} beyond rtol {rtol}; max err {err.max():.3e} scale {scale:.3e}"
+
+
+def assert_neighbor_structures_equal(g, o, n_f, n_b, n_r):
+    for sp, n in ((0, n_f), (1, n_b), (2, n_r)):
+        if n == 0:
+            continue
+        assert np.array_equal(g.cell_ids(sp), o.cell_ids(sp)), f"cell ids {sp}"
+        assert np.array_equal(g.permutation(sp), o.permutation(sp)), f"permutation {sp}"
+        gu, gs = g.cell_table(sp)
+        ou, os_ = o.cell_table(sp)
+        assert np.array_equal(gu, ou) and np.array_equal(gs, os_), f"cell table {sp}"
+    for lst in range(6):
+        go, gi = g.rows(lst)
+        oo, oi = o.rows(lst)
+        assert np.array_equal(go, oo), f"row offsets {lst}"
+        assert np.array_equal(gi, oi), f"rows {lst}"
+    for lst in range(3):
+        if n_f == 0:
+            continue
+        gm, om = g.sell32(lst), o.sell32(lst)
+        for k in ("counts", "pitch", "format", "base", "offset"):
+            assert np.array_equal(gm[k], om[k]), f"sell32 {lst} {k}"
+        # second base: only meaningful for Delta16x2 chunks
+        d = om["format"] == 0
+        assert np.array_equal(gm["base2"][d], om["base2"][d]), f"sell32 {lst} base2"
+        assert gm["w16"].size == om["w16"].size and gm["w32"].size == om["w32"].size
+        # packed words: every written slot (k < count of the lane) is identical
+        for key, fmt in (("w16", 0), ("w32", 1)):
+            mask = np.zeros(gm[key].size, bool)
+            cnt = om["counts"]
+            for c in np.nonzero(om["format"] == fmt)[0]:
+                lanes = np.arange(32)
+                i = c * 32 + lanes
+                valid_lane = i < n_f
+                cl = np.zeros(32, np.int64)
+                cl[valid_lane] = cnt[i[valid_lane]]
+                for k in range(int(om["pitch"][c])):
+                    m = cl > k
+                    mask[int(om["offset"][c]) + k * 32 + lanes[m]] = True
+            assert np.array_equal(gm[key][mask], om[key][mask]), f"sell32 {lst} {key}"
+
+
+# ------------------------------------------------------------------------------ known answers
+def test_gpu_pressure_pair_known_answers():
+    K.check_pressure_pair(K.pressure_pair_kats(SimBackendB200(K.pressure_params())))
+
+
+def test_gpu_density_and_viscosity_known_answers():
+    st, p, expected = K.density_kat_state()
+    g = SimBackendB200(p)
+    g.pull(st, p)
+    g.neighbor_search(p)
+    g.run_stage(abi.STAGE_DENSITY, p)
+    ids = g.push().idF
+    d = g.read_field(abi.FIELD_DENSITY)
+    assert abs(d[int(np.where(ids == 0)[0][0])] - expected) <= 1e-7 + 3e-6 * abs(expected)
+    for mass, rho in ((1.0, 2.0), (3.0, 5.0)):
+        st, p, expected = K.viscosity_kat_state(mass, rho)
+        g = SimBackendB200(p)
+        g.pull(st, p)
+        g.neighbor_search(p)
+        g.run_stage(abi.STAGE_NON_PRESSURE, p)
+        ids = g.push().idF
+        vp = g.read_field(abi.FIELD_VEL_PRED)
+        k = int(np.where(ids == 0)[0][0])
+        assert abs(vp[k, 0] - expected) <= 2e-6 + 8e-6 * abs(expected)
+
+
+def test_gpu_integration_exact():
+    for (x, vp, a), dt, (x1, v1) in K.integration_kats():
+        p = K.SimParams(timeStep=dt)
+        st = K.UniversalSimState(1, 0, 0, 0)
+        st.xPosF[:], st.yPosF[:], st.zPosF[:] = x
+        st.xVelPredF[:], st.yVelPredF[:], st.zVelPredF[:] = vp
+        st.xAccPressF[:], st.yAccPressF[:], st.zAccPressF[:] = a
+        g = SimBackendB200(p)
+        g.pull(st, p)
+        g.run_stage(abi.STAGE_INTEGRATION, p)
+        assert np.array_equal(g.read_field(abi.FIELD_POS)[0], np.array(x1, np.float32))
+        assert np.array_equal(g.read_field(abi.FIELD_VEL)[0], np.array(v1, np.float32))
+
+
+# ------------------------------------------------------------------------------ neighbor search
+NS_CASES = [(n, 1.0) for n in K.NS_SCENES] + [("small_cells", 0.5), ("small_cells", 0.25)] + \
+    [(f"simd_{n}", 1.0) for n in (15, 16, 17, 31, 32, 33, 63, 65)] + [(f"dense_{n}", 1.0) for n in (256, 272)]
+
+
+def ns_scene(name):
+    if name.startswith("simd_"):
+        return K.simd_width_scene(int(name.split("_")[1]))
+    if name.startswith("dense_"):
+        return K.dense_lattice_scene(int(name.split("_")[1]))
+    return K.NS_SCENES[name]
+
+
+@pytest.mark.parametrize("name,ratio", NS_CASES)
+def test_gpu_reference_neighbor_scenes(name, ratio):
+    """tests/unit/neighbor_search.cpp scenes: FP64 all-pairs sets, and bit-exact structures."""
+    scene = ns_scene(name)
+    p = K.ns_params(ratio)
+    st = K.make_particles(**scene)
+    g, o = pair(p)
+    load((g, o), st, p)
+    g.neighbor_search(p)
+    o.neighbor_search(p)
+    assert K.backend_neighbors(g, g.push()) == K.reference_neighbors(scene, 1.0)
+    assert_neighbor_structures_equal(g, o, st.N_F, st.N_B, st.N_R)
+
+
+def test_gpu_search_after_particles_move():
+    """neighbor_search.cpp:347-371: repeated imports of moved scenes reuse the backend."""
+    orig = dict(fluid=[(0, 0, 0), (0.5, 0, 0), (-4, 0.25, 0.25)], boundary=[(0.25, 0, 0), (-4.25, 0.25, 0.25)],
+                rigid=[(0.75, 0, 0), (-4, 0.5, 0.25)])
+    moved = dict(fluid=[(32, 0, 0), (-4.5, 0.25, 0.25), (-4, 0.25, 0.25)],
+                 boundary=[(32.25, 0, 0), (-4.25, 0.25, 0.25)], rigid=[(32.75, 0, 0), (-4, 0.5, 0.25)])
+    shifted = {k: [tuple(np.add(v, (64, -16, 8))) for v in vs] for k, vs in moved.items()}
+    p = K.ns_params()
+    g = SimBackendB200(p)
+    for sc in (orig, moved, shifted, orig):
+        g.pull(K.make_particles(**sc), p)
+        g.neighbor_search(p)
+        assert K.backend_neighbors(g, g.push()) == K.reference_neighbors(sc, 1.0)
+
+
+@pytest.mark.parametrize("dist,n", [("uniform", 50_000), ("clustered", 50_000), ("uniform", 1 << 20),
+                                    ("clustered", 1 << 20)])
+def test_gpu_neighbor_search_bit_exact(dist, n):
+    """Neighbor-search workload (uniform / 16 Gaussian blobs + 20 % background in the unit
+    cube, ~50 neighbors): every structure bit-exact with the oracle."""
+    st, dmin, dmax, p = S.neighbor_search_scene(n, dist, seed=7)
+    g, o = pair(p)
+    load((g, o), st, p, dmin, dmax)
+    g.neighbor_search(p)
+    o.neighbor_search(p)
+    assert_neighbor_structures_equal(g, o, st.N_F, 0, 0)
+
+
+def test_gpu_neighbor_search_4m_properties():
+    """4,194,304 points: size-independent properties (the oracle is not run at this size):
+    FF rows ascending, self included, the FF relation symmetric, SELL32 decode == rows."""
+    st, dmin, dmax, p = S.neighbor_search_scene(1 << 22, "clustered", seed=11)
+    g = SimBackendB200(p)
+    g.set_sim_domain_bounds(dmin, dmax)
+    g.pull(st, p)
+    g.neighbor_search(p)
+    off, idx = g.rows(abi.LIST_FF)
+    n = st.N_F
+    cnt = np.diff(off.astype(np.int64))
+    src = np.repeat(np.arange(n, dtype=np.int64), cnt)
+    assert np.all((np.diff(idx.astype(np.int64)) > 0) | (np.diff(src) != 0))
+    cid = g.cell_ids(abi.SPECIES_F)
+    inframe = cid != np.uint64(0xFFFFFFFFFFFFFFFF)
+    self_hit = np.zeros(n, bool)
+    self_hit[src[idx == src]] = True
+    assert np.array_equal(self_hit, inframe)
+    a = src * n + idx.astype(np.int64)
+    b = idx.astype(np.int64) * n + src
+    assert np.array_equal(np.sort(a), np.sort(b))
+    assert np.all(np.diff(cid[inframe].astype(np.float64)) >= 0)
+
+
+# ------------------------------------------------------------------------------ SPH stages
+def dam_pair(fp64=False, steps_before=0):
+    st, dmin, dmax, p = S.dam_32k()
+    g, o = pair(p, fp64)
+    load((g, o), st, p, dmin, dmax)
+    for be in (g, o):
+        be.run_stage(abi.STAGE_BOUNDARY_VOLUMES, p)
+    return g, o, p
+
+
+def test_gpu_boundary_volumes_match_oracle():
+    g, o, p = dam_pair()
+    # same summation order as the reference's z-y-x cell walk: FP32 bit-exact expected
+    gb, ob = g.push(), o.push()
+    og = np.argsort(gb.idB)
+    oo = np.argsort(ob.idB)
+    assert_close(gb.volB[og], ob.volB[oo], 1e-6, "volB")
+    assert_close(gb.psiB[og], ob.psiB[oo], 1e-6, "psiB")
+
+
+def test_gpu_stages_match_oracle_from_identical_state():
+    g, o, p = dam_pair()
+    for be in (g, o):
+        be.neighbor_search(p)
+    # identical start state for every stage (fields copied from the oracle)
+    for stage, fields, rtol in (
+            (abi.STAGE_DENSITY, [abi.FIELD_DENSITY], 1e-6),
+            (abi.STAGE_NON_PRESSURE, [abi.FIELD_VEL_PRED], 1e-6),
+            (abi.STAGE_SOURCE_DIAG_INIT, [abi.FIELD_SOURCE, abi.FIELD_DIAG, abi.FIELD_PRESSURE], 1e-5),
+            (abi.STAGE_PRESSURE_ACC, [abi.FIELD_ACC_PRESS], 1e-5),
+            (abi.STAGE_JACOBI_UPDATE, [abi.FIELD_PRESSURE], 1e-5)):
+        for f in (abi.FIELD_DENSITY, abi.FIELD_VEL_PRED, abi.FIELD_SOURCE, abi.FIELD_DIAG, abi.FIELD_PRESSURE,
+                  abi.FIELD_ACC_PRESS):
+            g.write_field(f, o.read_field(f))
+        eg = g.run_stage(stage, p)
+        eo = o.run_stage(stage, p)
+        for f in fields:
+            assert_close(g.read_field(f), o.read_field(f), rtol, f"stage {stage} field {f}")
+        if stage == abi.STAGE_JACOBI_UPDATE:
+            assert_close(eg, eo, 1e-9, "FP64 error sums")
+
+
+def test_gpu_steps_match_oracle():
+    """Full IISPH steps of the 32K dam from an identical start: same Jacobi iteration counts,
+    fields within tolerance (sum order is the only difference)."""
+    g, o, p = dam_pair()
+    for k in range(3):
+        g.step(p)
+        o.step(p)
+        sg, so = g.stats(), o.stats()
+        assert sg.solverIters == so.solverIters
+        assert abs(sg.avgRelDensityErrPos - so.avgRelDensityErrPos) <= 1e-6 + 1e-3 * abs(so.avgRelDensityErrPos)
+        gs, os_ = g.push(), o.push()
+        assert np.array_equal(gs.idF, os_.idF), "identical particle order (bit-exact permutation)"
+        for name, rtol in (("densityF", 1e-5), ("pressureF", 1e-3), ("xPosF", 1e-6), ("yVelF", 1e-3),
+                           ("xAccPressF", 1e-3), ("sourceTermF", 1e-3), ("diagElemF", 1e-4)):
+            assert_close(getattr(gs, name), getattr(os_, name), rtol, f"step {k} {name}")

@@ -1,0 +1,163 @@
+"""ctypes mirror of include/tsp_b200.h and loader of the in-tree CUDA library.
+
+The structs here are byte-for-byte the C structs of the C ABI; both the product backend
+(`libtsp_b200.so`) and the test oracle use them.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "_build", "libtsp_b200.so")
+
+TSP_OK = 0
+STATUS_NAMES = {
+    -1: "TSP_ERR_INVALID", -2: "TSP_ERR_CUDA", -3: "TSP_ERR_OVERFLOW", -4: "TSP_ERR_FRAME",
+    -5: "TSP_ERR_NEIGHBOR_LIST", -6: "TSP_ERR_RIGID", -7: "TSP_ERR_UNSUPPORTED",
+    -8: "TSP_ERR_NO_DEVICE",
+}
+
+TERM_FIXED_ITERS, TERM_REL_ERR_RAW, TERM_REL_ERR_POS, TERM_REL_ERR_ABS = 0, 1, 2, 3
+SPECIES_F, SPECIES_B, SPECIES_R = 0, 1, 2
+LIST_FF, LIST_FB, LIST_FR, LIST_RF, LIST_RB, LIST_RR = range(6)
+STAGE_DENSITY, STAGE_NON_PRESSURE, STAGE_SOURCE_DIAG_INIT = 1, 2, 3
+STAGE_PRESSURE_ACC, STAGE_JACOBI_UPDATE, STAGE_INTEGRATION, STAGE_BOUNDARY_VOLUMES = 4, 5, 6, 7
+(FIELD_POS, FIELD_VEL, FIELD_VEL_PRED, FIELD_ACC_PRESS, FIELD_SOURCE, FIELD_DIAG, FIELD_PRESSURE,
+ FIELD_DENSITY, FIELD_VOL_B, FIELD_PSI_B, FIELD_VOL_R, FIELD_PSI_R, FIELD_FORCE_R,
+ FIELD_BODY_FT) = range(14)
+FIELD_COMPONENTS = {FIELD_POS: 3, FIELD_VEL: 3, FIELD_VEL_PRED: 3, FIELD_ACC_PRESS: 3,
+                    FIELD_SOURCE: 1, FIELD_DIAG: 1, FIELD_PRESSURE: 1, FIELD_DENSITY: 1,
+                    FIELD_VOL_B: 1, FIELD_PSI_B: 1, FIELD_VOL_R: 1, FIELD_PSI_R: 1,
+                    FIELD_FORCE_R: 3, FIELD_BODY_FT: 6}
+
+_f = C.c_float
+_u32 = C.c_uint32
+_pf = C.POINTER(C.c_float)
+_pu64 = C.POINTER(C.c_uint64)
+_pu32 = C.POINTER(C.c_uint32)
+
+
+class TspParams(C.Structure):
+    _fields_ = [
+        ("timeStep", _f), ("particleSizeF", _f), ("particleSizeB", _f),
+        ("kernelRadius", _f), ("kernelRadiusSqu", _f), ("restDensity", _f),
+        ("massF", _f), ("massB", _f), ("viscosityF", _f), ("viscosityB", _f),
+        ("gravity", _f * 3), ("pressGamma", _f), ("jacobiOmega", _f),
+        ("jacobiWarmStart", _f), ("densityDevTarget", _f),
+        ("fixedIters", _u32), ("minSolverIters", _u32), ("maxSolverIters", _u32),
+        ("solverTerminationCond", _u32), ("gridCellSizeRatio", _f), ("boundaryLayers", _u32),
+        ("cubicSplineAlphaOverride", _f), ("reserved", _u32 * 4),
+    ]
+
+
+_STATE_FIELDS = [
+    ("N_F", _u32), ("N_B", _u32), ("N_R", _u32), ("N_RB", _u32),
+    ("step", C.c_uint64), ("time", C.c_double),
+    ("idF", _pu64),
+    ("xPosF", _pf), ("yPosF", _pf), ("zPosF", _pf),
+    ("xVelF", _pf), ("yVelF", _pf), ("zVelF", _pf),
+    ("xVelPredF", _pf), ("yVelPredF", _pf), ("zVelPredF", _pf),
+    ("xAccPressF", _pf), ("yAccPressF", _pf), ("zAccPressF", _pf),
+    ("sourceTermF", _pf), ("diagElemF", _pf), ("pressureF", _pf), ("densityF", _pf),
+    ("idB", _pu64), ("xPosB", _pf), ("yPosB", _pf), ("zPosB", _pf), ("volB", _pf), ("psiB", _pf),
+    ("idR", _pu64), ("bodyIdR", _pu32),
+    ("xPosRelR", _pf), ("yPosRelR", _pf), ("zPosRelR", _pf), ("volR", _pf), ("psiR", _pf),
+    ("xPosR", _pf), ("yPosR", _pf), ("zPosR", _pf),
+    ("idRB", _pu64), ("rigidParticleCountRB", _pu32),
+    ("xCM", _pf), ("yCM", _pf), ("zCM", _pf),
+    ("xVelRB", _pf), ("yVelRB", _pf), ("zVelRB", _pf),
+    ("xOmegaRB", _pf), ("yOmegaRB", _pf), ("zOmegaRB", _pf),
+    ("xAngMomRB", _pf), ("yAngMomRB", _pf), ("zAngMomRB", _pf),
+    ("a00", _pf), ("a01", _pf), ("a02", _pf), ("a10", _pf), ("a11", _pf), ("a12", _pf),
+    ("a20", _pf), ("a21", _pf), ("a22", _pf),
+    ("massRB", _pf), ("massInvRB", _pf),
+    ("iBodyInv00", _pf), ("iBodyInv01", _pf), ("iBodyInv02", _pf),
+    ("iBodyInv10", _pf), ("iBodyInv11", _pf), ("iBodyInv12", _pf),
+    ("iBodyInv20", _pf), ("iBodyInv21", _pf), ("iBodyInv22", _pf),
+]
+
+
+class TspStateView(C.Structure):
+    _fields_ = _STATE_FIELDS
+
+
+STATE_ARRAY_FIELDS = [name for name, _ in _STATE_FIELDS[6:]]
+
+
+class TspStepStats(C.Structure):
+    _fields_ = [
+        ("step", C.c_uint64), ("time", C.c_double), ("solverIters", _u32), ("reserved0", _u32),
+        ("errSumRaw", C.c_double), ("errSumPos", C.c_double), ("errSumAbs", C.c_double),
+        ("avgRelDensityErrRaw", _f), ("avgRelDensityErrPos", _f), ("avgRelDensityErrAbs", _f),
+        ("frameRebuilds", _u32), ("cellOrig", C.c_int32 * 3), ("cellDims", _u32 * 3),
+        ("keyBits", _u32), ("nCellsF", _u32), ("nCellsB", _u32), ("nCellsR", _u32),
+        ("nNbrFF", C.c_uint64), ("nNbrFB", C.c_uint64), ("nNbrFR", C.c_uint64),
+        ("nNbrRF", C.c_uint64), ("nNbrRB", C.c_uint64), ("nNbrRR", C.c_uint64),
+        ("sellPackedBytes", C.c_uint64), ("lastStepMs", _f), ("lastNeighborMs", _f),
+        ("lastJacobiMs", _f), ("reserved1", _u32),
+    ]
+
+
+# every exported entry point of include/tsp_b200.h, with its ctypes signature
+_VP = C.c_void_p
+EXPORTS = {
+    "tsp_b200_create": (C.c_int, [C.POINTER(TspParams), C.c_int, C.POINTER(_VP)]),
+    "tsp_b200_destroy": (C.c_int, [_VP]),
+    "tsp_b200_name": (C.c_char_p, [_VP]),
+    "tsp_b200_last_error": (C.c_char_p, [_VP]),
+    "tsp_b200_set_domain": (C.c_int, [_VP, _pf, _pf]),
+    "tsp_b200_pull_state": (C.c_int, [_VP, C.POINTER(TspStateView), C.POINTER(TspParams)]),
+    "tsp_b200_push_state": (C.c_int, [_VP, C.POINTER(TspStateView)]),
+    "tsp_b200_get_counts": (C.c_int, [_VP, _pu32, _pu32, _pu32, _pu32]),
+    "tsp_b200_neighbor_search": (C.c_int, [_VP, C.POINTER(TspParams)]),
+    "tsp_b200_step": (C.c_int, [_VP, C.POINTER(TspParams), _u32]),
+    "tsp_b200_get_stats": (C.c_int, [_VP, C.POINTER(TspStepStats)]),
+    "tsp_b200_read_cell_ids": (C.c_int, [_VP, _u32, _pu64, _u32]),
+    "tsp_b200_read_permutation": (C.c_int, [_VP, _u32, _pu32, _u32]),
+    "tsp_b200_read_cell_table": (C.c_int, [_VP, _u32, _pu64, _pu32, _u32, _pu32]),
+    "tsp_b200_read_sell32_meta": (C.c_int, [_VP, _u32, C.POINTER(C.c_uint16),
+                                            C.POINTER(C.c_uint16), C.POINTER(C.c_uint8), _pu32,
+                                            _pu32, _pu64, _u32, _pu64, _pu64]),
+    "tsp_b200_read_sell32_words": (C.c_int, [_VP, _u32, C.POINTER(C.c_uint16), C.c_uint64,
+                                             _pu32, C.c_uint64]),
+    "tsp_b200_read_rows": (C.c_int, [_VP, _u32, _pu64, _u32, _pu32, C.c_uint64, _pu64]),
+    "tsp_b200_run_stage": (C.c_int, [_VP, C.POINTER(TspParams), _u32, C.POINTER(C.c_double)]),
+    "tsp_b200_read_field": (C.c_int, [_VP, _u32, _VP, _u32]),
+    "tsp_b200_write_field": (C.c_int, [_VP, _u32, _VP, _u32]),
+    "tsp_b200_time_stage": (C.c_int, [_VP, C.POINTER(TspParams), _u32, _u32, _pf]),
+    "tsp_b200_get_launch_count": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
+    "tsp_b200_get_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
+}
+
+
+class TspError(RuntimeError):
+    """Raised when a C-ABI call returns a negative status (the reference throws
+    std::runtime_error from GPU::Check, source/simulation/GPU/gpu_utils.h:24-45)."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_LIB = None
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Loads the in-tree CUDA library; raises if it is missing (there is no CPU fallback)."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(
+            f"{p} is missing: build it with `python -m turbospharticles_b200.build` "
+            "(the B200 backend has no CPU fallback)")
+    lib = C.CDLL(p)
+    for name, (res, args) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _LIB = lib
+    return lib

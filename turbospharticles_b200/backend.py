@@ -1,0 +1,199 @@
+"""SimBackendB200: Python mirror of the reference's `Sim::I_SimBackend`
+(source/simulation/core/backend_sim.h:194-261) over the C ABI of include/tsp_b200.h.
+
+Method names follow the reference interface (Name, SetSimDomainBounds,
+PullFromUniversalSimState, PushToUniversalSimState, ExecuteNeighborSearch,
+ExecuteFullSimStep, GetNum*Particles); failures raise `TspError` like the reference's
+std::runtime_error. The snake_case methods below them are the test-access surface
+(neighbor structures, single solver stages, field reads).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .abi import TspError, TspStepStats, FIELD_COMPONENTS, FIELD_BODY_FT
+from .params import SimParams
+from .state import UniversalSimState
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class SimBackendB200:
+    def __init__(self, params: SimParams | None = None, device: int = -1):
+        self.L = abi.load_library()
+        self.params = params or SimParams()
+        self._cp = self.params.to_c()
+        h = C.c_void_p()
+        rc = self.L.tsp_b200_create(C.byref(self._cp), device, C.byref(h))
+        if rc != 0:
+            raise TspError(rc, self.L.tsp_b200_last_error(None).decode())
+        self.h = h
+        self.counts = (0, 0, 0, 0)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.tsp_b200_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise TspError(rc, self.L.tsp_b200_last_error(self.h).decode())
+
+    def _cparams(self, params):
+        if params is not None:
+            self.params = params
+        self._cp = self.params.to_c()
+        return C.byref(self._cp)
+
+    # ------------------------------------------------------------ I_SimBackend surface
+    def Name(self) -> str:
+        return self.L.tsp_b200_name(self.h).decode()
+
+    def SetSimDomainBounds(self, mn, mx):
+        a = np.ascontiguousarray(mn, np.float32)
+        b = np.ascontiguousarray(mx, np.float32)
+        self._chk(self.L.tsp_b200_set_domain(self.h, a.ctypes.data_as(C.POINTER(C.c_float)),
+                                             b.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def PullFromUniversalSimState(self, state: UniversalSimState, params: SimParams | None = None):
+        v = state.view()
+        self._chk(self.L.tsp_b200_pull_state(self.h, C.byref(v), self._cparams(params)))
+        self.counts = (state.N_F, state.N_B, state.N_R, state.N_RB)
+
+    def PushToUniversalSimState(self, dst: UniversalSimState | None = None) -> UniversalSimState:
+        st = dst if dst is not None else UniversalSimState(*self.counts)
+        v = st.view()
+        self._chk(self.L.tsp_b200_push_state(self.h, C.byref(v)))
+        st.step, st.time = int(v.step), float(v.time)
+        return st
+
+    def ExecuteNeighborSearch(self, params: SimParams | None = None, bench: bool = False):
+        self._chk(self.L.tsp_b200_neighbor_search(self.h, self._cparams(params)))
+
+    def ExecuteFullSimStep(self, params: SimParams | None = None, N_steps: int = 1):
+        self._chk(self.L.tsp_b200_step(self.h, self._cparams(params), N_steps))
+
+    def GetNumFluidParticles(self):
+        return self.counts[0]
+
+    def GetNumBoundaryParticles(self):
+        return self.counts[1]
+
+    def GetNumRigidParticles(self):
+        return self.counts[2]
+
+    # ------------------------------------------------------------ shared test surface
+    set_sim_domain_bounds = SetSimDomainBounds
+    pull = PullFromUniversalSimState
+    push = PushToUniversalSimState
+    neighbor_search = ExecuteNeighborSearch
+
+    def step(self, params=None, n_steps=1):
+        self.ExecuteFullSimStep(params, n_steps)
+
+    def stats(self) -> TspStepStats:
+        s = TspStepStats()
+        self._chk(self.L.tsp_b200_get_stats(self.h, C.byref(s)))
+        return s
+
+    def cell_ids(self, species):
+        n = self.counts[species]
+        out = np.zeros(n, np.uint64)
+        self._chk(self.L.tsp_b200_read_cell_ids(self.h, species, out.ctypes.data_as(C.POINTER(C.c_uint64)), n))
+        return out
+
+    def permutation(self, species):
+        n = self.counts[species]
+        out = np.zeros(n, np.uint32)
+        self._chk(self.L.tsp_b200_read_permutation(self.h, species, out.ctypes.data_as(C.POINTER(C.c_uint32)), n))
+        return out
+
+    def cell_table(self, species):
+        nc = C.c_uint32()
+        self._chk(self.L.tsp_b200_read_cell_table(self.h, species, None, None, 0, C.byref(nc)))
+        u = np.zeros(nc.value, np.uint64)
+        s = np.zeros(nc.value + 1, np.uint32)
+        self._chk(self.L.tsp_b200_read_cell_table(self.h, species, u.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                  s.ctypes.data_as(C.POINTER(C.c_uint32)), nc.value, C.byref(nc)))
+        return u, (s if nc.value else np.zeros(0, np.uint32))
+
+    def rows(self, lst):
+        nsrc = self.counts[0] if lst < 3 else self.counts[2]
+        tot = C.c_uint64()
+        self._chk(self.L.tsp_b200_read_rows(self.h, lst, None, nsrc, None, 0, C.byref(tot)))
+        off = np.zeros(nsrc + 1, np.uint64)
+        idx = np.zeros(max(tot.value, 1), np.uint32)
+        self._chk(self.L.tsp_b200_read_rows(self.h, lst, off.ctypes.data_as(C.POINTER(C.c_uint64)), nsrc,
+                                            idx.ctypes.data_as(C.POINTER(C.c_uint32)), tot.value, C.byref(tot)))
+        return off, idx[:tot.value]
+
+    def sell32(self, lst):
+        nF = self.counts[0]
+        nch = (nF + 31) // 32
+        n16, n32 = C.c_uint64(), C.c_uint64()
+        m = dict(counts=np.zeros(nF, np.uint16), pitch=np.zeros(nch, np.uint16),
+                 format=np.zeros(nch, np.uint8), base=np.zeros(nch, np.uint32),
+                 base2=np.zeros(nch, np.uint32), offset=np.zeros(nch, np.uint64))
+        P = lambda a, t: a.ctypes.data_as(C.POINTER(t))  # noqa: E731
+        self._chk(self.L.tsp_b200_read_sell32_meta(
+            self.h, lst, P(m["counts"], C.c_uint16), P(m["pitch"], C.c_uint16), P(m["format"], C.c_uint8),
+            P(m["base"], C.c_uint32), P(m["base2"], C.c_uint32), P(m["offset"], C.c_uint64), nch,
+            C.byref(n16), C.byref(n32)))
+        m["w16"] = np.zeros(n16.value, np.uint16)
+        m["w32"] = np.zeros(n32.value, np.uint32)
+        self._chk(self.L.tsp_b200_read_sell32_words(self.h, lst, P(m["w16"], C.c_uint16), n16.value,
+                                                    P(m["w32"], C.c_uint32), n32.value))
+        return m
+
+    def run_stage(self, stage, params=None):
+        err = (C.c_double * 3)()
+        self._chk(self.L.tsp_b200_run_stage(self.h, self._cparams(params), stage, err))
+        return tuple(err)
+
+    def _field_n(self, field):
+        if field == FIELD_BODY_FT:
+            return self.counts[3]
+        if field in (abi.FIELD_VOL_B, abi.FIELD_PSI_B):
+            return self.counts[1]
+        if field in (abi.FIELD_VOL_R, abi.FIELD_PSI_R, abi.FIELD_FORCE_R):
+            return self.counts[2]
+        return self.counts[0]
+
+    def read_field(self, field):
+        n = self._field_n(field)
+        k = FIELD_COMPONENTS[field]
+        out = np.zeros(n * k, np.float64 if field == FIELD_BODY_FT else np.float32)
+        self._chk(self.L.tsp_b200_read_field(self.h, field, _p(out), n))
+        return out.reshape(n, k) if k > 1 else out
+
+    def time_stage(self, stage, reps=20, params=None) -> float:
+        """Average device milliseconds per launch of one solver stage (CUDA events)."""
+        ms = C.c_float()
+        self._chk(self.L.tsp_b200_time_stage(self.h, self._cparams(params), stage, reps, C.byref(ms)))
+        return ms.value
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        self._chk(self.L.tsp_b200_get_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def stream_handle(self) -> int:
+        s = C.c_void_p()
+        self._chk(self.L.tsp_b200_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def write_field(self, field, values):
+        v = np.ascontiguousarray(values, np.float32).ravel()
+        k = FIELD_COMPONENTS[field]
+        self._chk(self.L.tsp_b200_write_field(self.h, field, _p(v), v.size // k))

@@ -1,0 +1,1351 @@
+// backend.cu -- host driver of the B200 IISPH backend and its C ABI (include/tsp_b200.h).
+//
+// One `Backend` = one scene resident on one GPU, one CUDA stream. A solver step mirrors
+// SimBackend_CPU::Step_IISPH (source/simulation/CPU/backend/sph_solver.cpp:34-319):
+//   neighbor build (frame rule, sort, reorder, cell tables, SELL32 count -> offsets -> fill)
+//   density -> [rigid clear+gravity] -> non-pressure -> [rigid viscous forces, reduce,
+//   predict] -> source/diagonal/init -> relaxed Jacobi loop -> pressure acceleration ->
+//   [rigid pressure forces, reduce] -> integration -> [rigid predict, integrate, update]
+// Host round trips per step: the frame probe (6 floats + a flag, needed by the reference's
+// hysteresis frame rule) and the neighbor-list totals (buffer capacities). The Jacobi loop
+// runs entirely on the device inside a CUDA graph whose conditional WHILE node is driven
+// by the last block of each sweep (no host synchronisation per iteration, unlike
+// gpu_backend.cpp:1432-1496 of the reference GPU backend).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "../../include/tsp_b200.h"
+#include "kernels.h"
+#include "primitives.cuh"
+
+namespace tsp {
+
+void LaunchRigidVolumesSorted(const Consts& c, const float4* rel, const uint32_t* byBodyOff, const uint32_t* sortedIdx,
+                              const int4* sortedCell, const uint32_t* bodyOfSorted, uint32_t nR, int reach,
+                              float defaultVol, float defaultPsi, float restDensity, float* volOut, float* psiOut,
+                              cudaStream_t s);
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+#define CK(x)                                                                                       \
+    do {                                                                                            \
+        cudaError_t e_ = (x);                                                                       \
+        if (e_ != cudaSuccess) throw Error(TSP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    void ensure(size_t n) {  // contents are not preserved
+        if (n <= cap && (p || n == 0)) return;
+        release();
+        if (n == 0) return;
+        CK(cudaMalloc(&p, n * sizeof(T)));
+        cap = n;
+    }
+    void grow(size_t n, double slack) {
+        if (n <= cap && p) return;
+        ensure((size_t)((double)n * slack) + 16);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    ~DBuf() { release(); }
+};
+template <typename T> static void Swap(DBuf<T>& a, DBuf<T>& b) { std::swap(a.p, b.p); std::swap(a.cap, b.cap); }
+
+// ------------------------------------------------------------------------------ small kernels
+__global__ void KPack4(const float* a, const float* b, const float* c, const float* d, float dDefault, float4* out,
+                       uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = make_float4(a ? a[i] : 0.f, b ? b[i] : 0.f, c ? c[i] : 0.f, d ? d[i] : dDefault);
+}
+__global__ void KUnpack4(const float4* in, float* a, float* b, float* c, float* d, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 v = in[i];
+    if (a) a[i] = v.x;
+    if (b) b[i] = v.y;
+    if (c) c[i] = v.z;
+    if (d) d[i] = v.w;
+}
+__global__ void KPack2(const float* a, const float* b, float2* out, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = make_float2(a ? a[i] : 0.f, b ? b[i] : 0.f);
+}
+__global__ void KUnpack2(const float2* in, float* a, float* b, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (a) a[i] = in[i].x;
+    if (b) b[i] = in[i].y;
+}
+__global__ void KSetW(float4* v, const float* w, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i].w = w[i];
+}
+__global__ void KIota(uint32_t* v, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+static inline unsigned G(uint32_t n) { return (n + 255) / 256; }
+
+// ------------------------------------------------------------------------------ helpers
+static inline int HostFloorToInt(float v) {
+    const int i = (int)v;
+    return (v < (float)i) ? (i - 1) : i;
+}
+static inline uint32_t HostKeyBits(uint32_t nx, uint32_t ny, uint32_t nz) {  // neighbor_search.cpp:403-413
+    const uint32_t m = std::max(nx, std::max(ny, nz));
+    uint32_t axisBits = 1;
+    if (m >= 2) axisBits = 32u - (uint32_t)__builtin_clz(m - 1u);
+    return 3u * axisBits + 1u;
+}
+
+// solver constants exactly as the reference derives them (see common.cuh: Consts)
+static Consts MakeConsts(const tsp_params& p) {
+    Consts c{};
+    const double h = (double)p.particleSizeF, hInv = 1.0 / h, rho = (double)p.restDensity;
+    c.sizeInv = (float)hInv;
+    c.sizeSqu = (float)(h * h);
+    c.alpha = p.cubicSplineAlphaOverride > 0.0f ? p.cubicSplineAlphaOverride
+                                                : (float)(hInv * hInv * hInv / (4.0 * 3.14159265358979323846));
+    c.restDensitySquInv = (float)(1.0 / (rho * rho));
+    c.radSqu = p.kernelRadiusSqu;
+    c.dt = p.timeStep;
+    c.dt2 = p.timeStep * p.timeStep;
+    c.kSize = 1.0f / c.sizeInv;
+    c.kTwoSize = 2.0f / c.sizeInv;
+    c.kInnerSlope = 9.0f * c.alpha * c.sizeInv * c.sizeInv * c.sizeInv;
+    c.kInnerOffset = -12.0f * c.alpha * c.sizeInv * c.sizeInv;
+    c.kOuterScale = -3.0f * c.alpha * c.sizeInv * c.sizeInv * c.sizeInv;
+    c.massF = p.massF;
+    c.restDensity = p.restDensity;
+    c.densInvSqu = 1.0f / (p.restDensity * p.restDensity);
+    c.hEps = 0.01f * c.sizeSqu;
+    c.visFacF = 10.0f * p.viscosityF;
+    c.visFacB = 10.0f * p.viscosityB;
+    c.gx = p.gravity[0]; c.gy = p.gravity[1]; c.gz = p.gravity[2];
+    c.cTermFacF = -p.massF * c.restDensitySquInv;
+    c.cTermFacB = -2.0f * p.pressGamma * c.restDensitySquInv;
+    c.diagBFac = -p.massF * c.restDensitySquInv;
+    c.omega = p.jacobiOmega;
+    c.warmStart = p.jacobiWarmStart;
+    c.warm = p.jacobiWarmStart > 0.0f ? 1 : 0;
+    c.accCoeffB = 2.0f * p.pressGamma * c.densInvSqu;
+    return c;
+}
+
+struct HostMirror {
+    ProbeResult probe;
+    U64x2 sellTot[3];
+    uint64_t csrTot[3];
+    uint64_t nCells[3];
+    SolverState st;
+    uint32_t err;
+};
+
+static uint64_t HashBytes(uint64_t h, const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < n; i++) { h ^= b[i]; h *= 1099511628211ull; }
+    return h;
+}
+
+class Backend {
+public:
+    int device = 0;
+    cudaStream_t s = nullptr, capStream = nullptr;
+    tsp_params prm{};
+    DomainBox dom{};
+    uint32_t nF = 0, nB = 0, nR = 0, nRB = 0;
+    uint64_t stepCount = 0;
+    double simTime = 0.0;
+    // fluid
+    DBuf<float4> posP, posP2, velRho, velRho2, velPred, velPred2, acc, acc2;
+    DBuf<float2> srcDiag, srcDiag2;
+    DBuf<uint64_t> idF, idF2;
+    // boundary
+    DBuf<float4> posB, posB2;
+    DBuf<float> volB, volB2, psiTmpB;
+    DBuf<uint64_t> idB, idB2;
+    // rigid particles and bodies
+    DBuf<uint32_t> bodyR, byBodyOff, byBodyIdx;
+    DBuf<float4> relR, posR, velR, velPredR, forceR;
+    DBuf<uint64_t> idR;
+    DBuf<float> volR, psiR;
+    std::vector<float> hRelX, hRelY, hRelZ;
+    std::vector<uint32_t> hBodyR, hByBodyOff, hByBodyIdx;
+    std::vector<uint64_t> hIdRB;
+    std::vector<uint32_t> hCntRB;
+    DBuf<double> bodyState, bodyFT;
+    // neighbor search
+    Frame fr{};
+    bool frameValid = false;
+    float cellSize = 0.0f;
+    uint32_t reach = 1;
+    uint32_t frameRebuilds = 0;
+    bool bSortedForFrame = false;
+    bool bAabbValid = false;
+    float bMin[3] = {0, 0, 0}, bMax[3] = {0, 0, 0};
+    DBuf<uint64_t> keysA, keysB;
+    DBuf<uint32_t> valsA, valsB, tileHist, digitTotals;
+    DBuf<uint32_t> permF, permB, permR;
+    DBuf<uint64_t> cidF, cidB, cidR, cidRs;
+    DBuf<uint64_t> uniqF, uniqB, uniqR;
+    DBuf<uint32_t> startF, startB, startR;
+    DBuf<uint64_t> nCellsDev;
+    DBuf<uint32_t> gridF, gridB, gridR;
+    uint64_t gridCells = 0;
+    DBuf<uint64_t> scanScratch;
+    DBuf<U64x2> scanScratch2;
+    struct Sell {
+        DBuf<uint16_t> counts, pitch;
+        DBuf<uint8_t> format;
+        DBuf<uint32_t> base, base2;
+        DBuf<uint64_t> offset;
+        DBuf<uint16_t> l16;
+        DBuf<uint32_t> l32;
+        uint64_t n16 = 0, n32 = 0;
+    } sell[3];
+    DBuf<U64x2> sellTot;
+    DBuf<uint16_t> cntR[3];
+    DBuf<uint64_t> offR[3];
+    DBuf<uint32_t> listR[3];
+    DBuf<uint64_t> csrTot;
+    uint64_t csrN[3] = {0, 0, 0};
+    bool listsValid = false;
+    // solver
+    DBuf<SolverState> st;
+    DBuf<double> partials;
+    DBuf<uint32_t> err;
+    DBuf<ProbeResult> probe;
+    HostMirror* hm = nullptr;
+    struct JacobiGraph {
+        uint64_t key = 0;
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ex = nullptr;
+    };
+    std::vector<JacobiGraph> graphs;
+    size_t graphNext = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    float lastStepMs = 0.f, lastNbrMs = 0.f, lastJacMs = 0.f;
+    std::string lastErr;
+    uint64_t launches = 0;  // kernels launched by this backend (graph nodes included)
+    static uint32_t SortLaunches(uint32_t n, uint32_t bits) { return n < 2 ? 2u : 2u + 3u * ((bits + 7u) / 8u); }
+
+    explicit Backend(int dev) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw Error(TSP_ERR_NO_DEVICE, "no CUDA device");
+        if (dev < 0) CK(cudaGetDevice(&dev));
+        device = dev;
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&capStream, cudaStreamNonBlocking));
+        CK(cudaMallocHost(&hm, sizeof(HostMirror)));
+        std::memset(hm, 0, sizeof(HostMirror));
+        st.ensure(1);
+        err.ensure(1);
+        probe.ensure(1);
+        nCellsDev.ensure(3);
+        sellTot.ensure(3);
+        csrTot.ensure(3);
+        CK(cudaMemset(st.p, 0, sizeof(SolverState)));
+        CK(cudaMemset(err.p, 0, sizeof(uint32_t)));
+        for (auto& e : ev) CK(cudaEventCreate(&e));
+    }
+    ~Backend() {
+        cudaSetDevice(device);
+        if (s) cudaStreamSynchronize(s);
+        for (auto& g : graphs) {
+            if (g.ex) cudaGraphExecDestroy(g.ex);
+            if (g.g) cudaGraphDestroy(g.g);
+        }
+        for (auto& e : ev) if (e) cudaEventDestroy(e);
+        if (hm) cudaFreeHost(hm);
+        if (capStream) cudaStreamDestroy(capStream);
+        if (s) cudaStreamDestroy(s);
+    }
+    void Sync() { CK(cudaStreamSynchronize(s)); }
+    void CheckErrors() {
+        CK(cudaMemcpyAsync(&hm->err, err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        Sync();
+        CK(cudaGetLastError());
+        const uint32_t e = hm->err;
+        if (!e) return;
+        CK(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), s));
+        if (e & (ERR_RIGID_ORIENT | ERR_RIGID_ATTACH))
+            throw Error(TSP_ERR_RIGID, (e & ERR_RIGID_ORIENT) ? "Degenerate rigid body orientation."
+                                                               : "Invalid rigid particle attachment.");
+        if (e & ERR_QUERY_CAP) throw Error(TSP_ERR_UNSUPPORTED, "query stencil exceeds the shared-memory staging");
+        if (e & ERR_COUNT_U16) throw Error(TSP_ERR_OVERFLOW, "a neighbor count exceeds uint16 storage");
+        throw Error(TSP_ERR_NEIGHBOR_LIST, "SELL32 neighbor-list fill overflow / delta range error");
+    }
+
+    // -------------------------------------------------------------------------- state boundary
+    void SetDomain(const float* mn, const float* mx) {
+        for (int a = 0; a < 3; a++) { dom.mn[a] = mn[a]; dom.mx[a] = mx[a]; }
+        dom.bounded = !(mx[0] <= mn[0] || mx[1] <= mn[1] || mx[2] <= mn[2]);
+    }
+
+    template <typename T>
+    void Upload(DBuf<T>& d, const T* h, size_t n) {
+        d.ensure(std::max<size_t>(n, 1));
+        if (n && h) CK(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void Pack4(DBuf<float4>& out, uint32_t n, const float* a, const float* b, const float* c, const float* d,
+               float dDefault, DBuf<float>& tmp) {
+        out.ensure(std::max<uint32_t>(n, 1));
+        if (n == 0) return;
+        tmp.ensure(4ull * n);
+        const float* src[4] = {a, b, c, d};
+        float* dst[4] = {nullptr, nullptr, nullptr, nullptr};
+        for (int k = 0; k < 4; k++)
+            if (src[k]) {
+                dst[k] = tmp.p + (uint64_t)k * n;
+                CK(cudaMemcpyAsync(dst[k], src[k], n * sizeof(float), cudaMemcpyHostToDevice, s));
+            }
+        KPack4<<<G(n), 256, 0, s>>>(dst[0], dst[1], dst[2], dst[3], dDefault, out.p, n);
+    }
+    void Unpack4(const float4* in, uint32_t n, float* a, float* b, float* c, float* d, DBuf<float>& tmp) {
+        if (n == 0) return;
+        tmp.ensure(4ull * n);
+        float* host[4] = {a, b, c, d};
+        float* dev[4];
+        for (int k = 0; k < 4; k++) dev[k] = host[k] ? tmp.p + (uint64_t)k * n : nullptr;
+        KUnpack4<<<G(n), 256, 0, s>>>(in, dev[0], dev[1], dev[2], dev[3], n);
+        for (int k = 0; k < 4; k++)
+            if (host[k]) CK(cudaMemcpyAsync(host[k], dev[k], n * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+
+    void Pull(const tsp_state_view& v, const tsp_params& p) {
+        CK(cudaSetDevice(device));
+        prm = p;
+        nF = v.N_F; nB = v.N_B; nR = v.N_R; nRB = v.N_RB;
+        if (nF > 0x7fffffffu || nB > 0x7fffffffu || nR > 0x7fffffffu)
+            throw Error(TSP_ERR_OVERFLOW, "particle count exceeds the local particle limit");
+        stepCount = v.step; simTime = v.time;
+        DBuf<float> tmp;
+        // fluid
+        std::vector<uint64_t> ids;
+        if (!v.idF) { ids.resize(nF); for (uint32_t i = 0; i < nF; i++) ids[i] = i; }
+        Upload(idF, v.idF ? v.idF : ids.data(), nF);
+        Pack4(posP, nF, v.xPosF, v.yPosF, v.zPosF, v.pressureF, 0.0f, tmp);
+        Pack4(velRho, nF, v.xVelF, v.yVelF, v.zVelF, v.densityF, p.restDensity, tmp);
+        Pack4(velPred, nF, v.xVelPredF, v.yVelPredF, v.zVelPredF, nullptr, 0.0f, tmp);
+        Pack4(acc, nF, v.xAccPressF, v.yAccPressF, v.zAccPressF, nullptr, 0.0f, tmp);
+        srcDiag.ensure(std::max<uint32_t>(nF, 1));
+        if (nF) {
+            tmp.ensure(2ull * nF);
+            const float* sh[2] = {v.sourceTermF, v.diagElemF};
+            float* sd[2] = {nullptr, nullptr};
+            for (int k = 0; k < 2; k++)
+                if (sh[k]) {
+                    sd[k] = tmp.p + (uint64_t)k * nF;
+                    CK(cudaMemcpyAsync(sd[k], sh[k], nF * sizeof(float), cudaMemcpyHostToDevice, s));
+                }
+            KPack2<<<G(nF), 256, 0, s>>>(sd[0], sd[1], srcDiag.p, nF);
+        }
+        posP2.ensure(std::max<uint32_t>(nF, 1)); velRho2.ensure(std::max<uint32_t>(nF, 1));
+        idF2.ensure(std::max<uint32_t>(nF, 1));
+        // boundary: defaults psi = massB, vol = massB / rho0 (state_sim.h:347-362)
+        const float defPsi = p.massB, defVol = p.restDensity > 0.0f ? p.massB / p.restDensity : 0.0f;
+        ids.clear();
+        if (!v.idB) { ids.resize(nB); for (uint32_t i = 0; i < nB; i++) ids[i] = i; }
+        Upload(idB, v.idB ? v.idB : ids.data(), nB);
+        Pack4(posB, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, defPsi, tmp);
+        volB.ensure(std::max<uint32_t>(nB, 1));
+        if (nB) {
+            if (v.volB) CK(cudaMemcpyAsync(volB.p, v.volB, nB * sizeof(float), cudaMemcpyHostToDevice, s));
+            else {
+                std::vector<float> d(nB, defVol);
+                CK(cudaMemcpy(volB.p, d.data(), nB * sizeof(float), cudaMemcpyHostToDevice));
+            }
+        }
+        posB2.ensure(std::max<uint32_t>(nB, 1)); volB2.ensure(std::max<uint32_t>(nB, 1));
+        idB2.ensure(std::max<uint32_t>(nB, 1));
+        // rigid particles (storage order preserved)
+        ids.clear();
+        if (!v.idR) { ids.resize(nR); for (uint32_t i = 0; i < nR; i++) ids[i] = i; }
+        Upload(idR, v.idR ? v.idR : ids.data(), nR);
+        hBodyR.assign(nR, 0);
+        for (uint32_t i = 0; i < nR; i++) hBodyR[i] = v.bodyIdR ? v.bodyIdR[i] : 0u;
+        for (uint32_t i = 0; i < nR; i++)
+            if (hBodyR[i] >= nRB) throw Error(TSP_ERR_RIGID, "Invalid rigid particle attachment.");
+        Upload(bodyR, hBodyR.data(), nR);
+        hRelX.assign(nR, 0.f); hRelY.assign(nR, 0.f); hRelZ.assign(nR, 0.f);
+        for (uint32_t i = 0; i < nR; i++) {
+            hRelX[i] = v.xPosRelR ? v.xPosRelR[i] : 0.f;
+            hRelY[i] = v.yPosRelR ? v.yPosRelR[i] : 0.f;
+            hRelZ[i] = v.zPosRelR ? v.zPosRelR[i] : 0.f;
+        }
+        Pack4(relR, nR, v.xPosRelR, v.yPosRelR, v.zPosRelR, v.volR, defVol, tmp);
+        Pack4(posR, nR, nullptr, nullptr, nullptr, v.psiR, defPsi, tmp);
+        velR.ensure(std::max<uint32_t>(nR, 1)); velPredR.ensure(std::max<uint32_t>(nR, 1));
+        forceR.ensure(std::max<uint32_t>(nR, 1));
+        if (nR) CK(cudaMemsetAsync(forceR.p, 0, nR * sizeof(float4), s));
+        volR.ensure(std::max<uint32_t>(nR, 1)); psiR.ensure(std::max<uint32_t>(nR, 1));
+        hByBodyOff.assign(nRB + 1, 0);
+        for (uint32_t i = 0; i < nR; i++) hByBodyOff[hBodyR[i] + 1]++;
+        for (uint32_t b = 0; b < nRB; b++) hByBodyOff[b + 1] += hByBodyOff[b];
+        hByBodyIdx.assign(nR, 0);
+        {
+            std::vector<uint32_t> cur(hByBodyOff.begin(), hByBodyOff.end() - 1);
+            for (uint32_t i = 0; i < nR; i++) hByBodyIdx[cur[hBodyR[i]]++] = i;
+        }
+        Upload(byBodyOff, hByBodyOff.data(), hByBodyOff.size());
+        Upload(byBodyIdx, hByBodyIdx.data(), nR);
+        // bodies (FP64 state)
+        hIdRB.assign(nRB, 0); hCntRB.assign(nRB, 0);
+        std::vector<double> bs((size_t)nRB * 48, 0.0);
+        auto g = [](const float* a, uint32_t b, float d) { return a ? (double)a[b] : (double)d; };
+        for (uint32_t b = 0; b < nRB; b++) {
+            hIdRB[b] = v.idRB ? v.idRB[b] : b;
+            hCntRB[b] = v.rigidParticleCountRB ? v.rigidParticleCountRB[b] : 0u;
+            double* q = &bs[(size_t)b * 48];
+            q[0] = g(v.xCM, b, 0); q[1] = g(v.yCM, b, 0); q[2] = g(v.zCM, b, 0);
+            q[3] = g(v.xVelRB, b, 0); q[4] = g(v.yVelRB, b, 0); q[5] = g(v.zVelRB, b, 0);
+            q[6] = g(v.xOmegaRB, b, 0); q[7] = g(v.yOmegaRB, b, 0); q[8] = g(v.zOmegaRB, b, 0);
+            q[9] = g(v.xAngMomRB, b, 0); q[10] = g(v.yAngMomRB, b, 0); q[11] = g(v.zAngMomRB, b, 0);
+            const float* A[9] = {v.a00, v.a01, v.a02, v.a10, v.a11, v.a12, v.a20, v.a21, v.a22};
+            const float* I[9] = {v.iBodyInv00, v.iBodyInv01, v.iBodyInv02, v.iBodyInv10, v.iBodyInv11,
+                                 v.iBodyInv12, v.iBodyInv20, v.iBodyInv21, v.iBodyInv22};
+            for (int k = 0; k < 9; k++) { q[12 + k] = g(A[k], b, (k % 4 == 0) ? 1.f : 0.f); q[23 + k] = g(I[k], b, 0.f); }
+            q[21] = g(v.massRB, b, 0); q[22] = g(v.massInvRB, b, 0);
+        }
+        Upload(bodyState, bs.data(), bs.size());
+        bodyFT.ensure(std::max<size_t>((size_t)nRB * 6, 1));
+        CK(cudaMemsetAsync(bodyFT.p, 0, bodyFT.cap * sizeof(double), s));
+        // neighbor-search state is rebuilt from scratch
+        frameValid = false; frameRebuilds = 0; cellSize = 0.0f; reach = 1; bSortedForFrame = false;
+        bAabbValid = false; listsValid = false;
+        CK(cudaMemsetAsync(st.p, 0, sizeof(SolverState), s));
+        // UpdateRigidParticles() at import (cpu_backend.cpp:326)
+        if (nR) LaunchRigidUpdateParticles(RigidView(), BodyView(), false, err.p, s);
+        CheckErrors();
+    }
+
+    void Push(tsp_state_view& v) {
+        CK(cudaSetDevice(device));
+        v.N_F = nF; v.N_B = nB; v.N_R = nR; v.N_RB = nRB; v.step = stepCount; v.time = simTime;
+        DBuf<float> tmp, tmp2;
+        if (v.idF && nF) CK(cudaMemcpyAsync(v.idF, idF.p, nF * 8ull, cudaMemcpyDeviceToHost, s));
+        Unpack4(posP.p, nF, v.xPosF, v.yPosF, v.zPosF, v.pressureF, tmp);
+        Sync();
+        Unpack4(velRho.p, nF, v.xVelF, v.yVelF, v.zVelF, v.densityF, tmp);
+        Sync();
+        Unpack4(velPred.p, nF, v.xVelPredF, v.yVelPredF, v.zVelPredF, nullptr, tmp);
+        Sync();
+        Unpack4(acc.p, nF, v.xAccPressF, v.yAccPressF, v.zAccPressF, nullptr, tmp);
+        Sync();
+        if (nF && (v.sourceTermF || v.diagElemF)) {
+            tmp.ensure(2ull * nF);
+            KUnpack2<<<G(nF), 256, 0, s>>>(srcDiag.p, tmp.p, tmp.p + nF, nF);
+            if (v.sourceTermF) CK(cudaMemcpyAsync(v.sourceTermF, tmp.p, nF * 4ull, cudaMemcpyDeviceToHost, s));
+            if (v.diagElemF) CK(cudaMemcpyAsync(v.diagElemF, tmp.p + nF, nF * 4ull, cudaMemcpyDeviceToHost, s));
+            Sync();
+        }
+        if (v.idB && nB) CK(cudaMemcpyAsync(v.idB, idB.p, nB * 8ull, cudaMemcpyDeviceToHost, s));
+        Unpack4(posB.p, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, tmp);
+        if (v.volB && nB) CK(cudaMemcpyAsync(v.volB, volB.p, nB * 4ull, cudaMemcpyDeviceToHost, s));
+        Sync();
+        if (v.idR && nR) CK(cudaMemcpyAsync(v.idR, idR.p, nR * 8ull, cudaMemcpyDeviceToHost, s));
+        if (v.bodyIdR && nR) CK(cudaMemcpyAsync(v.bodyIdR, bodyR.p, nR * 4ull, cudaMemcpyDeviceToHost, s));
+        Unpack4(relR.p, nR, v.xPosRelR, v.yPosRelR, v.zPosRelR, v.volR, tmp);
+        Sync();
+        Unpack4(posR.p, nR, v.xPosR, v.yPosR, v.zPosR, v.psiR, tmp);
+        Sync();
+        if (nRB) {
+            std::vector<double> bs((size_t)nRB * 48);
+            CK(cudaMemcpyAsync(bs.data(), bodyState.p, bs.size() * 8, cudaMemcpyDeviceToHost, s));
+            Sync();
+            for (uint32_t b = 0; b < nRB; b++) {
+                const double* q = &bs[(size_t)b * 48];
+                auto put = [&](float* a, double x) { if (a) a[b] = (float)x; };
+                if (v.idRB) v.idRB[b] = hIdRB[b];
+                if (v.rigidParticleCountRB) v.rigidParticleCountRB[b] = hCntRB[b];
+                put(v.xCM, q[0]); put(v.yCM, q[1]); put(v.zCM, q[2]);
+                put(v.xVelRB, q[3]); put(v.yVelRB, q[4]); put(v.zVelRB, q[5]);
+                put(v.xOmegaRB, q[6]); put(v.yOmegaRB, q[7]); put(v.zOmegaRB, q[8]);
+                put(v.xAngMomRB, q[9]); put(v.yAngMomRB, q[10]); put(v.zAngMomRB, q[11]);
+                float* A[9] = {v.a00, v.a01, v.a02, v.a10, v.a11, v.a12, v.a20, v.a21, v.a22};
+                float* I[9] = {v.iBodyInv00, v.iBodyInv01, v.iBodyInv02, v.iBodyInv10, v.iBodyInv11,
+                               v.iBodyInv12, v.iBodyInv20, v.iBodyInv21, v.iBodyInv22};
+                for (int k = 0; k < 9; k++) { put(A[k], q[12 + k]); put(I[k], q[23 + k]); }
+                put(v.massRB, q[21]); put(v.massInvRB, q[22]);
+            }
+        }
+        Sync();
+    }
+
+    // -------------------------------------------------------------------------- views
+    FluidDev FluidView() { return FluidDev{posP.p, velRho.p, velPred.p, acc.p, srcDiag.p, nF}; }
+    BoundaryDev BoundaryView() { return BoundaryDev{posB.p, volB.p, nB}; }
+    RigidDev RigidDevView() { return RigidDev{posR.p, velR.p, velPredR.p, nR}; }
+    RigidParticlesDev RigidView() {
+        return RigidParticlesDev{bodyR.p, relR.p, posR.p, velR.p, velPredR.p, forceR.p, nR, byBodyOff.p, byBodyIdx.p};
+    }
+    BodyDev BodyView() { return BodyDev{bodyState.p, bodyFT.p, nRB}; }
+    SellMeta Meta(int k) {
+        Sell& m = sell[k];
+        return SellMeta{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p,
+                        (uint64_t)m.l16.cap, (uint64_t)m.l32.cap};
+    }
+    NeighborView NView() {
+        auto sv = [&](int k) {
+            Sell& m = sell[k];
+            return SellView{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p};
+        };
+        return NeighborView{sv(0), sv(1), sv(2)};
+    }
+    SolverControl Control() const {
+        return SolverControl{prm.minSolverIters, prm.maxSolverIters, prm.fixedIters, prm.solverTerminationCond,
+                             prm.densityDevTarget, nF};
+    }
+
+    // -------------------------------------------------------------------------- neighbor build
+    void SetCellSize() {  // neighbor_search.cpp:1645-1659
+        const float cs = prm.kernelRadius * prm.gridCellSizeRatio;
+        const bool zero = std::fabs(cs) <= 1e-7f;
+        const float span = zero ? 0.0f : (prm.kernelRadius / cs);
+        const uint32_t r = zero ? 1u : std::max<uint32_t>(1u, (uint32_t)std::ceil(std::max(0.0f, span - 1e-6f)));
+        if (std::fabs(cellSize - cs) > 1e-7f || reach != r) { frameValid = false; bSortedForFrame = false; }
+        cellSize = cs;
+        reach = r;
+        fr.cellSizeInv = zero ? 0.0f : 1.0f / cs;
+        fr.reach = r;
+    }
+    // UpdateCellFrame (neighbor_search.cpp:1902-2006); returns true when the frame changed
+    bool UpdateFrame() {
+        if (nF == 0 && nB == 0 && nR == 0) { frameValid = false; return false; }
+        ProbeResult init;
+        for (int a = 0; a < 3; a++) { init.mnKey[a] = 0x7fffffff; init.mxKey[a] = (int)0x80000000; }
+        init.exceeded = 0; init.pad = 0;
+        hm->probe = init;
+        CK(cudaMemcpyAsync(probe.p, &hm->probe, sizeof(ProbeResult), cudaMemcpyHostToDevice, s));
+        LaunchProbe(posP.p, nF, fr, frameValid, dom, probe.p, s);
+        LaunchProbe(posR.p, nR, fr, frameValid, dom, probe.p, s);
+        launches += (nF ? 1 : 0) + (nR ? 1 : 0);
+        CK(cudaMemcpyAsync(&hm->probe, probe.p, sizeof(ProbeResult), cudaMemcpyDeviceToHost, s));
+        Sync();
+        ProbeResult pr = hm->probe;
+        float mn[3], mx[3];
+        for (int a = 0; a < 3; a++) { mn[a] = OrderedIntToFloat(pr.mnKey[a]); mx[a] = OrderedIntToFloat(pr.mxKey[a]); }
+        if (nB && !bAabbValid) {
+            // boundary particles never move: their bounds are probed once per import
+            hm->probe = init;
+            CK(cudaMemcpyAsync(probe.p, &hm->probe, sizeof(ProbeResult), cudaMemcpyHostToDevice, s));
+            LaunchProbe(posB.p, nB, fr, false, dom, probe.p, s);
+            CK(cudaMemcpyAsync(&hm->probe, probe.p, sizeof(ProbeResult), cudaMemcpyDeviceToHost, s));
+            Sync();
+            for (int a = 0; a < 3; a++) { bMin[a] = OrderedIntToFloat(hm->probe.mnKey[a]); bMax[a] = OrderedIntToFloat(hm->probe.mxKey[a]); }
+            bAabbValid = true;
+        }
+        bool rebuild = !frameValid;
+        if (!rebuild) {
+            const int m = (int)reach;
+            const bool innerEmpty = fr.ox + m > fr.ox + (int)fr.nx - 1 - m || fr.oy + m > fr.oy + (int)fr.ny - 1 - m ||
+                                    fr.oz + m > fr.oz + (int)fr.nz - 1 - m;
+            rebuild = innerEmpty || pr.exceeded != 0;
+        }
+        if (!rebuild) return false;
+        if (nB)
+            for (int a = 0; a < 3; a++) { mn[a] = std::min(mn[a], bMin[a]); mx[a] = std::max(mx[a], bMax[a]); }
+        if (dom.bounded)
+            for (int a = 0; a < 3; a++) {
+                mn[a] = std::clamp(mn[a], dom.mn[a], dom.mx[a]);
+                mx[a] = std::clamp(mx[a], dom.mn[a], dom.mx[a]);
+            }
+        const int64_t margin = (int64_t)reach + 8;
+        int64_t o[3], e[3];
+        for (int a = 0; a < 3; a++) {
+            o[a] = (int64_t)HostFloorToInt(mn[a] * fr.cellSizeInv) - margin;
+            e[a] = (int64_t)HostFloorToInt(mx[a] * fr.cellSizeInv) + margin;
+            if (o[a] > e[a] || o[a] < INT32_MIN || e[a] > INT32_MAX || e[a] - o[a] + 1 > (int64_t)(1u << 21))
+                throw Error(TSP_ERR_FRAME, "Compact CLL cell frame exceeds the supported range.");
+        }
+        fr.ox = (int32_t)o[0]; fr.oy = (int32_t)o[1]; fr.oz = (int32_t)o[2];
+        fr.nx = (uint32_t)(e[0] - o[0] + 1); fr.ny = (uint32_t)(e[1] - o[1] + 1); fr.nz = (uint32_t)(e[2] - o[2] + 1);
+        fr.keyBits = HostKeyBits(fr.nx, fr.ny, fr.nz);
+        frameValid = true;
+        frameRebuilds++;
+        const uint64_t cells = (uint64_t)fr.nx * fr.ny * fr.nz;
+        if (cells > (1ull << 28))
+            throw Error(TSP_ERR_UNSUPPORTED, "cell frame volume exceeds the dense grid limit (2^28 cells)");
+        gridCells = cells;
+        return true;
+    }
+    void EnsureNsScratch() {
+        const uint32_t nMax = std::max(nF, std::max(nB, nR));
+        keysA.ensure(std::max<uint32_t>(nMax, 1)); keysB.ensure(std::max<uint32_t>(nMax, 1));
+        valsA.ensure(std::max<uint32_t>(nMax, 1)); valsB.ensure(std::max<uint32_t>(nMax, 1));
+        tileHist.ensure(RadixTileHistItems(std::max<uint32_t>(nMax, 1)));
+        digitTotals.ensure(256);
+        scanScratch.ensure(ScanScratchItems(std::max<uint32_t>(nMax, 1) + 1));
+        scanScratch2.ensure(ScanScratchItems(std::max<uint32_t>(nMax, 1) + 1));
+        permF.ensure(std::max<uint32_t>(nF, 1)); permB.ensure(std::max<uint32_t>(nB, 1));
+        permR.ensure(std::max<uint32_t>(nR, 1));
+        cidF.ensure(std::max<uint32_t>(nF, 1)); cidB.ensure(std::max<uint32_t>(nB, 1));
+        cidR.ensure(std::max<uint32_t>(nR, 1)); cidRs.ensure(std::max<uint32_t>(nR, 1));
+        uniqF.ensure(std::max<uint32_t>(nF, 1)); uniqB.ensure(std::max<uint32_t>(nB, 1));
+        uniqR.ensure(std::max<uint32_t>(nR, 1));
+        startF.ensure(nF + 1ull); startB.ensure(nB + 1ull); startR.ensure(nR + 1ull);
+        const uint32_t nChunks = (nF + SELL_W - 1) / SELL_W;
+        for (int k = 0; k < 3; k++) {
+            Sell& m = sell[k];
+            m.counts.ensure(std::max<uint32_t>(nF, 1));
+            m.pitch.ensure(std::max<uint32_t>(nChunks, 1)); m.format.ensure(std::max<uint32_t>(nChunks, 1));
+            m.base.ensure(std::max<uint32_t>(nChunks, 1)); m.base2.ensure(std::max<uint32_t>(nChunks, 1));
+            m.offset.ensure(std::max<uint32_t>(nChunks, 1));
+            m.l16.ensure(std::max<size_t>(m.l16.cap, 16)); m.l32.ensure(std::max<size_t>(m.l32.cap, 16));
+            cntR[k].ensure(std::max<uint32_t>(nR, 1)); offR[k].ensure(nR + 1ull);
+            listR[k].ensure(std::max<size_t>(listR[k].cap, 16));
+        }
+        velPred2.ensure(std::max<uint32_t>(nF, 1)); acc2.ensure(std::max<uint32_t>(nF, 1));
+        srcDiag2.ensure(std::max<uint32_t>(nF, 1));
+    }
+    // ReOrderParticleData + Construct + Query_Count + Finalize_Count + Query_Fill
+    void NeighborBuild(bool permuteAll) {
+        SetCellSize();
+        const bool frameChanged = UpdateFrame();
+        if (!frameValid) { listsValid = false; return; }
+        EnsureNsScratch();
+        SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p};
+        if (frameChanged || !bSortedForFrame) {
+            gridF.ensure(gridCells); gridB.ensure(gridCells); gridR.ensure(gridCells);
+            // boundary: a stable sort of already sorted cell IDs is the identity, so the
+            // reference's "sort only when not non-decreasing" (1779-1810) is the same result
+            if (nB) {
+                SortByCell(posB.p, nB, fr, sc, permB.p, cidB.p, s);
+                GatherF4(permB.p, posB.p, posB2.p, nB, s); Swap(posB, posB2);
+                GatherF1(permB.p, volB.p, volB2.p, nB, s); Swap(volB, volB2);
+                GatherU64(permB.p, idB.p, idB2.p, nB, s); Swap(idB, idB2);
+                BuildCellTable(cidB.p, nB, uniqB.p, startB.p, nCellsDev.p + 1, scanScratch.p, s);
+                BuildGrid(uniqB.p, nCellsDev.p + 1, nB, fr, gridB.p, gridCells, s);
+                launches += SortLaunches(nB, fr.keyBits) + 3 + 3 + 1;
+            }
+            bSortedForFrame = true;
+        } else if (nB) {
+            KIota<<<G(nB), 256, 0, s>>>(permB.p, nB);
+            launches += 1;
+        }
+        // fluid: IDs, pos (+pressure), vel (+density) always; all fields for a standalone search
+        if (nF) {
+            SortByCell(posP.p, nF, fr, sc, permF.p, cidF.p, s);
+            LaunchReorderFluidStep(permF.p, posP.p, velRho.p, idF.p, posP2.p, velRho2.p, idF2.p, nF, s);
+            Swap(posP, posP2); Swap(velRho, velRho2); Swap(idF, idF2);
+            if (permuteAll) {
+                GatherF4(permF.p, velPred.p, velPred2.p, nF, s); Swap(velPred, velPred2);
+                GatherF4(permF.p, acc.p, acc2.p, nF, s); Swap(acc, acc2);
+                GatherF2(permF.p, srcDiag.p, srcDiag2.p, nF, s); Swap(srcDiag, srcDiag2);
+            }
+            BuildCellTable(cidF.p, nF, uniqF.p, startF.p, nCellsDev.p + 0, scanScratch.p, s);
+            BuildGrid(uniqF.p, nCellsDev.p + 0, nF, fr, gridF.p, gridCells, s);
+            launches += SortLaunches(nF, fr.keyBits) + 1 + (permuteAll ? 3 : 0) + 3 + 1;
+        }
+        // rigid: cell IDs in storage order, sorted index permutation (747-774)
+        if (nR) {
+            LaunchCellIds(posR.p, nR, fr, cidR.p, s);
+            SortByCell(posR.p, nR, fr, sc, permR.p, cidRs.p, s);
+            BuildCellTable(cidRs.p, nR, uniqR.p, startR.p, nCellsDev.p + 2, scanScratch.p, s);
+            BuildGrid(uniqR.p, nCellsDev.p + 2, nR, fr, gridR.p, gridCells, s);
+            launches += 1 + SortLaunches(nR, fr.keyBits) + 3 + 1;
+        }
+        QueryArgs qa = MakeQueryArgs();
+        SellMeta m0 = Meta(0), m1 = Meta(1), m2 = Meta(2);
+        RigidLists rl = RLists();
+        LaunchQueryFluid(false, qa, m0, m1, m2, s);
+        LaunchQueryRigid(false, qa, rl, s);
+        const uint32_t nChunks = (nF + SELL_W - 1) / SELL_W;
+        for (int k = 0; k < 3; k++) FinalizeSell(Meta(k), nChunks, scanScratch2.p, sellTot.p + k, s);
+        for (int k = 0; k < 3; k++) FinalizeCsr(cntR[k].p, offR[k].p, nR, scanScratch.p, csrTot.p + k, s);
+        CK(cudaMemcpyAsync(hm->sellTot, sellTot.p, 3 * sizeof(U64x2), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hm->csrTot, csrTot.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hm->nCells, nCellsDev.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        Sync();
+        for (int k = 0; k < 3; k++) {
+            sell[k].n16 = hm->sellTot[k].a;
+            sell[k].n32 = hm->sellTot[k].b;
+            sell[k].l16.grow(sell[k].n16, 1.04);
+            sell[k].l32.grow(sell[k].n32, 1.04);
+            csrN[k] = hm->csrTot[k];
+            listR[k].grow(csrN[k], 1.04);
+        }
+        m0 = Meta(0); m1 = Meta(1); m2 = Meta(2);
+        rl = RLists();
+        LaunchQueryFluid(true, qa, m0, m1, m2, s);
+        LaunchQueryRigid(true, qa, rl, s);
+        launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + (nF ? 9u : 0u) + (nR ? 9u : 0u);
+        listsValid = true;
+    }
+    QueryArgs MakeQueryArgs() {
+        QueryArgs qa{};
+        qa.posF = posP.p; qa.cidF = cidF.p; qa.nF = nF;
+        qa.posB = posB.p; qa.nB = nB;
+        qa.posR = posR.p; qa.permR = permR.p; qa.bodyR = bodyR.p; qa.nR = nR;
+        qa.startF = startF.p; qa.startB = startB.p; qa.startR = startR.p;
+        qa.gridF = nF ? gridF.p : nullptr; qa.gridB = nB ? gridB.p : nullptr; qa.gridR = nR ? gridR.p : nullptr;
+        qa.fr = fr; qa.r2 = prm.kernelRadiusSqu; qa.cap = QueryCap(reach); qa.err = err.p;
+        return qa;
+    }
+    RigidLists RLists() {
+        return RigidLists{cntR[0].p, cntR[1].p, cntR[2].p, offR[0].p, offR[1].p, offR[2].p,
+                          listR[0].p, listR[1].p, listR[2].p};
+    }
+
+    // -------------------------------------------------------------------------- Jacobi loop graph
+    uint64_t GraphKey(const Consts& c, const SolverControl& ctl) {
+        uint64_t h = 1469598103934665603ull;
+        FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
+        h = HashBytes(h, &f, sizeof(f)); h = HashBytes(h, &b, sizeof(b)); h = HashBytes(h, &r, sizeof(r));
+        h = HashBytes(h, &nv, sizeof(nv)); h = HashBytes(h, &c, sizeof(c)); h = HashBytes(h, &ctl, sizeof(ctl));
+        void* ptrs[2] = {st.p, partials.p};
+        h = HashBytes(h, ptrs, sizeof(ptrs));
+        return h;
+    }
+    cudaGraphExec_t JacobiGraphFor(const Consts& c, const SolverControl& ctl) {
+        const uint64_t key = GraphKey(c, ctl);
+        for (auto& g : graphs)
+            if (g.ex && g.key == key) return g.ex;
+        // build: while (cond) { pressure acceleration; Jacobi sweep (sets cond) }
+        cudaGraph_t graph;
+        CK(cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle handle;
+        CK(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamBeginCaptureToGraph(capStream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
+        LaunchPressureAcc(c, f, b, r, nv, capStream);
+        LaunchJacobi(c, f, b, r, nv, ctl, st.p, partials.p, (unsigned long long)handle, true, capStream);
+        cudaGraph_t captured;
+        CK(cudaStreamEndCapture(capStream, &captured));
+        cudaGraphExec_t ex;
+        CK(cudaGraphInstantiate(&ex, graph, 0));
+        const size_t maxGraphs = 4;
+        if (graphs.size() < maxGraphs) graphs.push_back({});
+        JacobiGraph& slot = graphs[graphNext % graphs.size()];
+        graphNext++;
+        if (slot.ex) cudaGraphExecDestroy(slot.ex);
+        if (slot.g) cudaGraphDestroy(slot.g);
+        slot.key = key; slot.g = graph; slot.ex = ex;
+        return ex;
+    }
+
+    // -------------------------------------------------------------------------- step
+    void Step(const tsp_params& p) {  // Step_IISPH (sph_solver.cpp:34-319) without the contact solve
+        CK(cudaSetDevice(device));
+        prm = p;
+        if (p.solverTerminationCond > 3) throw Error(TSP_ERR_INVALID, "unknown solver termination condition");
+        if (p.maxSolverIters > MAX_JACOBI_SWEEPS || p.minSolverIters > MAX_JACOBI_SWEEPS)
+            throw Error(TSP_ERR_UNSUPPORTED, "solver iteration bounds above 100000");
+        if (!(p.timeStep >= 0.0f) || !(p.particleSizeF > 0.0f) || !(p.kernelRadiusSqu > 0.0f))
+            throw Error(TSP_ERR_INVALID, "time step, particle size and kernel radius must be positive");
+        if (nF == 0 && nRB == 0) return;  // empty serial sim (cpu_backend.cpp:2309-2315)
+        const Consts c = MakeConsts(prm);
+        CK(cudaEventRecord(ev[0], s));
+        NeighborBuild(false);
+        CK(cudaEventRecord(ev[1], s));
+        FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
+        RigidParticlesDev rp = RigidView(); BodyDev bd = BodyView();
+        LaunchDensity(c, f, b, r, nv, s);
+        if (nRB) LaunchRigidClearAddGravity(bd, prm.gravity[0], prm.gravity[1], prm.gravity[2], s);
+        LaunchNonPressure(c, f, b, r, nv, s);
+        if (nRB) {
+            LaunchRigidViscousForces(c, rp, f, offR[0].p, listR[0].p, s);
+            LaunchRigidReduce(rp, bd, s);
+            LaunchRigidPredict(bd, prm.timeStep, s);
+            LaunchRigidUpdateParticles(rp, bd, true, err.p, s);
+        }
+        LaunchSourceDiagInit(c, f, b, r, nv, st.p, s);
+        CK(cudaEventRecord(ev[2], s));
+        if (nF) {
+            partials.ensure(3ull * JacobiBlocks(nF) + 3);
+            const SolverControl ctl = Control();
+            cudaGraphExec_t ex = JacobiGraphFor(c, ctl);
+            CK(cudaGraphLaunch(ex, s));
+        }
+        CK(cudaEventRecord(ev[3], s));
+        LaunchPressureAcc(c, f, b, r, nv, s);
+        if (nRB) {
+            LaunchRigidPressureForces(c, rp, f, offR[0].p, listR[0].p, s);
+            LaunchRigidClearAddGravity(bd, prm.gravity[0], prm.gravity[1], prm.gravity[2], s);
+            LaunchRigidReduce(rp, bd, s);
+        }
+        LaunchIntegration(c, f, s);
+        if (nRB) {
+            LaunchRigidPredict(bd, prm.timeStep, s);
+            LaunchRigidIntegrate(bd, prm.timeStep, err.p, s);
+            LaunchRigidUpdateParticles(rp, bd, false, err.p, s);
+        }
+        CK(cudaMemcpyAsync(&hm->st, st.p, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
+        launches += (nF ? 6u : 0u) + (nRB ? 13u : 0u);
+        cudaEvent_t evEnd;
+        CK(cudaEventCreate(&evEnd));
+        CK(cudaEventRecord(evEnd, s));
+        CheckErrors();
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[0], evEnd); lastStepMs = t;
+        cudaEventElapsedTime(&t, ev[0], ev[1]); lastNbrMs = t;
+        cudaEventElapsedTime(&t, ev[2], ev[3]); lastJacMs = t;
+        cudaEventDestroy(evEnd);
+        if (nF && hm->st.iters > 0) launches += 2ull * (hm->st.iters - 1u);
+    }
+
+    void NeighborSearchStandalone(const tsp_params& p) {  // ExecuteNeighborSearch (cpu_backend.cpp:1593-1624)
+        CK(cudaSetDevice(device));
+        prm = p;
+        NeighborBuild(true);
+        CheckErrors();
+    }
+
+    void RunStage(const tsp_params& p, uint32_t stage, double* errSums) {
+        CK(cudaSetDevice(device));
+        prm = p;
+        const Consts c = MakeConsts(prm);
+        FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
+        if (stage != TSP_STAGE_BOUNDARY_VOLUMES && stage != TSP_STAGE_INTEGRATION && !listsValid)
+            throw Error(TSP_ERR_INVALID, "run the neighbor search before a solver stage");
+        switch (stage) {
+            case TSP_STAGE_DENSITY: LaunchDensity(c, f, b, r, nv, s); break;
+            case TSP_STAGE_NON_PRESSURE: LaunchNonPressure(c, f, b, r, nv, s); break;
+            case TSP_STAGE_SOURCE_DIAG_INIT: LaunchSourceDiagInit(c, f, b, r, nv, st.p, s); break;
+            case TSP_STAGE_PRESSURE_ACC: LaunchPressureAcc(c, f, b, r, nv, s); break;
+            case TSP_STAGE_JACOBI_UPDATE: {
+                partials.ensure(3ull * JacobiBlocks(nF) + 3);
+                LaunchJacobi(c, f, b, r, nv, Control(), st.p, partials.p, 0ull, false, s);
+                CK(cudaMemcpyAsync(&hm->st, st.p, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
+                Sync();
+                if (errSums) for (int k = 0; k < 3; k++) errSums[k] = hm->st.sums[k];
+                break;
+            }
+            case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); break;
+            case TSP_STAGE_BOUNDARY_VOLUMES: BoundaryVolumes(c); break;
+            default: throw Error(TSP_ERR_INVALID, "unknown stage");
+        }
+        CheckErrors();
+    }
+
+    // device time per launch of one solver stage (CUDA events on the backend stream)
+    float TimeStage(const tsp_params& p, uint32_t stage, uint32_t reps) {
+        CK(cudaSetDevice(device));
+        prm = p;
+        if (!listsValid) throw Error(TSP_ERR_INVALID, "run the neighbor search before timing a stage");
+        if (reps == 0) reps = 1;
+        const Consts c = MakeConsts(prm);
+        FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
+        partials.ensure(3ull * JacobiBlocks(nF) + 3);
+        const SolverControl ctl = Control();
+        Sync();
+        CK(cudaEventRecord(ev[0], s));
+        for (uint32_t k = 0; k < reps; k++) {
+            switch (stage) {
+                case TSP_STAGE_DENSITY: LaunchDensity(c, f, b, r, nv, s); break;
+                case TSP_STAGE_NON_PRESSURE: LaunchNonPressure(c, f, b, r, nv, s); break;
+                case TSP_STAGE_SOURCE_DIAG_INIT: LaunchSourceDiagInit(c, f, b, r, nv, st.p, s); break;
+                case TSP_STAGE_PRESSURE_ACC: LaunchPressureAcc(c, f, b, r, nv, s); break;
+                case TSP_STAGE_JACOBI_UPDATE: LaunchJacobi(c, f, b, r, nv, ctl, st.p, partials.p, 0ull, false, s); break;
+                case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); break;
+                default: throw Error(TSP_ERR_INVALID, "stage cannot be timed");
+            }
+            launches += 1;
+        }
+        CK(cudaEventRecord(ev[1], s));
+        CheckErrors();
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+        return ms / (float)reps;
+    }
+
+    // ComputeBoundaryCoefficients / ComputeRigidCoefficients (builder.cpp:150-376)
+    void BoundaryVolumes(const Consts& c) {
+        const float defPsi = prm.massB, defVol = prm.restDensity > 0.0f ? prm.massB / prm.restDensity : 0.0f;
+        const float cs = prm.kernelRadius * prm.gridCellSizeRatio;
+        if (!(prm.particleSizeF > 0.f && prm.kernelRadius > 0.f && prm.kernelRadiusSqu > 0.f &&
+              prm.gridCellSizeRatio > 0.f && prm.restDensity > 0.f && cs > 0.f)) {
+            std::vector<float> dv(std::max(nB, nR), defVol), dp(std::max(nB, nR), defPsi);
+            if (nB) {
+                CK(cudaMemcpy(volB.p, dv.data(), nB * 4ull, cudaMemcpyHostToDevice));
+                psiTmpB.ensure(nB);
+                CK(cudaMemcpy(psiTmpB.p, dp.data(), nB * 4ull, cudaMemcpyHostToDevice));
+                KSetW<<<G(nB), 256, 0, s>>>(posB.p, psiTmpB.p, nB);
+            }
+            if (nR) {
+                CK(cudaMemcpy(volR.p, dv.data(), nR * 4ull, cudaMemcpyHostToDevice));
+                CK(cudaMemcpy(psiR.p, dp.data(), nR * 4ull, cudaMemcpyHostToDevice));
+                KSetW<<<G(nR), 256, 0, s>>>(relR.p, volR.p, nR);
+                KSetW<<<G(nR), 256, 0, s>>>(posR.p, psiR.p, nR);
+            }
+            return;
+        }
+        if (nB) {
+            // the boundary must be sorted and gridded under the current frame
+            SetCellSize();
+            UpdateFrame();
+            EnsureNsScratch();
+            if (!bSortedForFrame) {
+                gridF.ensure(gridCells); gridB.ensure(gridCells); gridR.ensure(gridCells);
+                SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p};
+                SortByCell(posB.p, nB, fr, sc, permB.p, cidB.p, s);
+                GatherF4(permB.p, posB.p, posB2.p, nB, s); Swap(posB, posB2);
+                GatherF1(permB.p, volB.p, volB2.p, nB, s); Swap(volB, volB2);
+                GatherU64(permB.p, idB.p, idB2.p, nB, s); Swap(idB, idB2);
+                BuildCellTable(cidB.p, nB, uniqB.p, startB.p, nCellsDev.p + 1, scanScratch.p, s);
+                BuildGrid(uniqB.p, nCellsDev.p + 1, nB, fr, gridB.p, gridCells, s);
+                bSortedForFrame = true;
+            }
+            psiTmpB.ensure(nB);
+            LaunchBoundaryVolumes(c, posB.p, nB, startB.p, gridB.p, fr, defVol, defPsi, prm.restDensity, volB.p,
+                                  psiTmpB.p, s);
+            KSetW<<<G(nB), 256, 0, s>>>(posB.p, psiTmpB.p, nB);
+        }
+        if (nR) {
+            // per body, in the body frame, over the body's own particles, sorted by (z, y, x) cell
+            const float csInv = 1.0f / cs;
+            const float span = prm.kernelRadius / cs;
+            const int rr = std::max(1, (int)std::ceil(std::max(0.0f, span - 1e-6f)));
+            std::vector<uint32_t> sortedIdx(nR), bodyOf(nR);
+            std::vector<int4> cells(nR);
+            for (uint32_t b = 0; b < nRB; b++) {
+                const uint32_t lo = hByBodyOff[b], hi = hByBodyOff[b + 1];
+                std::vector<uint32_t> loc(hByBodyIdx.begin() + lo, hByBodyIdx.begin() + hi);
+                std::sort(loc.begin(), loc.end());
+                auto cellOf = [&](uint32_t i) {
+                    return int4{(int)std::floor(hRelX[i] * csInv), (int)std::floor(hRelY[i] * csInv),
+                                (int)std::floor(hRelZ[i] * csInv), 0};
+                };
+                std::stable_sort(loc.begin(), loc.end(), [&](uint32_t a, uint32_t bb) {
+                    const int4 ca = cellOf(a), cb = cellOf(bb);
+                    if (ca.z != cb.z) return ca.z < cb.z;
+                    if (ca.y != cb.y) return ca.y < cb.y;
+                    return ca.x < cb.x;
+                });
+                for (uint32_t k = 0; k < hi - lo; k++) {
+                    sortedIdx[lo + k] = loc[k];
+                    cells[lo + k] = cellOf(loc[k]);
+                    bodyOf[lo + k] = b;
+                }
+            }
+            DBuf<uint32_t> dIdx, dBody;
+            DBuf<int4> dCells;
+            Upload(dIdx, sortedIdx.data(), nR);
+            Upload(dBody, bodyOf.data(), nR);
+            Upload(dCells, cells.data(), nR);
+            LaunchRigidVolumesSorted(c, relR.p, byBodyOff.p, dIdx.p, dCells.p, dBody.p, nR, rr, defVol, defPsi,
+                                     prm.restDensity, volR.p, psiR.p, s);
+            KSetW<<<G(nR), 256, 0, s>>>(relR.p, volR.p, nR);
+            KSetW<<<G(nR), 256, 0, s>>>(posR.p, psiR.p, nR);
+            LaunchRigidUpdateParticles(RigidView(), BodyView(), false, err.p, s);
+            Sync();
+        }
+    }
+
+    // -------------------------------------------------------------------------- inspection
+    void ReadField(uint32_t field, void* out, uint32_t n) {
+        DBuf<float> tmp;
+        float* o = (float*)out;
+        auto un3 = [&](const float4* src, uint32_t cnt) {
+            if (n != cnt) throw Error(TSP_ERR_INVALID, "field size mismatch");
+            std::vector<float> a(cnt), b(cnt), c(cnt);
+            Unpack4(src, cnt, a.data(), b.data(), c.data(), nullptr, tmp);
+            Sync();
+            for (uint32_t i = 0; i < cnt; i++) { o[3 * i] = a[i]; o[3 * i + 1] = b[i]; o[3 * i + 2] = c[i]; }
+        };
+        auto unW = [&](const float4* src, uint32_t cnt) {
+            if (n != cnt) throw Error(TSP_ERR_INVALID, "field size mismatch");
+            Unpack4(src, cnt, nullptr, nullptr, nullptr, o, tmp);
+            Sync();
+        };
+        auto un1 = [&](const float* src, uint32_t cnt) {
+            if (n != cnt) throw Error(TSP_ERR_INVALID, "field size mismatch");
+            if (cnt) CK(cudaMemcpy(o, src, cnt * 4ull, cudaMemcpyDeviceToHost));
+        };
+        CK(cudaStreamSynchronize(s));
+        switch (field) {
+            case TSP_FIELD_POS: un3(posP.p, nF); break;
+            case TSP_FIELD_VEL: un3(velRho.p, nF); break;
+            case TSP_FIELD_VEL_PRED: un3(velPred.p, nF); break;
+            case TSP_FIELD_ACC_PRESS: un3(acc.p, nF); break;
+            case TSP_FIELD_PRESSURE: unW(posP.p, nF); break;
+            case TSP_FIELD_DENSITY: unW(velRho.p, nF); break;
+            case TSP_FIELD_SOURCE:
+            case TSP_FIELD_DIAG: {
+                if (n != nF) throw Error(TSP_ERR_INVALID, "field size mismatch");
+                std::vector<float2> v(nF);
+                if (nF) CK(cudaMemcpy(v.data(), srcDiag.p, nF * 8ull, cudaMemcpyDeviceToHost));
+                for (uint32_t i = 0; i < nF; i++) o[i] = field == TSP_FIELD_SOURCE ? v[i].x : v[i].y;
+                break;
+            }
+            case TSP_FIELD_VOL_B: un1(volB.p, nB); break;
+            case TSP_FIELD_PSI_B: unW(posB.p, nB); break;
+            case TSP_FIELD_VOL_R: unW(relR.p, nR); break;
+            case TSP_FIELD_PSI_R: unW(posR.p, nR); break;
+            case TSP_FIELD_FORCE_R: un3(forceR.p, nR); break;
+            case TSP_FIELD_BODY_FT:
+                if (n != nRB) throw Error(TSP_ERR_INVALID, "field size mismatch");
+                if (nRB) CK(cudaMemcpy(out, bodyFT.p, nRB * 6ull * 8ull, cudaMemcpyDeviceToHost));
+                break;
+            default: throw Error(TSP_ERR_INVALID, "unknown field");
+        }
+    }
+    void WriteField(uint32_t field, const void* in, uint32_t n) {
+        const float* x = (const float*)in;
+        CK(cudaStreamSynchronize(s));
+        auto setW = [&](DBuf<float4>& dst, uint32_t cnt) {
+            if (n != cnt) throw Error(TSP_ERR_INVALID, "field size mismatch");
+            DBuf<float> t;
+            t.ensure(std::max<uint32_t>(cnt, 1));
+            if (cnt) CK(cudaMemcpy(t.p, x, cnt * 4ull, cudaMemcpyHostToDevice));
+            KSetW<<<G(cnt), 256, 0, s>>>(dst.p, t.p, cnt);
+            Sync();
+        };
+        auto set3 = [&](DBuf<float4>& dst, uint32_t cnt) {
+            if (n != cnt) throw Error(TSP_ERR_INVALID, "field size mismatch");
+            std::vector<float4> h(cnt);
+            if (cnt) CK(cudaMemcpy(h.data(), dst.p, cnt * 16ull, cudaMemcpyDeviceToHost));
+            for (uint32_t i = 0; i < cnt; i++) { h[i].x = x[3 * i]; h[i].y = x[3 * i + 1]; h[i].z = x[3 * i + 2]; }
+            if (cnt) CK(cudaMemcpy(dst.p, h.data(), cnt * 16ull, cudaMemcpyHostToDevice));
+        };
+        switch (field) {
+            case TSP_FIELD_POS: set3(posP, nF); break;
+            case TSP_FIELD_VEL: set3(velRho, nF); break;
+            case TSP_FIELD_VEL_PRED: set3(velPred, nF); break;
+            case TSP_FIELD_ACC_PRESS: set3(acc, nF); break;
+            case TSP_FIELD_PRESSURE: setW(posP, nF); break;
+            case TSP_FIELD_DENSITY: setW(velRho, nF); break;
+            case TSP_FIELD_SOURCE:
+            case TSP_FIELD_DIAG: {
+                if (n != nF) throw Error(TSP_ERR_INVALID, "field size mismatch");
+                std::vector<float2> v(nF);
+                if (nF) CK(cudaMemcpy(v.data(), srcDiag.p, nF * 8ull, cudaMemcpyDeviceToHost));
+                for (uint32_t i = 0; i < nF; i++) (field == TSP_FIELD_SOURCE ? v[i].x : v[i].y) = x[i];
+                if (nF) CK(cudaMemcpy(srcDiag.p, v.data(), nF * 8ull, cudaMemcpyHostToDevice));
+                break;
+            }
+            case TSP_FIELD_VOL_B:
+                if (n != nB) throw Error(TSP_ERR_INVALID, "field size mismatch");
+                if (nB) CK(cudaMemcpy(volB.p, x, nB * 4ull, cudaMemcpyHostToDevice));
+                break;
+            case TSP_FIELD_PSI_B: setW(posB, nB); break;
+            default: throw Error(TSP_ERR_INVALID, "field is not writable");
+        }
+    }
+    void Stats(tsp_step_stats& o) {
+        Sync();
+        std::memset(&o, 0, sizeof(o));
+        o.step = stepCount; o.time = simTime;
+        o.solverIters = hm->st.iters;
+        o.errSumRaw = hm->st.sums[0]; o.errSumPos = hm->st.sums[1]; o.errSumAbs = hm->st.sums[2];
+        o.avgRelDensityErrRaw = hm->st.avg[0]; o.avgRelDensityErrPos = hm->st.avg[1]; o.avgRelDensityErrAbs = hm->st.avg[2];
+        o.frameRebuilds = frameRebuilds;
+        o.cellOrig[0] = fr.ox; o.cellOrig[1] = fr.oy; o.cellOrig[2] = fr.oz;
+        o.cellDims[0] = fr.nx; o.cellDims[1] = fr.ny; o.cellDims[2] = fr.nz;
+        o.keyBits = fr.keyBits;
+        CK(cudaMemcpy(hm->nCells, nCellsDev.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        o.nCellsF = nF ? (uint32_t)hm->nCells[0] : 0; o.nCellsB = nB ? (uint32_t)hm->nCells[1] : 0;
+        o.nCellsR = nR ? (uint32_t)hm->nCells[2] : 0;
+        uint64_t tot[3] = {0, 0, 0};
+        if (listsValid && nF) {
+            for (int k = 0; k < 3; k++) {
+                std::vector<uint16_t> cnt(nF);
+                CK(cudaMemcpy(cnt.data(), sell[k].counts.p, nF * 2ull, cudaMemcpyDeviceToHost));
+                for (uint16_t c : cnt) tot[k] += c;
+            }
+        }
+        o.nNbrFF = tot[0]; o.nNbrFB = tot[1]; o.nNbrFR = tot[2];
+        o.nNbrRF = csrN[0]; o.nNbrRB = csrN[1]; o.nNbrRR = csrN[2];
+        for (int k = 0; k < 3; k++) o.sellPackedBytes += sell[k].n16 * 2 + sell[k].n32 * 4;
+        o.lastStepMs = lastStepMs; o.lastNeighborMs = lastNbrMs; o.lastJacobiMs = lastJacMs;
+    }
+};
+
+}  // namespace tsp
+
+// ================================================================================ C ABI
+using tsp::Backend;
+using tsp::Error;
+
+struct tsp_backend {
+    Backend* b;
+};
+
+static thread_local std::string g_lastError;
+
+#define TSP_GUARD(h, body)                                                 \
+    try {                                                                  \
+        body;                                                              \
+        return TSP_OK;                                                     \
+    } catch (const Error& e) {                                             \
+        if (h) (h)->b->lastErr = e.what();                                 \
+        g_lastError = e.what();                                            \
+        return e.code;                                                     \
+    } catch (const std::exception& e) {                                    \
+        if (h) (h)->b->lastErr = e.what();                                 \
+        g_lastError = e.what();                                            \
+        return TSP_ERR_INVALID;                                            \
+    }
+
+#define TSP_NEED(h)                                                        \
+    if (!(h) || !(h)->b) {                                                 \
+        g_lastError = "NULL backend handle";                               \
+        return TSP_ERR_INVALID;                                            \
+    }
+
+extern "C" {
+
+int tsp_b200_create(const tsp_params* params, int device, tsp_backend** out) {
+    if (!params || !out) { g_lastError = "NULL argument"; return TSP_ERR_INVALID; }
+    tsp_backend* h = nullptr;
+    try {
+        h = new tsp_backend{new Backend(device)};
+        h->b->prm = *params;
+        *out = h;
+        return TSP_OK;
+    } catch (const Error& e) {
+        g_lastError = e.what();
+        if (h) { delete h->b; delete h; }
+        return e.code;
+    } catch (const std::exception& e) {
+        g_lastError = e.what();
+        return TSP_ERR_INVALID;
+    }
+}
+int tsp_b200_destroy(tsp_backend* h) {
+    if (!h) return TSP_OK;
+    delete h->b;
+    delete h;
+    return TSP_OK;
+}
+const char* tsp_b200_name(const tsp_backend*) { return "B200 (sm_100a) IISPH"; }
+const char* tsp_b200_last_error(const tsp_backend* h) {
+    return (h && h->b) ? h->b->lastErr.c_str() : g_lastError.c_str();
+}
+int tsp_b200_set_domain(tsp_backend* h, const float* mn, const float* mx) {
+    TSP_NEED(h);
+    if (!mn || !mx) return TSP_ERR_INVALID;
+    TSP_GUARD(h, h->b->SetDomain(mn, mx));
+}
+int tsp_b200_pull_state(tsp_backend* h, const tsp_state_view* src, const tsp_params* p) {
+    TSP_NEED(h);
+    if (!src || !p) return TSP_ERR_INVALID;
+    TSP_GUARD(h, h->b->Pull(*src, *p));
+}
+int tsp_b200_push_state(tsp_backend* h, tsp_state_view* dst) {
+    TSP_NEED(h);
+    if (!dst) return TSP_ERR_INVALID;
+    TSP_GUARD(h, h->b->Push(*dst));
+}
+int tsp_b200_get_counts(const tsp_backend* h, uint32_t* nF, uint32_t* nB, uint32_t* nR, uint32_t* nRB) {
+    TSP_NEED(h);
+    if (nF) *nF = h->b->nF;
+    if (nB) *nB = h->b->nB;
+    if (nR) *nR = h->b->nR;
+    if (nRB) *nRB = h->b->nRB;
+    return TSP_OK;
+}
+int tsp_b200_neighbor_search(tsp_backend* h, const tsp_params* p) {
+    TSP_NEED(h);
+    if (!p) return TSP_ERR_INVALID;
+    TSP_GUARD(h, h->b->NeighborSearchStandalone(*p));
+}
+int tsp_b200_step(tsp_backend* h, const tsp_params* p, uint32_t n) {
+    TSP_NEED(h);
+    if (!p) return TSP_ERR_INVALID;
+    TSP_GUARD(h, {
+        for (uint32_t k = 0; k < n; k++) {
+            h->b->Step(*p);
+            h->b->stepCount += 1;
+            h->b->simTime += (double)p->timeStep;
+        }
+    });
+}
+int tsp_b200_get_stats(const tsp_backend* h, tsp_step_stats* out) {
+    TSP_NEED(h);
+    if (!out) return TSP_ERR_INVALID;
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, hh->b->Stats(*out));
+}
+int tsp_b200_read_cell_ids(const tsp_backend* h, uint32_t species, uint64_t* out, uint32_t n) {
+    TSP_NEED(h);
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, {
+        Backend& b = *hh->b;
+        b.Sync();
+        const uint32_t cnt = species == 0 ? b.nF : species == 1 ? b.nB : b.nR;
+        if (n != cnt || !out) throw Error(TSP_ERR_INVALID, "size mismatch");
+        const uint64_t* src = species == 0 ? b.cidF.p : species == 1 ? b.cidB.p : b.cidR.p;
+        if (cnt) CK(cudaMemcpy(out, src, cnt * 8ull, cudaMemcpyDeviceToHost));
+    });
+}
+int tsp_b200_read_permutation(const tsp_backend* h, uint32_t species, uint32_t* out, uint32_t n) {
+    TSP_NEED(h);
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, {
+        Backend& b = *hh->b;
+        b.Sync();
+        const uint32_t cnt = species == 0 ? b.nF : species == 1 ? b.nB : b.nR;
+        if (n != cnt || !out) throw Error(TSP_ERR_INVALID, "size mismatch");
+        const uint32_t* src = species == 0 ? b.permF.p : species == 1 ? b.permB.p : b.permR.p;
+        if (cnt) CK(cudaMemcpy(out, src, cnt * 4ull, cudaMemcpyDeviceToHost));
+    });
+}
+int tsp_b200_read_cell_table(const tsp_backend* h, uint32_t species, uint64_t* uniq, uint32_t* start, uint32_t cap,
+                             uint32_t* nCells) {
+    TSP_NEED(h);
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, {
+        Backend& b = *hh->b;
+        b.Sync();
+        const uint32_t cnt = species == 0 ? b.nF : species == 1 ? b.nB : b.nR;
+        uint64_t nc = 0;
+        if (cnt) CK(cudaMemcpy(&nc, b.nCellsDev.p + species, 8, cudaMemcpyDeviceToHost));
+        if (nCells) *nCells = (uint32_t)nc;
+        if (uniq && start) {
+            if (cap < nc) throw Error(TSP_ERR_INVALID, "capacity");
+            const uint64_t* u = species == 0 ? b.uniqF.p : species == 1 ? b.uniqB.p : b.uniqR.p;
+            const uint32_t* s = species == 0 ? b.startF.p : species == 1 ? b.startB.p : b.startR.p;
+            if (nc) {
+                CK(cudaMemcpy(uniq, u, nc * 8ull, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(start, s, (nc + 1) * 4ull, cudaMemcpyDeviceToHost));
+            }
+        }
+    });
+}
+int tsp_b200_read_sell32_meta(const tsp_backend* h, uint32_t list, uint16_t* counts, uint16_t* pitch, uint8_t* fmt,
+                              uint32_t* base, uint32_t* base2, uint64_t* offs, uint32_t nChunks, uint64_t* n16,
+                              uint64_t* n32) {
+    TSP_NEED(h);
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, {
+        Backend& b = *hh->b;
+        b.Sync();
+        if (list > 2) throw Error(TSP_ERR_INVALID, "not a SELL32 list");
+        Backend::Sell& m = b.sell[list];
+        if (n16) *n16 = m.n16;
+        if (n32) *n32 = m.n32;
+        const uint32_t nc = (b.nF + 31) / 32;
+        if (counts) {
+            if (nChunks != nc) throw Error(TSP_ERR_INVALID, "chunk count mismatch");
+            if (b.nF) CK(cudaMemcpy(counts, m.counts.p, b.nF * 2ull, cudaMemcpyDeviceToHost));
+            if (nc) {
+                CK(cudaMemcpy(pitch, m.pitch.p, nc * 2ull, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(fmt, m.format.p, nc, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(base, m.base.p, nc * 4ull, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(base2, m.base2.p, nc * 4ull, cudaMemcpyDeviceToHost));
+                CK(cudaMemcpy(offs, m.offset.p, nc * 8ull, cudaMemcpyDeviceToHost));
+            }
+        }
+    });
+}
+int tsp_b200_read_sell32_words(const tsp_backend* h, uint32_t list, uint16_t* w16, uint64_t n16, uint32_t* w32,
+                               uint64_t n32) {
+    TSP_NEED(h);
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, {
+        Backend& b = *hh->b;
+        b.Sync();
+        if (list > 2) throw Error(TSP_ERR_INVALID, "not a SELL32 list");
+        Backend::Sell& m = b.sell[list];
+        if (n16 != m.n16 || n32 != m.n32) throw Error(TSP_ERR_INVALID, "size mismatch");
+        if (n16) CK(cudaMemcpy(w16, m.l16.p, n16 * 2ull, cudaMemcpyDeviceToHost));
+        if (n32) CK(cudaMemcpy(w32, m.l32.p, n32 * 4ull, cudaMemcpyDeviceToHost));
+    });
+}
+int tsp_b200_read_rows(const tsp_backend* h, uint32_t list, uint64_t* offsets, uint32_t nSrc, uint32_t* indices,
+                       uint64_t cap, uint64_t* total) {
+    TSP_NEED(h);
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, {
+        Backend& b = *hh->b;
+        b.Sync();
+        if (list > 5) throw Error(TSP_ERR_INVALID, "unknown list");
+        if (list >= 3) {
+            const int k = (int)list - 3;
+            if (total) *total = b.csrN[k];
+            if (offsets) {
+                if (nSrc != b.nR) throw Error(TSP_ERR_INVALID, "size mismatch");
+                CK(cudaMemcpy(offsets, b.offR[k].p, (b.nR + 1ull) * 8ull, cudaMemcpyDeviceToHost));
+            }
+            if (indices && b.csrN[k]) {
+                if (cap < b.csrN[k]) throw Error(TSP_ERR_INVALID, "capacity");
+                CK(cudaMemcpy(indices, b.listR[k].p, b.csrN[k] * 4ull, cudaMemcpyDeviceToHost));
+            }
+            return TSP_OK;
+        }
+        std::vector<uint16_t> cnt(b.nF);
+        if (b.nF) CK(cudaMemcpy(cnt.data(), b.sell[list].counts.p, b.nF * 2ull, cudaMemcpyDeviceToHost));
+        std::vector<uint64_t> off(b.nF + 1ull, 0);
+        for (uint32_t i = 0; i < b.nF; i++) off[i + 1] = off[i] + cnt[i];
+        if (total) *total = off[b.nF];
+        if (offsets) {
+            if (nSrc != b.nF) throw Error(TSP_ERR_INVALID, "size mismatch");
+            std::memcpy(offsets, off.data(), off.size() * 8);
+        }
+        if (indices && off[b.nF]) {
+            if (cap < off[b.nF]) throw Error(TSP_ERR_INVALID, "capacity");
+            tsp::DBuf<uint64_t> dOff;
+            tsp::DBuf<uint32_t> dOut;
+            dOff.ensure(b.nF + 1ull);
+            dOut.ensure(off[b.nF]);
+            CK(cudaMemcpy(dOff.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice));
+            tsp::LaunchDecodeSellRows(b.Meta((int)list), b.nF, dOff.p, dOut.p, b.s);
+            b.Sync();
+            CK(cudaMemcpy(indices, dOut.p, off[b.nF] * 4ull, cudaMemcpyDeviceToHost));
+        }
+    });
+}
+int tsp_b200_run_stage(tsp_backend* h, const tsp_params* p, uint32_t stage, double* errSums) {
+    TSP_NEED(h);
+    if (!p) return TSP_ERR_INVALID;
+    TSP_GUARD(h, h->b->RunStage(*p, stage, errSums));
+}
+int tsp_b200_read_field(const tsp_backend* h, uint32_t field, void* out, uint32_t n) {
+    TSP_NEED(h);
+    if (!out && n) return TSP_ERR_INVALID;
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, hh->b->ReadField(field, out, n));
+}
+int tsp_b200_write_field(tsp_backend* h, uint32_t field, const void* in, uint32_t n) {
+    TSP_NEED(h);
+    if (!in && n) return TSP_ERR_INVALID;
+    TSP_GUARD(h, h->b->WriteField(field, in, n));
+}
+
+int tsp_b200_time_stage(tsp_backend* h, const tsp_params* p, uint32_t stage, uint32_t reps, float* ms) {
+    TSP_NEED(h);
+    if (!p || !ms) return TSP_ERR_INVALID;
+    TSP_GUARD(h, *ms = h->b->TimeStage(*p, stage, reps));
+}
+int tsp_b200_get_stream(const tsp_backend* h, void** stream) {
+    TSP_NEED(h);
+    if (!stream) return TSP_ERR_INVALID;
+    *stream = (void*)h->b->s;
+    return TSP_OK;
+}
+int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count) {
+    TSP_NEED(h);
+    if (!count) return TSP_ERR_INVALID;
+    *count = h->b->launches;
+    return TSP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,199 @@
+// kernels.h -- host-side launch interface of the CUDA kernels (one declaration per launcher).
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace tsp {
+
+struct U64x2;
+
+constexpr uint32_t QUERY_THREADS = 128;  // 4 warps = 4 SELL32 chunks per block
+constexpr uint32_t MAX_JACOBI_SWEEPS = 100000;  // hard bound of the device-driven Jacobi loop
+
+// window of the Delta16x2 home group around a chunk (neighbor_search_kernels.cu:86-97)
+__host__ __device__ __forceinline__ void HomeWindow(uint32_t chunk, uint32_t& lo, uint32_t& hi) {
+    constexpr uint32_t reach = (0x8000u - SELL_W) / 2u;
+    constexpr uint32_t hiOff = SELL_W - 1u + reach;
+    const uint32_t b = chunk * SELL_W;
+    lo = (b > reach) ? (b - reach) : 0u;
+    hi = (b < 0xffffffffu - hiOff) ? (b + hiOff) : 0xffffffffu;
+}
+
+struct DomainBox {
+    float mn[3], mx[3];
+    int bounded;
+};
+
+struct ProbeResult {
+    int mnKey[3], mxKey[3];   // order-preserving integer images of the float bounds
+    uint32_t exceeded;
+    uint32_t pad;
+};
+float OrderedIntToFloat(int k);
+
+struct SortScratch {
+    uint64_t* keysA;
+    uint64_t* keysB;
+    uint32_t* valsA;
+    uint32_t* valsB;
+    uint32_t* tileHist;
+    uint32_t* digitTotals;
+};
+
+struct QueryArgs {
+    const float4* posF;
+    const uint64_t* cidF;
+    uint32_t nF;
+    const float4* posB;
+    uint32_t nB;
+    const float4* posR;
+    const uint32_t* permR;
+    const uint32_t* bodyR;
+    uint32_t nR;
+    const uint32_t *startF, *startB, *startR;
+    const uint32_t *gridF, *gridB, *gridR;  // NULL when the species is absent
+    Frame fr;
+    float r2;
+    uint32_t cap;
+    uint32_t* err;
+};
+
+struct RigidLists {
+    uint16_t *cntRF, *cntRB, *cntRR;
+    uint64_t *offRF, *offRB, *offRR;
+    uint32_t *listRF, *listRB, *listRR;
+};
+
+// solver iteration state kept on the device across the Jacobi loop
+struct SolverState {
+    double partial[3];        // unused padding for alignment of sums
+    double sums[3];           // FP64 raw / pos / abs of the last sweep
+    uint32_t iters;           // N_solverIters_ (sph_solver.cpp:208)
+    uint32_t done;
+    float avg[3];             // avgRelDensityErrorF_{raw,pos,abs}
+    uint32_t ticket;          // last-block-done counter of the reduction
+    uint32_t itersTotal;      // sweeps since pull (statistics)
+};
+
+struct SolverControl {
+    uint32_t minIters, maxIters, fixedIters, cond;
+    float target;
+    uint32_t nF;
+};
+
+// fluid SoA on the device (Morton order)
+struct FluidDev {
+    float4* posP;     // x, y, z, pressure
+    float4* velRho;   // vx, vy, vz, density
+    float4* velPred;  // vx*, vy*, vz*, -
+    float4* acc;      // a^p x, y, z, -
+    float2* srcDiag;  // source term, diagonal a_ii
+    uint32_t n;
+};
+struct BoundaryDev {
+    const float4* pos;  // x, y, z, psi
+    const float* vol;
+    uint32_t n;
+};
+struct RigidDev {
+    const float4* pos;      // world x, y, z, psi
+    const float4* vel;      // vx, vy, vz, vol
+    const float4* velPred;  // predicted particle velocities
+    uint32_t n;
+};
+struct SellView {
+    const uint16_t* counts;
+    const uint16_t* pitch;
+    const uint8_t* format;
+    const uint32_t* base;
+    const uint32_t* base2;
+    const uint64_t* offset;
+    const uint16_t* list16;
+    const uint32_t* list32;
+};
+struct NeighborView {
+    SellView ff, fb, fr;
+};
+
+// ---- ns_kernels.cu
+void LaunchProbe(const float4* pos, uint32_t n, const Frame& fr, bool frameValid, const DomainBox& dom,
+                 ProbeResult* out, cudaStream_t s);
+void SortByCell(const float4* pos, uint32_t n, const Frame& fr, SortScratch& sc, uint32_t* perm, uint64_t* cidSorted,
+                cudaStream_t s);
+void LaunchCellIds(const float4* pos, uint32_t n, const Frame& fr, uint64_t* cid, cudaStream_t s);
+void GatherF4(const uint32_t* perm, const float4* src, float4* dst, uint32_t n, cudaStream_t s);
+void GatherF2(const uint32_t* perm, const float2* src, float2* dst, uint32_t n, cudaStream_t s);
+void GatherF1(const uint32_t* perm, const float* src, float* dst, uint32_t n, cudaStream_t s);
+void GatherU64(const uint32_t* perm, const uint64_t* src, uint64_t* dst, uint32_t n, cudaStream_t s);
+void LaunchReorderFluidStep(const uint32_t* perm, const float4* posIn, const float4* velIn, const uint64_t* idIn,
+                            float4* posOut, float4* velOut, uint64_t* idOut, uint32_t n, cudaStream_t s);
+void BuildCellTable(const uint64_t* cidSorted, uint32_t n, uint64_t* unique, uint32_t* start, uint64_t* nCellsDev,
+                    uint64_t* scanScratch, cudaStream_t s);
+void BuildGrid(const uint64_t* unique, const uint64_t* nCellsDev, uint32_t nMax, const Frame& fr, uint32_t* grid,
+               uint64_t gridCells, cudaStream_t s);
+uint32_t QueryCap(uint32_t reach);
+void LaunchQueryFluid(bool fill, const QueryArgs& a, const SellMeta& ff, const SellMeta& fb, const SellMeta& fr,
+                      cudaStream_t s);
+void LaunchQueryRigid(bool fill, const QueryArgs& a, const RigidLists& L, cudaStream_t s);
+void FinalizeSell(const SellMeta& m, uint32_t nChunks, U64x2* scratch, U64x2* totals, cudaStream_t s);
+void FinalizeCsr(const uint16_t* counts, uint64_t* off, uint32_t n, uint64_t* scratch, uint64_t* total, cudaStream_t s);
+void LaunchDecodeSellRows(const SellMeta& m, uint32_t nF, const uint64_t* rowOff, uint32_t* out, cudaStream_t s);
+
+// ---- sph_kernels.cu
+void LaunchDensity(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
+                   cudaStream_t s);
+void LaunchNonPressure(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
+                       const NeighborView& nv, cudaStream_t s);
+void LaunchSourceDiagInit(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
+                          const NeighborView& nv, SolverState* st, cudaStream_t s);
+void LaunchPressureAcc(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
+                       const NeighborView& nv, cudaStream_t s);
+// one relaxed Jacobi sweep with the FP64 error reduction; the last block applies the
+// termination rule and, when `cond` is non-zero, sets the graph's loop condition
+void LaunchJacobi(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
+                  const SolverControl& ctl, SolverState* st, double* partials, unsigned long long cond,
+                  bool hasCond, cudaStream_t s);
+uint32_t JacobiBlocks(uint32_t nF);
+void LaunchIntegration(const Consts& c, const FluidDev& f, cudaStream_t s);
+void LaunchBoundaryVolumes(const Consts& c, const float4* posB, uint32_t nB, const uint32_t* startB,
+                           const uint32_t* gridB, const Frame& fr, float defaultVol, float defaultPsi, float restDensity,
+                           float* volOut, float* psiOut, cudaStream_t s);
+void LaunchSolverReset(SolverState* st, uint32_t nF, cudaStream_t s);
+
+// ---- rigid_kernels.cu
+struct BodyDev {
+    double* state;       // per body: 32 doubles (see rigid_kernels.cu)
+    double* forceTorque; // per body: 6 doubles
+    uint32_t n;
+};
+struct RigidParticlesDev {
+    const uint32_t* body;
+    const float4* rel;   // body-frame x, y, z, vol
+    float4* pos;         // world x, y, z, psi
+    float4* vel;         // x, y, z, vol
+    float4* velPred;
+    float4* force;       // x, y, z, -
+    uint32_t n;
+    const uint32_t* byBodyOff;
+    const uint32_t* byBodyIdx;
+};
+void LaunchRigidUpdateParticles(const RigidParticlesDev& r, const BodyDev& b, bool predicted, uint32_t* err,
+                                cudaStream_t s);
+void LaunchRigidClearAddGravity(const BodyDev& b, float gx, float gy, float gz, cudaStream_t s);
+void LaunchRigidViscousForces(const Consts& c, const RigidParticlesDev& r, const FluidDev& f, const uint64_t* offRF,
+                              const uint32_t* listRF, cudaStream_t s);
+void LaunchRigidPressureForces(const Consts& c, const RigidParticlesDev& r, const FluidDev& f, const uint64_t* offRF,
+                               const uint32_t* listRF, cudaStream_t s);
+void LaunchRigidReduce(const RigidParticlesDev& r, const BodyDev& b, cudaStream_t s);
+void LaunchRigidPredict(const BodyDev& b, float dt, cudaStream_t s);
+void LaunchRigidIntegrate(const BodyDev& b, float dt, uint32_t* err, cudaStream_t s);
+void LaunchRigidVolumes(const Consts& c, const float4* rel, const uint32_t* byBodyOff, const uint32_t* byBodyIdx,
+                        uint32_t nBodies, uint32_t nR, float defaultVol, float defaultPsi, float restDensity,
+                        float* volOut, float* psiOut, cudaStream_t s);
+
+}  // namespace tsp

@@ -1,0 +1,495 @@
+// sph_kernels.cu -- IISPH solver kernels over SELL32 neighbor lists.
+//
+// One warp per SELL32 chunk, lane = fluid particle: slot k of all 32 lanes is one coalesced
+// 64 B (Delta16x2) or 128 B (Abs32) load, the loop bound (chunk pitch) is warp-uniform and
+// slots past a lane's own count are predicated off. Neighbor attributes are gathered as
+// float4 (position + pressure, velocity + density), one 16 B load per neighbor.
+//
+// Arithmetic: compiled with -fmad=false; each per-pair term and each accumulation follows
+// the operation order of the reference CPU kernels (source/simulation/CPU/backend/
+// sph_solver.cpp:734-2089) with explicit fmaf where the reference uses fma, and the FF, FB
+// and FR partial sums are kept apart and combined exactly as the reference combines them.
+#include "kernels.h"
+
+namespace tsp {
+
+constexpr uint32_t SPH_THREADS = 256;
+
+struct ChunkCursor {
+    uint32_t pitch, cnt, base, base2;
+    uint64_t off;
+    uint8_t fmt;
+    __device__ __forceinline__ void load(const SellView& v, uint32_t chunk, uint32_t i, bool act) {
+        pitch = v.pitch[chunk]; fmt = v.format[chunk]; base = v.base[chunk]; base2 = v.base2[chunk];
+        off = v.offset[chunk];
+        cnt = act ? v.counts[i] : 0u;
+    }
+    __device__ __forceinline__ uint32_t nbr(const SellView& v, uint32_t k, uint32_t lane) const {
+        return SellNeighbor(fmt, base, base2, off, k, lane, v.list16, v.list32);
+    }
+};
+
+// ----------------------------------------------------------------------------- density
+__global__ void __launch_bounds__(SPH_THREADS) KDensity(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv) {
+    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
+    const uint32_t chunk = i >> 5, lane = i & 31;
+    if (chunk * SELL_W >= f.n) return;
+    const bool act = i < f.n;
+    const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float dF = 0.f, dB = 0.f, dR = 0.f;
+    ChunkCursor cur;
+    cur.load(nv.ff, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const float4 pj = f.posP[cur.nbr(nv.ff, k, lane)];
+            dF = fmaf(c.massF, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dF);
+        }
+    }
+    cur.load(nv.fb, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const float4 pj = b.pos[cur.nbr(nv.fb, k, lane)];
+            dB = fmaf(pj.w, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dB);
+        }
+    }
+    cur.load(nv.fr, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const float4 pj = r.pos[cur.nbr(nv.fr, k, lane)];
+            dR = fmaf(pj.w, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dR);
+        }
+    }
+    if (act) reinterpret_cast<float*>(f.velRho)[4ull * i + 3] = dF + dB + dR;
+}
+
+// ----------------------------------------------------------------------------- non-pressure
+__global__ void __launch_bounds__(SPH_THREADS) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+                                                         NeighborView nv) {
+    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
+    const uint32_t chunk = i >> 5, lane = i & 31;
+    if (chunk * SELL_W >= f.n) return;
+    const bool act = i < f.n;
+    const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 vi = act ? f.velRho[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float fx = 0.f, fy = 0.f, fz = 0.f, bx = 0.f, by = 0.f, bz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
+    ChunkCursor cur;
+    cur.load(nv.ff, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const uint32_t j = cur.nbr(nv.ff, k, lane);
+            const float4 pj = f.posP[j];
+            const float4 vj = f.velRho[j];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float kg = GradFactor(d2, c);
+            const float dot = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
+            const float rhoJ = fmaxf(vj.w, 1e-7f);
+            const float a = (c.massF * dot) / (rhoJ * (d2 + c.hEps)) * kg;
+            fx = fmaf(a, dx, fx); fy = fmaf(a, dy, fy); fz = fmaf(a, dz, fz);
+        }
+    }
+    cur.load(nv.fb, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const uint32_t j = cur.nbr(nv.fb, k, lane);
+            const float4 pj = b.pos[j];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+            const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+            const float dvx = vi.x - 0.0f, dvy = vi.y - 0.0f, dvz = vi.z - 0.0f;
+            const float dot = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float a = (b.vol[j] * dot) / (d2 + c.hEps);
+            bx = fmaf(a, gx, bx); by = fmaf(a, gy, by); bz = fmaf(a, gz, bz);
+        }
+    }
+    cur.load(nv.fr, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const uint32_t j = cur.nbr(nv.fr, k, lane);
+            const float4 pj = r.pos[j];
+            const float4 vj = r.vel[j];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+            const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+            const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+            const float dot = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float a = (vj.w * dot) / (d2 + c.hEps);
+            rx = fmaf(a, gx, rx); ry = fmaf(a, gy, ry); rz = fmaf(a, gz, rz);
+        }
+    }
+    if (!act) return;
+    const float ax = fx * c.visFacF + (bx + rx) * c.visFacB + c.gx;
+    const float ay = fy * c.visFacF + (by + ry) * c.visFacB + c.gy;
+    const float az = fz * c.visFacF + (bz + rz) * c.visFacB + c.gz;
+    f.velPred[i] = make_float4(fmaf(ax, c.dt, vi.x), fmaf(ay, c.dt, vi.y), fmaf(az, c.dt, vi.z), 0.0f);
+}
+
+// ----------------------------------------------------------------------------- source / diagonal / init
+__global__ void __launch_bounds__(SPH_THREADS) KSourceDiagInit(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+                                                            NeighborView nv) {
+    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
+    const uint32_t chunk = i >> 5, lane = i & 31;
+    if (chunk * SELL_W >= f.n) return;
+    const bool act = i < f.n;
+    const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 vi = act ? f.velPred[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float sF = 0.f, sB = 0.f, sR = 0.f, cxF = 0.f, cyF = 0.f, czF = 0.f, g2 = 0.f;
+    float cxB = 0.f, cyB = 0.f, czB = 0.f, cxR = 0.f, cyR = 0.f, czR = 0.f;
+    ChunkCursor cur;
+    cur.load(nv.ff, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const uint32_t j = cur.nbr(nv.ff, k, lane);
+            const float4 pj = f.posP[j];
+            const float4 vj = f.velPred[j];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float kg = GradFactor(d2, c);
+            const float st = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
+            sF = fmaf(kg, st, sF);
+            cxF = fmaf(kg, dx, cxF); cyF = fmaf(kg, dy, cyF); czF = fmaf(kg, dz, czF);
+            g2 = fmaf(kg, kg * d2, g2);  // (kgFac * distSqu first keeps the self pair exactly zero)
+        }
+    }
+    cur.load(nv.fb, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const float4 pj = b.pos[cur.nbr(nv.fb, k, lane)];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+            const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+            const float dvx = vi.x - 0.0f, dvy = vi.y - 0.0f, dvz = vi.z - 0.0f;
+            const float st = fmaf(dvx, gx, fmaf(dvy, gy, dvz * gz));
+            sB = fmaf(pj.w, st, sB);
+            cxB = fmaf(pj.w, gx, cxB); cyB = fmaf(pj.w, gy, cyB); czB = fmaf(pj.w, gz, czB);
+        }
+    }
+    cur.load(nv.fr, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const uint32_t j = cur.nbr(nv.fr, k, lane);
+            const float4 pj = r.pos[j];
+            const float4 vj = r.velPred[j];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+            const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+            const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
+            const float st = fmaf(dvx, gx, fmaf(dvy, gy, dvz * gz));
+            sR = fmaf(pj.w, st, sR);
+            cxR = fmaf(pj.w, gx, cxR); cyR = fmaf(pj.w, gy, cyR); czR = fmaf(pj.w, gz, czR);
+        }
+    }
+    if (!act) return;
+    sF *= c.massF;
+    const float rho = f.velRho[i].w;
+    const float src = c.restDensity - rho - c.dt * (sF + sB + sR);
+    const float cx = cxF * c.cTermFacF + (cxB + cxR) * c.cTermFacB;
+    const float cy = cyF * c.cTermFacF + (cyB + cyR) * c.cTermFacB;
+    const float cz = czF * c.cTermFacF + (czB + czR) * c.cTermFacB;
+    const float dA = c.massF * fmaf(cx, cxF, fmaf(cy, cyF, cz * czF));
+    const float dB = c.massF * c.diagBFac * g2;
+    const float dC = fmaf(cx, cxB + cxR, fmaf(cy, cyB + cyR, cz * (czB + czR)));
+    const float diag = c.dt2 * (dA + dB + dC);
+    const bool valid = fabsf(diag) > 1e-7f;
+    const float cold = c.omega * (src / diag);
+    const float prev = c.warm ? pi.w : 0.0f;
+    const float init = c.warm ? ((prev > 0.0f) ? c.warmStart * prev : cold) : cold;
+    f.srcDiag[i] = make_float2(src, diag);
+    reinterpret_cast<float*>(f.posP)[4ull * i + 3] = fmaxf(0.0f, valid ? init : 0.0f);
+}
+
+// ----------------------------------------------------------------------------- pressure acceleration
+__global__ void __launch_bounds__(SPH_THREADS) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+                                                         NeighborView nv) {
+    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
+    const uint32_t chunk = i >> 5, lane = i & 31;
+    if (chunk * SELL_W >= f.n) return;
+    const bool act = i < f.n;
+    const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float fOuter = c.massF * pi.w * c.densInvSqu;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    ChunkCursor cur;
+    cur.load(nv.ff, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const float4 pj = f.posP[cur.nbr(nv.ff, k, lane)];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+            const float a = (fOuter + c.massF * pj.w * c.densInvSqu) * kg;
+            ax = fmaf(a, dx, ax); ay = fmaf(a, dy, ay); az = fmaf(a, dz, az);
+        }
+    }
+    cur.load(nv.fb, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const float4 pj = b.pos[cur.nbr(nv.fb, k, lane)];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+            const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+            const float a = c.accCoeffB * pj.w * pi.w;
+            ax = fmaf(a, gx, ax); ay = fmaf(a, gy, ay); az = fmaf(a, gz, az);
+        }
+    }
+    cur.load(nv.fr, chunk, i, act);
+    for (uint32_t k = 0; k < cur.pitch; k++) {
+        if (k < cur.cnt) {
+            const float4 pj = r.pos[cur.nbr(nv.fr, k, lane)];
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+            const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+            const float a = c.accCoeffB * pj.w * pi.w;
+            ax = fmaf(a, gx, ax); ay = fmaf(a, gy, ay); az = fmaf(a, gz, az);
+        }
+    }
+    if (act) f.acc[i] = make_float4(0.0f - ax, 0.0f - ay, 0.0f - az, 0.0f);
+}
+
+// ----------------------------------------------------------------------------- relaxed Jacobi sweep
+__device__ __forceinline__ bool Terminated(const SolverControl& ctl, uint32_t iters, const float* avg) {
+    // TerminationConditionSatisfied (sph_solver.cpp:686-732)
+    if (iters < ctl.minIters) return false;
+    if (iters >= ctl.maxIters) return true;
+    switch (ctl.cond) {
+        case 0: return iters >= ctl.fixedIters;
+        case 1: return avg[0] <= ctl.target;
+        case 2: return avg[1] <= ctl.target;
+        case 3: return avg[2] <= ctl.target;
+        default: return iters >= 3;
+    }
+}
+
+__global__ void __launch_bounds__(SPH_THREADS) KJacobi(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv,
+                                                    SolverControl ctl, SolverState* st, double* partials,
+                                                    cudaGraphConditionalHandle cond, int hasCond) {
+    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
+    const uint32_t chunk = i >> 5, lane = i & 31;
+    const bool act = i < f.n;
+    double eRaw = 0.0, ePos = 0.0, eAbs = 0.0;
+    if (chunk * SELL_W < f.n) {
+        const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 ai = act ? f.acc[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float sF = 0.f, sB = 0.f;
+        ChunkCursor cur;
+        cur.load(nv.ff, chunk, i, act);
+        for (uint32_t k = 0; k < cur.pitch; k++) {
+            if (k < cur.cnt) {
+                const uint32_t j = cur.nbr(nv.ff, k, lane);
+                const float4 pj = f.posP[j];
+                const float4 aj = f.acc[j];
+                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+                const float dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
+                const float sv = fmaf(dax, dx, fmaf(day, dy, daz * dz));
+                sF = fmaf(kg, sv, sF);
+            }
+        }
+        sF *= c.massF;
+        cur.load(nv.fb, chunk, i, act);
+        for (uint32_t k = 0; k < cur.pitch; k++) {
+            if (k < cur.cnt) {
+                const float4 pj = b.pos[cur.nbr(nv.fb, k, lane)];
+                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+                const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+                const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
+                sB = sB + pj.w * sv;
+            }
+        }
+        cur.load(nv.fr, chunk, i, act);
+        for (uint32_t k = 0; k < cur.pitch; k++) {
+            if (k < cur.cnt) {
+                const float4 pj = r.pos[cur.nbr(nv.fr, k, lane)];
+                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+                const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+                const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+                const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
+                sB = sB + pj.w * sv;
+            }
+        }
+        if (act) {
+            const float2 sd = f.srcDiag[i];
+            const float sys = c.dt2 * (sF + sB);
+            const float resid = sd.x - sys;
+            const float err = sys - sd.x;
+            const bool valid = fabsf(sd.y) > 1e-7f;
+            const float pn = fmaxf(0.0f, valid ? fmaf(c.omega, resid / sd.y, pi.w) : 0.0f);
+            reinterpret_cast<float*>(f.posP)[4ull * i + 3] = pn;
+            if (valid) {
+                const double re = (double)(err / c.restDensity);
+                eRaw = re;
+                ePos = re > 0.0 ? re : 0.0;
+                eAbs = fabs(re);
+            }
+        }
+    }
+    // FP64 block reduction (fixed order), last block folds the partials in fixed order
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        eRaw += __shfl_xor_sync(0xffffffffu, eRaw, d);
+        ePos += __shfl_xor_sync(0xffffffffu, ePos, d);
+        eAbs += __shfl_xor_sync(0xffffffffu, eAbs, d);
+    }
+    __shared__ double ws[3][SPH_THREADS / 32];
+    __shared__ bool amLast;
+    const uint32_t warp = threadIdx.x >> 5;
+    if (lane == 0) { ws[0][warp] = eRaw; ws[1][warp] = ePos; ws[2][warp] = eAbs; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (int w = 0; w < SPH_THREADS / 32; w++) { s0 += ws[0][w]; s1 += ws[1][w]; s2 += ws[2][w]; }
+        partials[3ull * blockIdx.x + 0] = s0;
+        partials[3ull * blockIdx.x + 1] = s1;
+        partials[3ull * blockIdx.x + 2] = s2;
+        __threadfence();
+        const uint32_t t = atomicAdd(&st->ticket, 1u);
+        amLast = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!amLast) return;
+    __threadfence();
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (uint32_t p = threadIdx.x; p < gridDim.x; p += SPH_THREADS) {
+        s0 += __ldcg(partials + 3ull * p + 0);
+        s1 += __ldcg(partials + 3ull * p + 1);
+        s2 += __ldcg(partials + 3ull * p + 2);
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, d);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, d);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, d);
+    }
+    __syncthreads();
+    if (lane == 0) { ws[0][warp] = s0; ws[1][warp] = s1; ws[2][warp] = s2; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+    for (int w = 0; w < SPH_THREADS / 32; w++) { t0 += ws[0][w]; t1 += ws[1][w]; t2 += ws[2][w]; }
+    st->sums[0] = t0; st->sums[1] = t1; st->sums[2] = t2;
+    st->ticket = 0;
+    // loop bookkeeping of Step_IISPH (sph_solver.cpp:213-261)
+    const uint32_t iters = st->iters + 1;
+    st->iters = iters;
+    st->itersTotal += 1;
+    float avg[3] = {st->avg[0], st->avg[1], st->avg[2]};
+    const bool compute = iters >= ctl.minIters && (ctl.cond != 0 || Terminated(ctl, iters, avg));
+    if (compute) {
+        avg[0] = (float)t0 / (float)ctl.nF;
+        avg[1] = (float)t1 / (float)ctl.nF;
+        avg[2] = (float)t2 / (float)ctl.nF;
+        st->avg[0] = avg[0]; st->avg[1] = avg[1]; st->avg[2] = avg[2];
+    }
+    // the loop always ends: maxIters is validated on the host, MAX_JACOBI_SWEEPS bounds it anyway
+    const bool done = Terminated(ctl, iters, avg) || iters >= MAX_JACOBI_SWEEPS;
+    st->done = done ? 1u : 0u;
+    if (hasCond) cudaGraphSetConditional(cond, done ? 0u : 1u);
+}
+
+__global__ void KSolverReset(SolverState* st, uint32_t nF) {
+    st->iters = nF > 0 ? 1u : 0u;
+    st->avg[0] = st->avg[1] = st->avg[2] = 0.0f;
+    st->sums[0] = st->sums[1] = st->sums[2] = 0.0;
+    st->done = 0;
+    st->ticket = 0;
+}
+
+// ----------------------------------------------------------------------------- integration
+__global__ void __launch_bounds__(256) KIntegration(Consts c, FluidDev f) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= f.n) return;
+    const float4 vp = f.velPred[i];
+    const float4 a = f.acc[i];
+    const float4 p = f.posP[i];
+    const float4 v = f.velRho[i];
+    const float vx = fmaf(c.dt, a.x, vp.x), vy = fmaf(c.dt, a.y, vp.y), vz = fmaf(c.dt, a.z, vp.z);
+    f.velRho[i] = make_float4(vx, vy, vz, v.w);
+    f.posP[i] = make_float4(fmaf(c.dt, vx, p.x), fmaf(c.dt, vy, p.y), fmaf(c.dt, vz, p.z), p.w);
+}
+
+// ----------------------------------------------------------------------------- boundary volumes
+// ComputeParticleCoefficients (source/simulation/scene/builder.cpp:174-376): the reference
+// walks, per particle, the (2 reach + 1)^2 rows of cells in z, y order with the cells of a
+// row in ascending x and the particles of a cell in their (stable) order. The dense Morton
+// grid visits exactly those cells in exactly that order, so the FP32 sums are the reference's.
+__global__ void __launch_bounds__(256) KBoundaryVolumes(Consts c, const float4* __restrict__ pos, uint32_t n,
+                                                      const uint32_t* __restrict__ start,
+                                                      const uint32_t* __restrict__ grid, Frame fr, float defVol,
+                                                      float defPsi, float rho0, float* __restrict__ vol,
+                                                      float* __restrict__ psi) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos[i];
+    const int cx = FloorToInt(p.x * fr.cellSizeInv) - fr.ox, cy = FloorToInt(p.y * fr.cellSizeInv) - fr.oy,
+              cz = FloorToInt(p.z * fr.cellSizeInv) - fr.oz;
+    const int r = (int)fr.reach;
+    float sum = 0.0f;
+    for (int oz = cz - r; oz <= cz + r; oz++) {
+        if (oz < 0 || oz >= (int)fr.nz) continue;
+        for (int oy = cy - r; oy <= cy + r; oy++) {
+            if (oy < 0 || oy >= (int)fr.ny) continue;
+            for (int ox = cx - r; ox <= cx + r; ox++) {
+                if (ox < 0 || ox >= (int)fr.nx) continue;
+                const uint32_t cc = grid[(uint64_t)ox + (uint64_t)fr.nx * ((uint64_t)oy + (uint64_t)fr.ny * oz)];
+                if (cc == EMPTY_32) continue;
+                for (uint32_t j = start[cc]; j < start[cc + 1]; j++) {
+                    const float4 q = pos[j];
+                    sum += BoundaryWeight(p.x - q.x, p.y - q.y, p.z - q.z, c);
+                }
+            }
+        }
+    }
+    if (sum > 0.0f && isfinite(sum)) {
+        const float v = 1.0f / sum;
+        vol[i] = v;
+        psi[i] = rho0 * v;
+    } else {
+        vol[i] = defVol;
+        psi[i] = defPsi;
+    }
+}
+
+// ----------------------------------------------------------------------------- launchers
+static inline uint32_t SphBlocks(uint32_t n) { return (n + SPH_THREADS - 1) / SPH_THREADS; }
+uint32_t JacobiBlocks(uint32_t nF) { return SphBlocks(nF); }
+
+void LaunchDensity(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
+                   cudaStream_t s) {
+    if (f.n) KDensity<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+}
+void LaunchNonPressure(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
+                       const NeighborView& nv, cudaStream_t s) {
+    if (f.n) KNonPressure<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+}
+void LaunchSourceDiagInit(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
+                          const NeighborView& nv, SolverState* st, cudaStream_t s) {
+    if (f.n) KSourceDiagInit<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+    KSolverReset<<<1, 1, 0, s>>>(st, f.n);
+}
+void LaunchSolverReset(SolverState* st, uint32_t nF, cudaStream_t s) { KSolverReset<<<1, 1, 0, s>>>(st, nF); }
+void LaunchPressureAcc(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
+                       const NeighborView& nv, cudaStream_t s) {
+    if (f.n) KPressureAcc<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+}
+void LaunchJacobi(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
+                  const SolverControl& ctl, SolverState* st, double* partials, unsigned long long cond, bool hasCond,
+                  cudaStream_t s) {
+    if (f.n)
+        KJacobi<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv, ctl, st, partials,
+                                                      (cudaGraphConditionalHandle)cond, hasCond ? 1 : 0);
+}
+void LaunchIntegration(const Consts& c, const FluidDev& f, cudaStream_t s) {
+    if (f.n) KIntegration<<<(f.n + 255) / 256, 256, 0, s>>>(c, f);
+}
+void LaunchBoundaryVolumes(const Consts& c, const float4* posB, uint32_t nB, const uint32_t* startB,
+                           const uint32_t* gridB, const Frame& fr, float defaultVol, float defaultPsi, float restDensity,
+                           float* volOut, float* psiOut, cudaStream_t s) {
+    if (nB)
+        KBoundaryVolumes<<<(nB + 255) / 256, 256, 0, s>>>(c, posB, nB, startB, gridB, fr, defaultVol, defaultPsi,
+                                                          restDensity, volOut, psiOut);
+}
+
+}  // namespace tsp
