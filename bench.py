@@ -36,38 +36,12 @@ METRIC = "particle-updates/s @1M (plain vs served batch, same B200); p50/p99 ste
 UNIT = "particle-updates/s"
 
 
-def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+from turbospharticles_b200.replicas import (dist_env, init as init_dist_group, barrier, max_over_ranks,
+                                            aggregate_rate, replica_seed)
 
 
 def init_dist(ws, backend):
-    if ws <= 1:
-        return None
-    import datetime
-    import torch.distributed as dist
-    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
-    return dist
-
-
-def max_over_ranks(dist, v, device=None):
-    if dist is None:
-        return v
-    import torch
-    t = torch.tensor([v], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def barrier(dist, device=None):
-    if dist is not None:
-        import torch
-        if device is not None:
-            dist.all_reduce(torch.zeros(1, device=device))
-        else:
-            dist.barrier()
+    return init_dist_group(backend, ws)
 
 
 class ClockSampler:
@@ -134,9 +108,9 @@ def profiled_traffic():
         return None
 
 
-def build_workload():
+def build_workload(rank=0):
     from turbospharticles_b200 import scene as S
-    st, dmin, dmax, p = S.dam_1m(seed=42)
+    st, dmin, dmax, p = S.dam_1m(seed=replica_seed(42, rank))
     return st, dmin, dmax, p
 
 
@@ -163,7 +137,7 @@ def run_b200(args):
     torch.cuda.set_device(local)
     dist = init_dist(ws, "nccl")
     dev = torch.device("cuda", local)
-    st, dmin, dmax, p = build_workload()
+    st, dmin, dmax, p = build_workload(rank)
     be = SimBackendB200(p, device=local)
     be.set_sim_domain_bounds(dmin, dmax)
     be.pull(st, p)
@@ -191,8 +165,7 @@ def run_b200(args):
     elapsed_ms = max_over_ranks(dist, e0.elapsed_time(e1), dev)
     launches = be.launch_count() - l0
     nF = st.N_F
-    total_updates = nF * args.steps * ws
-    value = total_updates / (elapsed_ms / 1e3)
+    value = aggregate_rate(nF * args.steps, ws, elapsed_ms)
     sweeps = int(np.sum(iters))
     # ---- roofline of the dominant kernel: the relaxed-Jacobi sweep (KJacobi)
     s = be.stats()

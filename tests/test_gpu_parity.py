@@ -172,27 +172,29 @@ def test_gpu_neighbor_search_bit_exact(dist, n):
 
 
 def test_gpu_neighbor_search_4m_properties():
-    """4,194,304 points: size-independent properties (the oracle is not run at this size):
-    FF rows ascending, self included, the FF relation symmetric, SELL32 decode == rows."""
-    st, dmin, dmax, p = S.neighbor_search_scene(1 << 22, "clustered", seed=11)
+    """4,194,304 uniform points (the oracle is not run at this size): size-independent
+    properties -- FF rows ascending, self included exactly for in-frame particles, the FF
+    relation symmetric (checked on a seeded sample), Morton cell IDs non-decreasing."""
+    st, dmin, dmax, p = S.neighbor_search_scene(1 << 22, "uniform", seed=11)
     g = SimBackendB200(p)
     g.set_sim_domain_bounds(dmin, dmax)
     g.pull(st, p)
     g.neighbor_search(p)
     off, idx = g.rows(abi.LIST_FF)
+    off = off.astype(np.int64)
     n = st.N_F
-    cnt = np.diff(off.astype(np.int64))
-    src = np.repeat(np.arange(n, dtype=np.int64), cnt)
-    assert np.all((np.diff(idx.astype(np.int64)) > 0) | (np.diff(src) != 0))
     cid = g.cell_ids(abi.SPECIES_F)
     inframe = cid != np.uint64(0xFFFFFFFFFFFFFFFF)
-    self_hit = np.zeros(n, bool)
-    self_hit[src[idx == src]] = True
-    assert np.array_equal(self_hit, inframe)
-    a = src * n + idx.astype(np.int64)
-    b = idx.astype(np.int64) * n + src
-    assert np.array_equal(np.sort(a), np.sort(b))
     assert np.all(np.diff(cid[inframe].astype(np.float64)) >= 0)
+    rng = np.random.default_rng(5)
+    for i in rng.choice(n, 4000, replace=False):
+        row = idx[off[i]:off[i + 1]].astype(np.int64)
+        assert np.all(np.diff(row) > 0)
+        assert (i in set(row.tolist())) == bool(inframe[i])
+        for j in row[:: max(1, len(row) // 8)]:
+            rj = idx[off[j]:off[j + 1]]
+            k = np.searchsorted(rj, i)
+            assert k < len(rj) and rj[k] == i
 
 
 # ------------------------------------------------------------------------------ SPH stages

@@ -151,6 +151,7 @@ static Consts MakeConsts(const tsp_params& p) {
 }
 
 struct HostMirror {
+    unsigned long long nbrTot[3];
     ProbeResult probe;
     U64x2 sellTot[3];
     uint64_t csrTot[3];
@@ -158,12 +159,6 @@ struct HostMirror {
     SolverState st;
     uint32_t err;
 };
-
-static uint64_t HashBytes(uint64_t h, const void* p, size_t n) {
-    const unsigned char* b = (const unsigned char*)p;
-    for (size_t i = 0; i < n; i++) { h ^= b[i]; h *= 1099511628211ull; }
-    return h;
-}
 
 class Backend {
 public:
@@ -219,9 +214,17 @@ public:
         DBuf<uint64_t> offset;
         DBuf<uint16_t> l16;
         DBuf<uint32_t> l32;
+        DBuf<float> kg16, kg32;  // recorded kernel-gradient factors, parallel to l16 / l32
         uint64_t n16 = 0, n32 = 0;
     } sell[3];
+    bool kgValid = false;  // the recorded factors belong to the current positions and lists
     DBuf<U64x2> sellTot;
+    DBuf<unsigned long long> nbrTot;
+    // count-pass hit-mask record replayed by the fill pass (scratch, DICT_CAP entries per chunk)
+    static constexpr uint32_t DICT_CAP = 512;
+    DBuf<uint2> dict;
+    DBuf<uint32_t> dictCount;
+    uint64_t nNbr[3] = {0, 0, 0};
     DBuf<uint16_t> cntR[3];
     DBuf<uint64_t> offR[3];
     DBuf<uint32_t> listR[3];
@@ -235,11 +238,12 @@ public:
     DBuf<ProbeResult> probe;
     HostMirror* hm = nullptr;
     struct JacobiGraph {
-        uint64_t key = 0;
+        std::vector<uint64_t> key;
         cudaGraph_t g = nullptr;
         cudaGraphExec_t ex = nullptr;
     };
     std::vector<JacobiGraph> graphs;
+    DBuf<float> stage;  // device staging of the SoA <-> packed conversions at the state boundary (grow-only)
     size_t graphNext = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     float lastStepMs = 0.f, lastNbrMs = 0.f, lastJacMs = 0.f;
@@ -262,6 +266,7 @@ public:
         probe.ensure(1);
         nCellsDev.ensure(3);
         sellTot.ensure(3);
+        nbrTot.ensure(3);
         csrTot.ensure(3);
         CK(cudaMemset(st.p, 0, sizeof(SolverState)));
         CK(cudaMemset(err.p, 0, sizeof(uint32_t)));
@@ -333,12 +338,12 @@ public:
 
     void Pull(const tsp_state_view& v, const tsp_params& p) {
         CK(cudaSetDevice(device));
+        DBuf<float>& tmp = stage;
         prm = p;
         nF = v.N_F; nB = v.N_B; nR = v.N_R; nRB = v.N_RB;
         if (nF > 0x7fffffffu || nB > 0x7fffffffu || nR > 0x7fffffffu)
             throw Error(TSP_ERR_OVERFLOW, "particle count exceeds the local particle limit");
         stepCount = v.step; simTime = v.time;
-        DBuf<float> tmp;
         // fluid
         std::vector<uint64_t> ids;
         if (!v.idF) { ids.resize(nF); for (uint32_t i = 0; i < nF; i++) ids[i] = i; }
@@ -441,7 +446,7 @@ public:
     void Push(tsp_state_view& v) {
         CK(cudaSetDevice(device));
         v.N_F = nF; v.N_B = nB; v.N_R = nR; v.N_RB = nRB; v.step = stepCount; v.time = simTime;
-        DBuf<float> tmp, tmp2;
+        DBuf<float>& tmp = stage;
         if (v.idF && nF) CK(cudaMemcpyAsync(v.idF, idF.p, nF * 8ull, cudaMemcpyDeviceToHost, s));
         Unpack4(posP.p, nF, v.xPosF, v.yPosF, v.zPosF, v.pressureF, tmp);
         Sync();
@@ -502,12 +507,13 @@ public:
     SellMeta Meta(int k) {
         Sell& m = sell[k];
         return SellMeta{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p,
-                        (uint64_t)m.l16.cap, (uint64_t)m.l32.cap};
+                        (uint64_t)m.l16.cap, (uint64_t)m.l32.cap, m.kg16.p, m.kg32.p};
     }
     NeighborView NView() {
         auto sv = [&](int k) {
             Sell& m = sell[k];
-            return SellView{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p};
+            return SellView{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p,
+                            m.kg16.p, m.kg32.p};
         };
         return NeighborView{sv(0), sv(1), sv(2)};
     }
@@ -531,8 +537,8 @@ public:
     // UpdateCellFrame (neighbor_search.cpp:1902-2006); returns true when the frame changed
     bool UpdateFrame() {
         if (nF == 0 && nB == 0 && nR == 0) { frameValid = false; return false; }
-        ProbeResult init;
-        for (int a = 0; a < 3; a++) { init.mnKey[a] = 0x7fffffff; init.mxKey[a] = (int)0x80000000; }
+        ProbeResult init;  // identity bounds of an empty class (neighbor_search.cpp:205-213)
+        for (int a = 0; a < 3; a++) { init.mnKey[a] = OrderedIntHost(3.402823466e38f); init.mxKey[a] = OrderedIntHost(-3.402823466e38f); }
         init.exceeded = 0; init.pad = 0;
         hm->probe = init;
         CK(cudaMemcpyAsync(probe.p, &hm->probe, sizeof(ProbeResult), cudaMemcpyHostToDevice, s));
@@ -611,11 +617,14 @@ public:
             m.base.ensure(std::max<uint32_t>(nChunks, 1)); m.base2.ensure(std::max<uint32_t>(nChunks, 1));
             m.offset.ensure(std::max<uint32_t>(nChunks, 1));
             m.l16.ensure(std::max<size_t>(m.l16.cap, 16)); m.l32.ensure(std::max<size_t>(m.l32.cap, 16));
+            m.kg16.ensure(m.l16.cap); m.kg32.ensure(m.l32.cap);
             cntR[k].ensure(std::max<uint32_t>(nR, 1)); offR[k].ensure(nR + 1ull);
             listR[k].ensure(std::max<size_t>(listR[k].cap, 16));
         }
         velPred2.ensure(std::max<uint32_t>(nF, 1)); acc2.ensure(std::max<uint32_t>(nF, 1));
         srcDiag2.ensure(std::max<uint32_t>(nF, 1));
+        dict.ensure((size_t)std::max<uint32_t>(nChunks, 1) * DICT_CAP);
+        dictCount.ensure(std::max<uint32_t>(nChunks, 1));
     }
     // ReOrderParticleData + Construct + Query_Count + Finalize_Count + Query_Fill
     void NeighborBuild(bool permuteAll) {
@@ -667,6 +676,7 @@ public:
         QueryArgs qa = MakeQueryArgs();
         SellMeta m0 = Meta(0), m1 = Meta(1), m2 = Meta(2);
         RigidLists rl = RLists();
+        CK(cudaMemsetAsync(nbrTot.p, 0, 3 * sizeof(unsigned long long), s));
         LaunchQueryFluid(false, qa, m0, m1, m2, s);
         LaunchQueryRigid(false, qa, rl, s);
         const uint32_t nChunks = (nF + SELL_W - 1) / SELL_W;
@@ -675,12 +685,16 @@ public:
         CK(cudaMemcpyAsync(hm->sellTot, sellTot.p, 3 * sizeof(U64x2), cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(hm->csrTot, csrTot.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(hm->nCells, nCellsDev.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(hm->nbrTot, nbrTot.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
         Sync();
         for (int k = 0; k < 3; k++) {
+            nNbr[k] = nF ? hm->nbrTot[k] : 0;
             sell[k].n16 = hm->sellTot[k].a;
             sell[k].n32 = hm->sellTot[k].b;
             sell[k].l16.grow(sell[k].n16, 1.04);
             sell[k].l32.grow(sell[k].n32, 1.04);
+            sell[k].kg16.ensure(sell[k].l16.cap);
+            sell[k].kg32.ensure(sell[k].l32.cap);
             csrN[k] = hm->csrTot[k];
             listR[k].grow(csrN[k], 1.04);
         }
@@ -688,6 +702,7 @@ public:
         rl = RLists();
         LaunchQueryFluid(true, qa, m0, m1, m2, s);
         LaunchQueryRigid(true, qa, rl, s);
+        kgValid = false;
         launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + (nF ? 9u : 0u) + (nR ? 9u : 0u);
         listsValid = true;
     }
@@ -699,6 +714,8 @@ public:
         qa.startF = startF.p; qa.startB = startB.p; qa.startR = startR.p;
         qa.gridF = nF ? gridF.p : nullptr; qa.gridB = nB ? gridB.p : nullptr; qa.gridR = nR ? gridR.p : nullptr;
         qa.fr = fr; qa.r2 = prm.kernelRadiusSqu; qa.cap = QueryCap(reach); qa.err = err.p;
+        qa.nbrTotals = nbrTot.p;
+        qa.dict = dict.p; qa.dictCount = dictCount.p; qa.dictCap = DICT_CAP;
         return qa;
     }
     RigidLists RLists() {
@@ -707,17 +724,32 @@ public:
     }
 
     // -------------------------------------------------------------------------- Jacobi loop graph
-    uint64_t GraphKey(const Consts& c, const SolverControl& ctl) {
-        uint64_t h = 1469598103934665603ull;
-        FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
-        h = HashBytes(h, &f, sizeof(f)); h = HashBytes(h, &b, sizeof(b)); h = HashBytes(h, &r, sizeof(r));
-        h = HashBytes(h, &nv, sizeof(nv)); h = HashBytes(h, &c, sizeof(c)); h = HashBytes(h, &ctl, sizeof(ctl));
-        void* ptrs[2] = {st.p, partials.p};
-        h = HashBytes(h, ptrs, sizeof(ptrs));
-        return h;
+    // Exact key of a captured Jacobi graph: every pointer, size and constant its kernels were
+    // captured with, field by field (struct padding never enters the key).
+    std::vector<uint64_t> GraphKey(const Consts& c, const SolverControl& ctl) {
+        std::vector<uint64_t> k;
+        auto P = [&](const void* q) { k.push_back((uint64_t)(uintptr_t)q); };
+        const FluidDev f = FluidView(); const BoundaryDev b = BoundaryView(); const RigidDev r = RigidDevView();
+        const NeighborView nv = NView();
+        P(f.posP); P(f.velRho); P(f.velPred); P(f.acc); P(f.srcDiag); k.push_back(f.n);
+        P(b.pos); P(b.vol); k.push_back(b.n);
+        P(r.pos); P(r.vel); P(r.velPred); k.push_back(r.n);
+        for (const SellView* v : {&nv.ff, &nv.fb, &nv.fr}) {
+            P(v->counts); P(v->pitch); P(v->format); P(v->base); P(v->base2); P(v->offset);
+            P(v->list16); P(v->list32); P(v->kg16); P(v->kg32);
+        }
+        static_assert(sizeof(Consts) % 4 == 0, "Consts holds 4-byte fields only");
+        const uint32_t* cw = reinterpret_cast<const uint32_t*>(&c);
+        for (size_t i = 0; i < sizeof(Consts) / 4; i++) k.push_back(cw[i]);
+        k.push_back(ctl.minIters); k.push_back(ctl.maxIters); k.push_back(ctl.fixedIters); k.push_back(ctl.cond);
+        uint32_t tb;
+        std::memcpy(&tb, &ctl.target, 4);
+        k.push_back(tb); k.push_back(ctl.nF);
+        P(st.p); P(partials.p);
+        return k;
     }
     cudaGraphExec_t JacobiGraphFor(const Consts& c, const SolverControl& ctl) {
-        const uint64_t key = GraphKey(c, ctl);
+        std::vector<uint64_t> key = GraphKey(c, ctl);
         for (auto& g : graphs)
             if (g.ex && g.key == key) return g.ex;
         // build: while (cond) { pressure acceleration; Jacobi sweep (sets cond) }
@@ -747,7 +779,7 @@ public:
         graphNext++;
         if (slot.ex) cudaGraphExecDestroy(slot.ex);
         if (slot.g) cudaGraphDestroy(slot.g);
-        slot.key = key; slot.g = graph; slot.ex = ex;
+        slot.key = std::move(key); slot.g = graph; slot.ex = ex;
         return ex;
     }
 
@@ -777,6 +809,7 @@ public:
             LaunchRigidUpdateParticles(rp, bd, true, err.p, s);
         }
         LaunchSourceDiagInit(c, f, b, r, nv, st.p, s);
+        kgValid = true;
         CK(cudaEventRecord(ev[2], s));
         if (nF) {
             partials.ensure(3ull * JacobiBlocks(nF) + 3);
@@ -792,6 +825,7 @@ public:
             LaunchRigidReduce(rp, bd, s);
         }
         LaunchIntegration(c, f, s);
+        kgValid = false;
         if (nRB) {
             LaunchRigidPredict(bd, prm.timeStep, s);
             LaunchRigidIntegrate(bd, prm.timeStep, err.p, s);
@@ -828,9 +862,13 @@ public:
         switch (stage) {
             case TSP_STAGE_DENSITY: LaunchDensity(c, f, b, r, nv, s); break;
             case TSP_STAGE_NON_PRESSURE: LaunchNonPressure(c, f, b, r, nv, s); break;
-            case TSP_STAGE_SOURCE_DIAG_INIT: LaunchSourceDiagInit(c, f, b, r, nv, st.p, s); break;
-            case TSP_STAGE_PRESSURE_ACC: LaunchPressureAcc(c, f, b, r, nv, s); break;
+            case TSP_STAGE_SOURCE_DIAG_INIT: LaunchSourceDiagInit(c, f, b, r, nv, st.p, s); kgValid = true; break;
+            case TSP_STAGE_PRESSURE_ACC:
+                if (!kgValid) { LaunchGradFactors(c, f, b, r, nv, s); kgValid = true; }
+                LaunchPressureAcc(c, f, b, r, nv, s);
+                break;
             case TSP_STAGE_JACOBI_UPDATE: {
+                if (!kgValid) { LaunchGradFactors(c, f, b, r, nv, s); kgValid = true; }
                 partials.ensure(3ull * JacobiBlocks(nF) + 3);
                 LaunchJacobi(c, f, b, r, nv, Control(), st.p, partials.p, 0ull, false, s);
                 CK(cudaMemcpyAsync(&hm->st, st.p, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
@@ -838,8 +876,8 @@ public:
                 if (errSums) for (int k = 0; k < 3; k++) errSums[k] = hm->st.sums[k];
                 break;
             }
-            case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); break;
-            case TSP_STAGE_BOUNDARY_VOLUMES: BoundaryVolumes(c); break;
+            case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); kgValid = false; break;
+            case TSP_STAGE_BOUNDARY_VOLUMES: BoundaryVolumes(c); kgValid = false; break;
             default: throw Error(TSP_ERR_INVALID, "unknown stage");
         }
         CheckErrors();
@@ -855,6 +893,10 @@ public:
         FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
         partials.ensure(3ull * JacobiBlocks(nF) + 3);
         const SolverControl ctl = Control();
+        if (!kgValid && (stage == TSP_STAGE_PRESSURE_ACC || stage == TSP_STAGE_JACOBI_UPDATE)) {
+            LaunchGradFactors(c, f, b, r, nv, s);
+            kgValid = true;
+        }
         Sync();
         CK(cudaEventRecord(ev[0], s));
         for (uint32_t k = 0; k < reps; k++) {
@@ -961,7 +1003,7 @@ public:
 
     // -------------------------------------------------------------------------- inspection
     void ReadField(uint32_t field, void* out, uint32_t n) {
-        DBuf<float> tmp;
+        DBuf<float>& tmp = stage;
         float* o = (float*)out;
         auto un3 = [&](const float4* src, uint32_t cnt) {
             if (n != cnt) throw Error(TSP_ERR_INVALID, "field size mismatch");
@@ -1025,6 +1067,7 @@ public:
             for (uint32_t i = 0; i < cnt; i++) { h[i].x = x[3 * i]; h[i].y = x[3 * i + 1]; h[i].z = x[3 * i + 2]; }
             if (cnt) CK(cudaMemcpy(dst.p, h.data(), cnt * 16ull, cudaMemcpyHostToDevice));
         };
+        if (field == TSP_FIELD_POS || field == TSP_FIELD_PSI_B) kgValid = false;
         switch (field) {
             case TSP_FIELD_POS: set3(posP, nF); break;
             case TSP_FIELD_VEL: set3(velRho, nF); break;
@@ -1060,18 +1103,10 @@ public:
         o.cellOrig[0] = fr.ox; o.cellOrig[1] = fr.oy; o.cellOrig[2] = fr.oz;
         o.cellDims[0] = fr.nx; o.cellDims[1] = fr.ny; o.cellDims[2] = fr.nz;
         o.keyBits = fr.keyBits;
-        CK(cudaMemcpy(hm->nCells, nCellsDev.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost));
         o.nCellsF = nF ? (uint32_t)hm->nCells[0] : 0; o.nCellsB = nB ? (uint32_t)hm->nCells[1] : 0;
         o.nCellsR = nR ? (uint32_t)hm->nCells[2] : 0;
-        uint64_t tot[3] = {0, 0, 0};
-        if (listsValid && nF) {
-            for (int k = 0; k < 3; k++) {
-                std::vector<uint16_t> cnt(nF);
-                CK(cudaMemcpy(cnt.data(), sell[k].counts.p, nF * 2ull, cudaMemcpyDeviceToHost));
-                for (uint16_t c : cnt) tot[k] += c;
-            }
-        }
-        o.nNbrFF = tot[0]; o.nNbrFB = tot[1]; o.nNbrFR = tot[2];
+        const bool lv = listsValid && nF;
+        o.nNbrFF = lv ? nNbr[0] : 0; o.nNbrFB = lv ? nNbr[1] : 0; o.nNbrFR = lv ? nNbr[2] : 0;
         o.nNbrRF = csrN[0]; o.nNbrRB = csrN[1]; o.nNbrRR = csrN[2];
         for (int k = 0; k < 3; k++) o.sellPackedBytes += sell[k].n16 * 2 + sell[k].n32 * 4;
         o.lastStepMs = lastStepMs; o.lastNeighborMs = lastNbrMs; o.lastJacobiMs = lastJacMs;
@@ -1280,6 +1315,14 @@ int tsp_b200_read_rows(const tsp_backend* h, uint32_t list, uint64_t* offsets, u
         if (list > 5) throw Error(TSP_ERR_INVALID, "unknown list");
         if (list >= 3) {
             const int k = (int)list - 3;
+            if (b.nR == 0 || !b.listsValid) {  // nothing built: every row is empty
+                if (total) *total = 0;
+                if (offsets) {
+                    if (nSrc != b.nR) throw Error(TSP_ERR_INVALID, "size mismatch");
+                    std::memset(offsets, 0, (b.nR + 1ull) * 8ull);
+                }
+                return TSP_OK;
+            }
             if (total) *total = b.csrN[k];
             if (offsets) {
                 if (nSrc != b.nR) throw Error(TSP_ERR_INVALID, "size mismatch");
@@ -1291,8 +1334,8 @@ int tsp_b200_read_rows(const tsp_backend* h, uint32_t list, uint64_t* offsets, u
             }
             return TSP_OK;
         }
-        std::vector<uint16_t> cnt(b.nF);
-        if (b.nF) CK(cudaMemcpy(cnt.data(), b.sell[list].counts.p, b.nF * 2ull, cudaMemcpyDeviceToHost));
+        std::vector<uint16_t> cnt(b.nF, 0);
+        if (b.nF && b.listsValid) CK(cudaMemcpy(cnt.data(), b.sell[list].counts.p, b.nF * 2ull, cudaMemcpyDeviceToHost));
         std::vector<uint64_t> off(b.nF + 1ull, 0);
         for (uint32_t i = 0; i < b.nF; i++) off[i + 1] = off[i] + cnt[i];
         if (total) *total = off[b.nF];
@@ -1300,7 +1343,7 @@ int tsp_b200_read_rows(const tsp_backend* h, uint32_t list, uint64_t* offsets, u
             if (nSrc != b.nF) throw Error(TSP_ERR_INVALID, "size mismatch");
             std::memcpy(offsets, off.data(), off.size() * 8);
         }
-        if (indices && off[b.nF]) {
+        if (indices && off[b.nF] && b.listsValid) {
             if (cap < off[b.nF]) throw Error(TSP_ERR_INVALID, "capacity");
             tsp::DBuf<uint64_t> dOff;
             tsp::DBuf<uint32_t> dOut;

@@ -35,6 +35,7 @@ struct ProbeResult {
     uint32_t pad;
 };
 float OrderedIntToFloat(int k);
+int OrderedIntHost(float f);
 
 struct SortScratch {
     uint64_t* keysA;
@@ -61,6 +62,10 @@ struct QueryArgs {
     float r2;
     uint32_t cap;
     uint32_t* err;
+    unsigned long long* nbrTotals;  // FF, FB, FR neighbor totals (accumulated by the count pass)
+    uint2* dict;                    // per-chunk hit-mask record of the count pass (NULL: fill re-sweeps)
+    uint32_t* dictCount;            // entries per chunk, EMPTY_32 when the record overflowed
+    uint32_t dictCap;               // entries per chunk
 };
 
 struct RigidLists {
@@ -115,6 +120,8 @@ struct SellView {
     const uint64_t* offset;
     const uint16_t* list16;
     const uint32_t* list32;
+    float* kg16;   // per-slot kernel-gradient factors of the current positions, written by the
+    float* kg32;   // source/diagonal stage and read by the pressure-acceleration / Jacobi sweeps
 };
 struct NeighborView {
     SellView ff, fb, fr;
@@ -164,6 +171,10 @@ void LaunchBoundaryVolumes(const Consts& c, const float4* posB, uint32_t nB, con
                            const uint32_t* gridB, const Frame& fr, float defaultVol, float defaultPsi, float restDensity,
                            float* volOut, float* psiOut, cudaStream_t s);
 void LaunchSolverReset(SolverState* st, uint32_t nF, cudaStream_t s);
+// per-slot kernel-gradient factors for the current positions (same values the source /
+// diagonal stage records), for stage-level use after positions were rewritten
+void LaunchGradFactors(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
+                       const NeighborView& nv, cudaStream_t s);
 
 // ---- rigid_kernels.cu
 struct BodyDev {

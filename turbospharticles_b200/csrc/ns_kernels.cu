@@ -27,6 +27,11 @@ __device__ __forceinline__ int OrderedInt(float f) {
     const int i = __float_as_int(f);
     return (i >= 0) ? i : (i ^ 0x7fffffff);
 }
+int OrderedIntHost(float f) {
+    int i;
+    memcpy(&i, &f, 4);
+    return (i >= 0) ? i : (i ^ 0x7fffffff);
+}
 __host__ float OrderedIntToFloat(int k) {
     const int i = (k >= 0) ? k : (k ^ 0x7fffffff);
     float f;
@@ -291,6 +296,113 @@ __device__ __forceinline__ void WarpBitonicSort(uint64_t* v, uint32_t S, uint32_
     }
 }
 
+// per-warp record of the count pass: (candidate | species << 30, 32-lane hit mask) for every
+// candidate that is a neighbor of at least one lane, in sweep order, staged 32 entries per
+// coalesced 256 B store; the fill pass replays it instead of repeating the candidate sweep
+struct DictRec {
+    uint2* base;
+    uint32_t n, cap;
+    uint32_t pj, pm;
+    bool ok;
+    __device__ __forceinline__ void push(uint32_t tagged, uint32_t mask, uint32_t lane) {
+        if (n < cap) {
+            if (lane == (n & 31u)) { pj = tagged; pm = mask; }
+            if ((n & 31u) == 31u) base[(n & ~31u) + lane] = make_uint2(pj, pm);
+        }
+        n++;
+    }
+    __device__ __forceinline__ void finish(uint32_t lane) {
+        if (n <= cap && lane < (n & 31u)) base[(n & ~31u) + lane] = make_uint2(pj, pm);
+    }
+};
+
+struct QueryLane {
+    float4 pi;
+    int lx, ly, lz;
+    bool member;
+    uint32_t homeLo, homeHi;
+};
+
+// candidate sweep of one species over the group's sorted candidate cells (warp-uniform loop)
+template <int SP, bool FILL>
+__device__ __forceinline__ void SweepSpecies(const QueryArgs& a, const uint64_t* cells, uint32_t vol, const QueryLane& q,
+                                             uint32_t lane, LaneRefs& ref, LaneWriter& w, const SellMeta& m,
+                                             DictRec& dict) {
+    const uint32_t* grid = SP == 0 ? a.gridF : SP == 1 ? a.gridB : a.gridR;
+    const uint32_t* start = SP == 0 ? a.startF : SP == 1 ? a.startB : a.startR;
+    const float4* pos = SP == 0 ? a.posF : SP == 1 ? a.posB : a.posR;
+    if (grid == nullptr) return;
+    const int r = (int)a.fr.reach;
+    for (uint32_t cb = 0; cb < vol; cb += 32) {
+        const uint32_t t = cb + lane;
+        uint32_t b = 0, e = 0;
+        int cx = 0, cy = 0, cz = 0;
+        if (t < vol) {
+            const uint64_t mc = cells[t];
+            cx = (int)Compact21(mc); cy = (int)Compact21(mc >> 1); cz = (int)Compact21(mc >> 2);
+            const uint32_t c = grid[(uint64_t)cx + (uint64_t)a.fr.nx * ((uint64_t)cy + (uint64_t)a.fr.ny * cz)];
+            if (c != EMPTY_32) { b = start[c]; e = start[c + 1]; }
+        }
+        uint32_t nonEmpty = __ballot_sync(0xffffffffu, b < e);
+        while (nonEmpty) {
+            const int l = __ffs(nonEmpty) - 1;
+            nonEmpty &= nonEmpty - 1;
+            const uint32_t cb_ = __shfl_sync(0xffffffffu, b, l), ce = __shfl_sync(0xffffffffu, e, l);
+            const int ccx = __shfl_sync(0xffffffffu, cx, l), ccy = __shfl_sync(0xffffffffu, cy, l),
+                      ccz = __shfl_sync(0xffffffffu, cz, l);
+            // strict per-particle stencil (GatherCellQueryRanges, neighbor_search.cpp:917-947)
+            const bool ok = q.member && abs(ccx - q.lx) <= r && abs(ccy - q.ly) <= r && abs(ccz - q.lz) <= r;
+            if (!__any_sync(0xffffffffu, ok)) continue;
+            for (uint32_t k = cb_; k < ce; k++) {
+                const uint32_t j = (SP == 2) ? a.permR[k] : k;
+                const float4 pj = pos[j];
+                const bool hit = ok && IsNeighbor(q.pi.x, q.pi.y, q.pi.z, pj.x, pj.y, pj.z, a.r2);
+                if (FILL) {
+                    if (hit) w.store(m, lane, j, a.err);
+                } else {
+                    const uint32_t mask = __ballot_sync(0xffffffffu, hit);
+                    if (mask) dict.push(j < (1u << 30) ? (j | ((uint32_t)SP << 30)) : 0xffffffffu, mask, lane);
+                    if (j >= (1u << 30)) dict.ok = false;
+                    if (hit) {
+                        ref.cnt++;
+                        ref.mn = min(ref.mn, j);
+                        ref.mx = max(ref.mx, j);
+                        if (SP == 0) {
+                            if (j < q.homeLo) ref.farLoMax = max(ref.farLoMax, j);
+                            else if (j > q.homeHi) ref.farHiMin = min(ref.farHiMin, j);
+                            else ref.homeMin = min(ref.homeMin, j);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void SortRowSell(const SellMeta& m, const LaneWriter& w, uint32_t lane) {
+    // rigid candidates arrive in sorted-cell order; rows are kept in ascending index order
+    // (the Delta16x2 / Abs32 codes of an FR chunk are monotonic in the index)
+    for (uint32_t x = 1; x < w.wr; x++) {
+        const uint64_t at = w.off + (uint64_t)x * SELL_W + lane;
+        uint32_t y = x;
+        if (w.fmt == FMT_DELTA16X2) {
+            const uint16_t v = m.list16[at];
+            while (y > 0 && m.list16[w.off + (uint64_t)(y - 1) * SELL_W + lane] > v) {
+                m.list16[w.off + (uint64_t)y * SELL_W + lane] = m.list16[w.off + (uint64_t)(y - 1) * SELL_W + lane];
+                y--;
+            }
+            m.list16[w.off + (uint64_t)y * SELL_W + lane] = v;
+        } else {
+            const uint32_t v = m.list32[at];
+            while (y > 0 && m.list32[w.off + (uint64_t)(y - 1) * SELL_W + lane] > v) {
+                m.list32[w.off + (uint64_t)y * SELL_W + lane] = m.list32[w.off + (uint64_t)(y - 1) * SELL_W + lane];
+                y--;
+            }
+            m.list32[w.off + (uint64_t)y * SELL_W + lane] = v;
+        }
+    }
+}
+
 template <bool FILL>
 __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluid(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
     extern __shared__ uint64_t qsmem[];
@@ -303,23 +415,49 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluid(QueryArgs a, SellMe
     const bool inRange = i < a.nF;
     const uint64_t cid = inRange ? a.cidF[i] : EMPTY_64;
     const bool valid = cid != EMPTY_64;
-    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (inRange) pi = a.posF[i];
-    int lx = 0, ly = 0, lz = 0;
-    if (valid) { lx = (int)Compact21(cid); ly = (int)Compact21(cid >> 1); lz = (int)Compact21(cid >> 2); }
+    QueryLane q;
+    q.pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (inRange) q.pi = a.posF[i];
+    q.lx = q.ly = q.lz = 0;
+    if (valid) { q.lx = (int)Compact21(cid); q.ly = (int)Compact21(cid >> 1); q.lz = (int)Compact21(cid >> 2); }
+    HomeWindow(chunk, q.homeLo, q.homeHi);
     const int r = (int)a.fr.reach;
 
     LaneRefs rFF, rFB, rFR;
     rFF.init(); rFB.init(); rFR.init();
     LaneWriter wFF, wFB, wFR;
     if (FILL) { wFF.init(mFF, chunk); wFB.init(mFB, chunk); wFR.init(mFR, chunk); }
-    uint32_t homeLo, homeHi;
-    HomeWindow(chunk, homeLo, homeHi);
+    DictRec dict;
+    dict.base = a.dict ? a.dict + (uint64_t)chunk * a.dictCap : nullptr;
+    dict.n = 0; dict.cap = a.dict ? a.dictCap : 0u; dict.pj = 0; dict.pm = 0; dict.ok = a.dict != nullptr;
+
+    if (FILL && a.dict) {
+        // replay the count pass's hit masks (same order as the sweep)
+        const uint32_t nd = a.dictCount[chunk];
+        if (nd != EMPTY_32) {
+            const uint2* d = a.dict + (uint64_t)chunk * a.dictCap;
+            for (uint32_t b0 = 0; b0 < nd; b0 += 32) {
+                const uint2 mine = (b0 + lane < nd) ? d[b0 + lane] : make_uint2(0u, 0u);
+                const uint32_t cntHere = min(32u, nd - b0);
+                for (uint32_t e = 0; e < cntHere; e++) {
+                    const uint32_t tj = __shfl_sync(0xffffffffu, mine.x, e);
+                    const uint32_t tm = __shfl_sync(0xffffffffu, mine.y, e);
+                    if (!((tm >> lane) & 1u)) continue;
+                    const uint32_t sp = tj >> 30, j = tj & 0x3fffffffu;
+                    if (sp == 0) wFF.store(mFF, lane, j, a.err);
+                    else if (sp == 1) wFB.store(mFB, lane, j, a.err);
+                    else wFR.store(mFR, lane, j, a.err);
+                }
+            }
+            if (inRange && wFR.wr > 1) SortRowSell(mFR, wFR, lane);
+            return;
+        }
+    }
 
     const uint32_t validMask = __ballot_sync(0xffffffffu, valid);
     if (validMask) {
-        int mnx = valid ? lx : 0x7fffffff, mny = valid ? ly : 0x7fffffff, mnz = valid ? lz : 0x7fffffff;
-        int mxx = valid ? lx : -1, mxy = valid ? ly : -1, mxz = valid ? lz : -1;
+        int mnx = valid ? q.lx : 0x7fffffff, mny = valid ? q.ly : 0x7fffffff, mnz = valid ? q.lz : 0x7fffffff;
+        int mxx = valid ? q.lx : -1, mxy = valid ? q.ly : -1, mxz = valid ? q.lz : -1;
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) {
             mnx = min(mnx, __shfl_xor_sync(0xffffffffu, mnx, d)); mxx = max(mxx, __shfl_xor_sync(0xffffffffu, mxx, d));
@@ -342,14 +480,14 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluid(QueryArgs a, SellMe
         uint32_t groupsLeft = startMask;
         for (uint32_t g = 0; g < nGroups; g++) {
             int gx0 = bx0, gy0 = by0, gz0 = bz0, gx1 = bx1, gy1 = by1, gz1 = bz1;
-            bool member = valid;
+            q.member = valid;
             if (!boxMode) {
                 const int L = __ffs(groupsLeft) - 1;
                 groupsLeft &= groupsLeft - 1;
                 const uint64_t gcid = __shfl_sync(0xffffffffu, cid, L);
-                const int cx = __shfl_sync(0xffffffffu, lx, L), cy = __shfl_sync(0xffffffffu, ly, L),
-                          cz = __shfl_sync(0xffffffffu, lz, L);
-                member = valid && cid == gcid;
+                const int cx = __shfl_sync(0xffffffffu, q.lx, L), cy = __shfl_sync(0xffffffffu, q.ly, L),
+                          cz = __shfl_sync(0xffffffffu, q.lz, L);
+                q.member = valid && cid == gcid;
                 gx0 = max(cx - r, 0); gy0 = max(cy - r, 0); gz0 = max(cz - r, 0);
                 gx1 = min(cx + r, (int)a.fr.nx - 1); gy1 = min(cy + r, (int)a.fr.ny - 1); gz1 = min(cz + r, (int)a.fr.nz - 1);
             }
@@ -371,88 +509,39 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluid(QueryArgs a, SellMe
             }
             __syncwarp();
             WarpBitonicSort(cells, S, lane);
-
-            for (int species = 0; species < 3; species++) {
-                const uint32_t* grid = species == 0 ? a.gridF : species == 1 ? a.gridB : a.gridR;
-                const uint32_t* start = species == 0 ? a.startF : species == 1 ? a.startB : a.startR;
-                const float4* pos = species == 0 ? a.posF : species == 1 ? a.posB : a.posR;
-                if (grid == nullptr) continue;
-                for (uint32_t cb = 0; cb < vol; cb += 32) {
-                    const uint32_t t = cb + lane;
-                    uint32_t b = 0, e = 0;
-                    int cx = 0, cy = 0, cz = 0;
-                    if (t < vol) {
-                        const uint64_t m = cells[t];
-                        cx = (int)Compact21(m); cy = (int)Compact21(m >> 1); cz = (int)Compact21(m >> 2);
-                        const uint32_t c = grid[(uint64_t)cx + (uint64_t)a.fr.nx * ((uint64_t)cy + (uint64_t)a.fr.ny * cz)];
-                        if (c != EMPTY_32) { b = start[c]; e = start[c + 1]; }
-                    }
-                    uint32_t nonEmpty = __ballot_sync(0xffffffffu, b < e);
-                    while (nonEmpty) {
-                        const int l = __ffs(nonEmpty) - 1;
-                        nonEmpty &= nonEmpty - 1;
-                        const uint32_t cb_ = __shfl_sync(0xffffffffu, b, l), ce = __shfl_sync(0xffffffffu, e, l);
-                        const int ccx = __shfl_sync(0xffffffffu, cx, l), ccy = __shfl_sync(0xffffffffu, cy, l),
-                                  ccz = __shfl_sync(0xffffffffu, cz, l);
-                        // strict per-particle stencil (GatherCellQueryRanges, neighbor_search.cpp:917-947)
-                        const bool ok = member && abs(ccx - lx) <= r && abs(ccy - ly) <= r && abs(ccz - lz) <= r;
-                        for (uint32_t k = cb_; k < ce; k++) {
-                            const uint32_t j = (species == 2) ? a.permR[k] : k;
-                            const float4 pj = pos[j];
-                            const bool hit = ok && IsNeighbor(pi.x, pi.y, pi.z, pj.x, pj.y, pj.z, a.r2);
-                            if (!hit) continue;
-                            if (species == 0) {
-                                if (FILL) wFF.store(mFF, lane, j, a.err);
-                                else {
-                                    rFF.cnt++; rFF.mn = min(rFF.mn, j); rFF.mx = max(rFF.mx, j);
-                                    if (j < homeLo) rFF.farLoMax = max(rFF.farLoMax, j);
-                                    else if (j > homeHi) rFF.farHiMin = min(rFF.farHiMin, j);
-                                    else rFF.homeMin = min(rFF.homeMin, j);
-                                }
-                            } else if (species == 1) {
-                                if (FILL) wFB.store(mFB, lane, j, a.err);
-                                else { rFB.cnt++; rFB.mn = min(rFB.mn, j); rFB.mx = max(rFB.mx, j); }
-                            } else {
-                                if (FILL) wFR.store(mFR, lane, j, a.err);
-                                else { rFR.cnt++; rFR.mn = min(rFR.mn, j); rFR.mx = max(rFR.mx, j); }
-                            }
-                        }
-                    }
-                }
-            }
+            SweepSpecies<0, FILL>(a, cells, vol, q, lane, rFF, wFF, mFF, dict);
+            SweepSpecies<1, FILL>(a, cells, vol, q, lane, rFB, wFB, mFB, dict);
+            SweepSpecies<2, FILL>(a, cells, vol, q, lane, rFR, wFR, mFR, dict);
             __syncwarp();
         }
     }
     if (FILL) {
-        // rigid candidates arrive in sorted-cell order; rows are kept in ascending index order
-        if (inRange && wFR.wr > 1) {
-            for (uint32_t x = 1; x < wFR.wr; x++) {
-                const uint64_t lx_ = wFR.off + (uint64_t)x * SELL_W + lane;
-                uint32_t y = x;
-                if (wFR.fmt == FMT_DELTA16X2) {
-                    const uint16_t v = mFR.list16[lx_];
-                    while (y > 0 && mFR.list16[wFR.off + (uint64_t)(y - 1) * SELL_W + lane] > v) {
-                        mFR.list16[wFR.off + (uint64_t)y * SELL_W + lane] = mFR.list16[wFR.off + (uint64_t)(y - 1) * SELL_W + lane];
-                        y--;
-                    }
-                    mFR.list16[wFR.off + (uint64_t)y * SELL_W + lane] = v;
-                } else {
-                    const uint32_t v = mFR.list32[lx_];
-                    while (y > 0 && mFR.list32[wFR.off + (uint64_t)(y - 1) * SELL_W + lane] > v) {
-                        mFR.list32[wFR.off + (uint64_t)y * SELL_W + lane] = mFR.list32[wFR.off + (uint64_t)(y - 1) * SELL_W + lane];
-                        y--;
-                    }
-                    mFR.list32[wFR.off + (uint64_t)y * SELL_W + lane] = v;
-                }
-            }
-        }
+        if (inRange && wFR.wr > 1) SortRowSell(mFR, wFR, lane);
         return;
+    }
+    if (a.dict) {
+        dict.finish(lane);
+        if (lane == 0) a.dictCount[chunk] = (dict.ok && dict.n <= dict.cap) ? dict.n : EMPTY_32;
     }
     if (inRange) {
         if ((rFF.cnt | rFB.cnt | rFR.cnt) > 0xffffu) atomicOr(a.err, ERR_COUNT_U16);
         mFF.counts[i] = (uint16_t)rFF.cnt;
         mFB.counts[i] = (uint16_t)rFB.cnt;
         mFR.counts[i] = (uint16_t)rFR.cnt;
+    }
+    {
+        uint32_t t0 = rFF.cnt & 0xffffu, t1 = rFB.cnt & 0xffffu, t2 = rFR.cnt & 0xffffu;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            t0 += __shfl_xor_sync(0xffffffffu, t0, d);
+            t1 += __shfl_xor_sync(0xffffffffu, t1, d);
+            t2 += __shfl_xor_sync(0xffffffffu, t2, d);
+        }
+        if (lane == 0 && a.nbrTotals) {
+            atomicAdd(a.nbrTotals + 0, (unsigned long long)t0);
+            atomicAdd(a.nbrTotals + 1, (unsigned long long)t1);
+            atomicAdd(a.nbrTotals + 2, (unsigned long long)t2);
+        }
     }
     const bool owner = lane == 0;
     CommitChunkMeta(chunk, owner, rFF, true, mFF);

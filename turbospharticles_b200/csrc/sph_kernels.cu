@@ -27,58 +27,111 @@ struct ChunkCursor {
     __device__ __forceinline__ uint32_t nbr(const SellView& v, uint32_t k, uint32_t lane) const {
         return SellNeighbor(fmt, base, base2, off, k, lane, v.list16, v.list32);
     }
+    // recorded kernel-gradient factor of slot k (same index as the list entry)
+    __device__ __forceinline__ float* kgSlot(const SellView& v, uint32_t k, uint32_t lane) const {
+        return (fmt == FMT_DELTA16X2 ? v.kg16 : v.kg32) + off + (uint64_t)k * SELL_W + lane;
+    }
 };
+
+// Visits the FF slots of a lane in order, U slots at a time: the U list entries are loaded
+// together, then the U neighbor gathers (one or two float4 each), then the U pair terms are
+// applied in slot order. The sum order is unchanged; the loads of a group are independent, so
+// up to 3U memory requests per lane are in flight instead of one dependent chain per slot.
+template <int U, bool TWO, typename Body>
+__device__ __forceinline__ void SweepSlots(const ChunkCursor& cur, const SellView& v, uint32_t lane,
+                                           const float4* A, const float4* B, Body&& body) {
+    for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
+        uint32_t j[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) j[u] = (k0 + u < cur.cnt) ? cur.nbr(v, k0 + u, lane) : EMPTY_32;
+        float4 a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            a[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+            b[u] = a[u];
+            if (j[u] != EMPTY_32) {
+                a[u] = A[j[u]];
+                if (TWO) b[u] = B[j[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (j[u] != EMPTY_32) body(k0 + u, j[u], a[u], b[u]);
+    }
+}
+
+// as SweepSlots, also loading each slot's recorded kernel-gradient factor (no sqrt / division)
+template <int U, bool TWO, typename Body>
+__device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellView& v, uint32_t lane,
+                                             const float4* A, const float4* B, Body&& body) {
+    for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
+        uint32_t j[U];
+        float kg[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool ok = k0 + u < cur.cnt;
+            j[u] = ok ? cur.nbr(v, k0 + u, lane) : EMPTY_32;
+            kg[u] = ok ? *cur.kgSlot(v, k0 + u, lane) : 0.0f;
+        }
+        float4 a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            a[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+            b[u] = a[u];
+            if (j[u] != EMPTY_32) {
+                a[u] = A[j[u]];
+                if (TWO) b[u] = B[j[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (j[u] != EMPTY_32) body(kg[u], a[u], b[u]);
+    }
+}
+
+// persistent warps: warp w of the grid handles chunks w, w + W, w + 2W, ...
+#define FOR_EACH_CHUNK(n)                                                                  \
+    const uint32_t lane = threadIdx.x & 31;                                                \
+    const uint32_t nChunks_ = ((n) + SELL_W - 1) / SELL_W;                                 \
+    const uint32_t warps_ = (gridDim.x * blockDim.x) >> 5;                                 \
+    for (uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < nChunks_; chunk += warps_)
 
 // ----------------------------------------------------------------------------- density
 __global__ void __launch_bounds__(SPH_THREADS) KDensity(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv) {
-    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
-    const uint32_t chunk = i >> 5, lane = i & 31;
-    if (chunk * SELL_W >= f.n) return;
-    const bool act = i < f.n;
-    const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    float dF = 0.f, dB = 0.f, dR = 0.f;
-    ChunkCursor cur;
-    cur.load(nv.ff, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const float4 pj = f.posP[cur.nbr(nv.ff, k, lane)];
+    FOR_EACH_CHUNK(f.n) {
+        const uint32_t i = chunk * SELL_W + lane;
+        const bool act = i < f.n;
+        const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float dF = 0.f, dB = 0.f, dR = 0.f;
+        ChunkCursor cur;
+        cur.load(nv.ff, chunk, i, act);
+        SweepSlots<4, false>(cur, nv.ff, lane, f.posP, nullptr, [&](uint32_t, uint32_t, const float4& pj, const float4&) {
             dF = fmaf(c.massF, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dF);
-        }
-    }
-    cur.load(nv.fb, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const float4 pj = b.pos[cur.nbr(nv.fb, k, lane)];
+        });
+        cur.load(nv.fb, chunk, i, act);
+        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](uint32_t, uint32_t, const float4& pj, const float4&) {
             dB = fmaf(pj.w, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dB);
-        }
-    }
-    cur.load(nv.fr, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const float4 pj = r.pos[cur.nbr(nv.fr, k, lane)];
+        });
+        cur.load(nv.fr, chunk, i, act);
+        SweepSlots<2, false>(cur, nv.fr, lane, r.pos, nullptr, [&](uint32_t, uint32_t, const float4& pj, const float4&) {
             dR = fmaf(pj.w, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dR);
-        }
+        });
+        if (act) reinterpret_cast<float*>(f.velRho)[4ull * i + 3] = dF + dB + dR;
     }
-    if (act) reinterpret_cast<float*>(f.velRho)[4ull * i + 3] = dF + dB + dR;
 }
 
 // ----------------------------------------------------------------------------- non-pressure
-__global__ void __launch_bounds__(SPH_THREADS) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+__global__ void __launch_bounds__(SPH_THREADS, 4) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
-    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
-    const uint32_t chunk = i >> 5, lane = i & 31;
-    if (chunk * SELL_W >= f.n) return;
-    const bool act = i < f.n;
-    const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 vi = act ? f.velRho[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    float fx = 0.f, fy = 0.f, fz = 0.f, bx = 0.f, by = 0.f, bz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
-    ChunkCursor cur;
-    cur.load(nv.ff, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const uint32_t j = cur.nbr(nv.ff, k, lane);
-            const float4 pj = f.posP[j];
-            const float4 vj = f.velRho[j];
+    FOR_EACH_CHUNK(f.n) {
+        const uint32_t i = chunk * SELL_W + lane;
+        const bool act = i < f.n;
+        const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 vi = act ? f.velRho[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float fx = 0.f, fy = 0.f, fz = 0.f, bx = 0.f, by = 0.f, bz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
+        ChunkCursor cur;
+        cur.load(nv.ff, chunk, i, act);
+        SweepSlots<4, true>(cur, nv.ff, lane, f.posP, f.velRho, [&](uint32_t, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -87,13 +140,9 @@ __global__ void __launch_bounds__(SPH_THREADS) KNonPressure(Consts c, FluidDev f
             const float rhoJ = fmaxf(vj.w, 1e-7f);
             const float a = (c.massF * dot) / (rhoJ * (d2 + c.hEps)) * kg;
             fx = fmaf(a, dx, fx); fy = fmaf(a, dy, fy); fz = fmaf(a, dz, fz);
-        }
-    }
-    cur.load(nv.fb, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const uint32_t j = cur.nbr(nv.fb, k, lane);
-            const float4 pj = b.pos[j];
+        });
+        cur.load(nv.fb, chunk, i, act);
+        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](uint32_t, uint32_t j, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
@@ -102,14 +151,9 @@ __global__ void __launch_bounds__(SPH_THREADS) KNonPressure(Consts c, FluidDev f
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float a = (b.vol[j] * dot) / (d2 + c.hEps);
             bx = fmaf(a, gx, bx); by = fmaf(a, gy, by); bz = fmaf(a, gz, bz);
-        }
-    }
-    cur.load(nv.fr, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const uint32_t j = cur.nbr(nv.fr, k, lane);
-            const float4 pj = r.pos[j];
-            const float4 vj = r.vel[j];
+        });
+        cur.load(nv.fr, chunk, i, act);
+        SweepSlots<2, true>(cur, nv.fr, lane, r.pos, r.vel, [&](uint32_t, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
@@ -118,134 +162,112 @@ __global__ void __launch_bounds__(SPH_THREADS) KNonPressure(Consts c, FluidDev f
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float a = (vj.w * dot) / (d2 + c.hEps);
             rx = fmaf(a, gx, rx); ry = fmaf(a, gy, ry); rz = fmaf(a, gz, rz);
-        }
+        });
+        if (!act) continue;
+        const float ax = fx * c.visFacF + (bx + rx) * c.visFacB + c.gx;
+        const float ay = fy * c.visFacF + (by + ry) * c.visFacB + c.gy;
+        const float az = fz * c.visFacF + (bz + rz) * c.visFacB + c.gz;
+        f.velPred[i] = make_float4(fmaf(ax, c.dt, vi.x), fmaf(ay, c.dt, vi.y), fmaf(az, c.dt, vi.z), 0.0f);
     }
-    if (!act) return;
-    const float ax = fx * c.visFacF + (bx + rx) * c.visFacB + c.gx;
-    const float ay = fy * c.visFacF + (by + ry) * c.visFacB + c.gy;
-    const float az = fz * c.visFacF + (bz + rz) * c.visFacB + c.gz;
-    f.velPred[i] = make_float4(fmaf(ax, c.dt, vi.x), fmaf(ay, c.dt, vi.y), fmaf(az, c.dt, vi.z), 0.0f);
 }
 
 // ----------------------------------------------------------------------------- source / diagonal / init
-__global__ void __launch_bounds__(SPH_THREADS) KSourceDiagInit(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+__global__ void __launch_bounds__(SPH_THREADS, 4) KSourceDiagInit(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                             NeighborView nv) {
-    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
-    const uint32_t chunk = i >> 5, lane = i & 31;
-    if (chunk * SELL_W >= f.n) return;
-    const bool act = i < f.n;
-    const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 vi = act ? f.velPred[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    float sF = 0.f, sB = 0.f, sR = 0.f, cxF = 0.f, cyF = 0.f, czF = 0.f, g2 = 0.f;
-    float cxB = 0.f, cyB = 0.f, czB = 0.f, cxR = 0.f, cyR = 0.f, czR = 0.f;
-    ChunkCursor cur;
-    cur.load(nv.ff, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const uint32_t j = cur.nbr(nv.ff, k, lane);
-            const float4 pj = f.posP[j];
-            const float4 vj = f.velPred[j];
+    FOR_EACH_CHUNK(f.n) {
+        const uint32_t i = chunk * SELL_W + lane;
+        const bool act = i < f.n;
+        const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 vi = act ? f.velPred[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float sF = 0.f, sB = 0.f, sR = 0.f, cxF = 0.f, cyF = 0.f, czF = 0.f, g2 = 0.f;
+        float cxB = 0.f, cyB = 0.f, czB = 0.f, cxR = 0.f, cyR = 0.f, czR = 0.f;
+        ChunkCursor cur;
+        cur.load(nv.ff, chunk, i, act);
+        SweepSlots<4, true>(cur, nv.ff, lane, f.posP, f.velPred, [&](uint32_t k, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float kg = GradFactor(d2, c);
+            *cur.kgSlot(nv.ff, k, lane) = kg;
             const float st = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
             sF = fmaf(kg, st, sF);
             cxF = fmaf(kg, dx, cxF); cyF = fmaf(kg, dy, cyF); czF = fmaf(kg, dz, czF);
             g2 = fmaf(kg, kg * d2, g2);  // (kgFac * distSqu first keeps the self pair exactly zero)
-        }
-    }
-    cur.load(nv.fb, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const float4 pj = b.pos[cur.nbr(nv.fb, k, lane)];
+        });
+        cur.load(nv.fb, chunk, i, act);
+        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+            *cur.kgSlot(nv.fb, k, lane) = kg;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float dvx = vi.x - 0.0f, dvy = vi.y - 0.0f, dvz = vi.z - 0.0f;
             const float st = fmaf(dvx, gx, fmaf(dvy, gy, dvz * gz));
             sB = fmaf(pj.w, st, sB);
             cxB = fmaf(pj.w, gx, cxB); cyB = fmaf(pj.w, gy, cyB); czB = fmaf(pj.w, gz, czB);
-        }
-    }
-    cur.load(nv.fr, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const uint32_t j = cur.nbr(nv.fr, k, lane);
-            const float4 pj = r.pos[j];
-            const float4 vj = r.velPred[j];
+        });
+        cur.load(nv.fr, chunk, i, act);
+        SweepSlots<2, true>(cur, nv.fr, lane, r.pos, r.velPred, [&](uint32_t k, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+            *cur.kgSlot(nv.fr, k, lane) = kg;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float st = fmaf(dvx, gx, fmaf(dvy, gy, dvz * gz));
             sR = fmaf(pj.w, st, sR);
             cxR = fmaf(pj.w, gx, cxR); cyR = fmaf(pj.w, gy, cyR); czR = fmaf(pj.w, gz, czR);
-        }
+        });
+        if (!act) continue;
+        sF *= c.massF;
+        const float rho = f.velRho[i].w;
+        const float src = c.restDensity - rho - c.dt * (sF + sB + sR);
+        const float cx = cxF * c.cTermFacF + (cxB + cxR) * c.cTermFacB;
+        const float cy = cyF * c.cTermFacF + (cyB + cyR) * c.cTermFacB;
+        const float cz = czF * c.cTermFacF + (czB + czR) * c.cTermFacB;
+        const float dA = c.massF * fmaf(cx, cxF, fmaf(cy, cyF, cz * czF));
+        const float dB = c.massF * c.diagBFac * g2;
+        const float dC = fmaf(cx, cxB + cxR, fmaf(cy, cyB + cyR, cz * (czB + czR)));
+        const float diag = c.dt2 * (dA + dB + dC);
+        const bool valid = fabsf(diag) > 1e-7f;
+        const float cold = c.omega * (src / diag);
+        const float prev = c.warm ? pi.w : 0.0f;
+        const float init = c.warm ? ((prev > 0.0f) ? c.warmStart * prev : cold) : cold;
+        f.srcDiag[i] = make_float2(src, diag);
+        reinterpret_cast<float*>(f.posP)[4ull * i + 3] = fmaxf(0.0f, valid ? init : 0.0f);
     }
-    if (!act) return;
-    sF *= c.massF;
-    const float rho = f.velRho[i].w;
-    const float src = c.restDensity - rho - c.dt * (sF + sB + sR);
-    const float cx = cxF * c.cTermFacF + (cxB + cxR) * c.cTermFacB;
-    const float cy = cyF * c.cTermFacF + (cyB + cyR) * c.cTermFacB;
-    const float cz = czF * c.cTermFacF + (czB + czR) * c.cTermFacB;
-    const float dA = c.massF * fmaf(cx, cxF, fmaf(cy, cyF, cz * czF));
-    const float dB = c.massF * c.diagBFac * g2;
-    const float dC = fmaf(cx, cxB + cxR, fmaf(cy, cyB + cyR, cz * (czB + czR)));
-    const float diag = c.dt2 * (dA + dB + dC);
-    const bool valid = fabsf(diag) > 1e-7f;
-    const float cold = c.omega * (src / diag);
-    const float prev = c.warm ? pi.w : 0.0f;
-    const float init = c.warm ? ((prev > 0.0f) ? c.warmStart * prev : cold) : cold;
-    f.srcDiag[i] = make_float2(src, diag);
-    reinterpret_cast<float*>(f.posP)[4ull * i + 3] = fmaxf(0.0f, valid ? init : 0.0f);
 }
 
 // ----------------------------------------------------------------------------- pressure acceleration
-__global__ void __launch_bounds__(SPH_THREADS) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+__global__ void __launch_bounds__(SPH_THREADS, 4) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
-    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
-    const uint32_t chunk = i >> 5, lane = i & 31;
-    if (chunk * SELL_W >= f.n) return;
-    const bool act = i < f.n;
-    const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float fOuter = c.massF * pi.w * c.densInvSqu;
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    ChunkCursor cur;
-    cur.load(nv.ff, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const float4 pj = f.posP[cur.nbr(nv.ff, k, lane)];
+    FOR_EACH_CHUNK(f.n) {
+        const uint32_t i = chunk * SELL_W + lane;
+        const bool act = i < f.n;
+        const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float fOuter = c.massF * pi.w * c.densInvSqu;
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        ChunkCursor cur;
+        cur.load(nv.ff, chunk, i, act);
+        SweepSlotsKg<4, false>(cur, nv.ff, lane, f.posP, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
             const float a = (fOuter + c.massF * pj.w * c.densInvSqu) * kg;
             ax = fmaf(a, dx, ax); ay = fmaf(a, dy, ay); az = fmaf(a, dz, az);
-        }
-    }
-    cur.load(nv.fb, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const float4 pj = b.pos[cur.nbr(nv.fb, k, lane)];
+        });
+        cur.load(nv.fb, chunk, i, act);
+        SweepSlotsKg<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float a = c.accCoeffB * pj.w * pi.w;
             ax = fmaf(a, gx, ax); ay = fmaf(a, gy, ay); az = fmaf(a, gz, az);
-        }
-    }
-    cur.load(nv.fr, chunk, i, act);
-    for (uint32_t k = 0; k < cur.pitch; k++) {
-        if (k < cur.cnt) {
-            const float4 pj = r.pos[cur.nbr(nv.fr, k, lane)];
+        });
+        cur.load(nv.fr, chunk, i, act);
+        SweepSlotsKg<2, false>(cur, nv.fr, lane, r.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float a = c.accCoeffB * pj.w * pi.w;
             ax = fmaf(a, gx, ax); ay = fmaf(a, gy, ay); az = fmaf(a, gz, az);
-        }
+        });
+        if (act) f.acc[i] = make_float4(0.0f - ax, 0.0f - ay, 0.0f - az, 0.0f);
     }
-    if (act) f.acc[i] = make_float4(0.0f - ax, 0.0f - ay, 0.0f - az, 0.0f);
 }
 
 // ----------------------------------------------------------------------------- relaxed Jacobi sweep
@@ -262,54 +284,39 @@ __device__ __forceinline__ bool Terminated(const SolverControl& ctl, uint32_t it
     }
 }
 
-__global__ void __launch_bounds__(SPH_THREADS) KJacobi(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv,
+__global__ void __launch_bounds__(SPH_THREADS, 4) KJacobi(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv,
                                                     SolverControl ctl, SolverState* st, double* partials,
                                                     cudaGraphConditionalHandle cond, int hasCond) {
-    const uint32_t i = blockIdx.x * SPH_THREADS + threadIdx.x;
-    const uint32_t chunk = i >> 5, lane = i & 31;
-    const bool act = i < f.n;
-    double eRaw = 0.0, ePos = 0.0, eAbs = 0.0;
-    if (chunk * SELL_W < f.n) {
+    double eRaw = 0.0, ePos = 0.0, eAbs = 0.0;  // per-lane FP64 sums over the warp's chunks
+    FOR_EACH_CHUNK(f.n) {
+        const uint32_t i = chunk * SELL_W + lane;
+        const bool act = i < f.n;
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 ai = act ? f.acc[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         float sF = 0.f, sB = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        for (uint32_t k = 0; k < cur.pitch; k++) {
-            if (k < cur.cnt) {
-                const uint32_t j = cur.nbr(nv.ff, k, lane);
-                const float4 pj = f.posP[j];
-                const float4 aj = f.acc[j];
-                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
-                const float dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
-                const float sv = fmaf(dax, dx, fmaf(day, dy, daz * dz));
-                sF = fmaf(kg, sv, sF);
-            }
-        }
+        SweepSlotsKg<4, true>(cur, nv.ff, lane, f.posP, f.acc, [&](float kg, const float4& pj, const float4& aj) {
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
+            const float sv = fmaf(dax, dx, fmaf(day, dy, daz * dz));
+            sF = fmaf(kg, sv, sF);
+        });
         sF *= c.massF;
         cur.load(nv.fb, chunk, i, act);
-        for (uint32_t k = 0; k < cur.pitch; k++) {
-            if (k < cur.cnt) {
-                const float4 pj = b.pos[cur.nbr(nv.fb, k, lane)];
-                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
-                const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
-                const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
-                sB = sB + pj.w * sv;
-            }
-        }
+        SweepSlotsKg<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+            const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
+            sB = sB + pj.w * sv;
+        });
         cur.load(nv.fr, chunk, i, act);
-        for (uint32_t k = 0; k < cur.pitch; k++) {
-            if (k < cur.cnt) {
-                const float4 pj = r.pos[cur.nbr(nv.fr, k, lane)];
-                const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-                const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
-                const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
-                const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
-                sB = sB + pj.w * sv;
-            }
-        }
+        SweepSlotsKg<2, false>(cur, nv.fr, lane, r.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
+            const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
+            sB = sB + pj.w * sv;
+        });
         if (act) {
             const float2 sd = f.srcDiag[i];
             const float sys = c.dt2 * (sF + sB);
@@ -320,9 +327,9 @@ __global__ void __launch_bounds__(SPH_THREADS) KJacobi(Consts c, FluidDev f, Bou
             reinterpret_cast<float*>(f.posP)[4ull * i + 3] = pn;
             if (valid) {
                 const double re = (double)(err / c.restDensity);
-                eRaw = re;
-                ePos = re > 0.0 ? re : 0.0;
-                eAbs = fabs(re);
+                eRaw += re;
+                ePos += re > 0.0 ? re : 0.0;
+                eAbs += fabs(re);
             }
         }
     }
@@ -389,6 +396,33 @@ __global__ void __launch_bounds__(SPH_THREADS) KJacobi(Consts c, FluidDev f, Bou
     if (hasCond) cudaGraphSetConditional(cond, done ? 0u : 1u);
 }
 
+// records the per-slot kernel-gradient factors of the current positions (the values the
+// source / diagonal stage records), for stage-level runs after positions were rewritten
+__global__ void __launch_bounds__(SPH_THREADS) KGradFactors(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+                                                         NeighborView nv) {
+    FOR_EACH_CHUNK(f.n) {
+        const uint32_t i = chunk * SELL_W + lane;
+        const bool act = i < f.n;
+        const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        ChunkCursor cur;
+        cur.load(nv.ff, chunk, i, act);
+        SweepSlots<4, false>(cur, nv.ff, lane, f.posP, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            *cur.kgSlot(nv.ff, k, lane) = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+        });
+        cur.load(nv.fb, chunk, i, act);
+        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            *cur.kgSlot(nv.fb, k, lane) = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+        });
+        cur.load(nv.fr, chunk, i, act);
+        SweepSlots<2, false>(cur, nv.fr, lane, r.pos, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            *cur.kgSlot(nv.fr, k, lane) = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
+        });
+    }
+}
+
 __global__ void KSolverReset(SolverState* st, uint32_t nF) {
     st->iters = nF > 0 ? 1u : 0u;
     st->avg[0] = st->avg[1] = st->avg[2] = 0.0f;
@@ -453,32 +487,52 @@ __global__ void __launch_bounds__(256) KBoundaryVolumes(Consts c, const float4* 
 }
 
 // ----------------------------------------------------------------------------- launchers
+// persistent grids: at most (resident blocks per SM) x (SMs) blocks, never more than the chunks need
+static uint32_t g_numSMs = 0;
+template <typename K>
+static uint32_t PersistentBlocks(K kernel, uint32_t n) {
+    if (g_numSMs == 0) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g_numSMs = sms > 0 ? (uint32_t)sms : 148u;
+    }
+    int perSM = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, SPH_THREADS, 0);
+    if (perSM <= 0) perSM = 1;
+    const uint32_t need = (n + SPH_THREADS - 1) / SPH_THREADS;
+    return std::max(1u, std::min(need, (uint32_t)perSM * g_numSMs));
+}
 static inline uint32_t SphBlocks(uint32_t n) { return (n + SPH_THREADS - 1) / SPH_THREADS; }
 uint32_t JacobiBlocks(uint32_t nF) { return SphBlocks(nF); }
 
 void LaunchDensity(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
                    cudaStream_t s) {
-    if (f.n) KDensity<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+    if (f.n) KDensity<<<PersistentBlocks(KDensity, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
 }
 void LaunchNonPressure(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
                        const NeighborView& nv, cudaStream_t s) {
-    if (f.n) KNonPressure<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+    if (f.n) KNonPressure<<<PersistentBlocks(KNonPressure, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
 }
 void LaunchSourceDiagInit(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
                           const NeighborView& nv, SolverState* st, cudaStream_t s) {
-    if (f.n) KSourceDiagInit<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+    if (f.n) KSourceDiagInit<<<PersistentBlocks(KSourceDiagInit, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
     KSolverReset<<<1, 1, 0, s>>>(st, f.n);
 }
 void LaunchSolverReset(SolverState* st, uint32_t nF, cudaStream_t s) { KSolverReset<<<1, 1, 0, s>>>(st, nF); }
+void LaunchGradFactors(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
+                       const NeighborView& nv, cudaStream_t s) {
+    if (f.n) KGradFactors<<<PersistentBlocks(KGradFactors, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+}
 void LaunchPressureAcc(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
                        const NeighborView& nv, cudaStream_t s) {
-    if (f.n) KPressureAcc<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+    if (f.n) KPressureAcc<<<PersistentBlocks(KPressureAcc, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
 }
 void LaunchJacobi(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
                   const SolverControl& ctl, SolverState* st, double* partials, unsigned long long cond, bool hasCond,
                   cudaStream_t s) {
     if (f.n)
-        KJacobi<<<SphBlocks(f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv, ctl, st, partials,
+        KJacobi<<<PersistentBlocks(KJacobi, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv, ctl, st, partials,
                                                       (cudaGraphConditionalHandle)cond, hasCond ? 1 : 0);
 }
 void LaunchIntegration(const Consts& c, const FluidDev& f, cudaStream_t s) {
