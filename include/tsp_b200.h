@@ -241,6 +241,14 @@ int tsp_b200_get_stream(const tsp_backend* h, void** stream);
 /* number of CUDA kernels this backend launched since creation (graph nodes included) */
 int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count);
 
+/* ---- host helpers (no GPU work) -------------------------------------------------------- */
+/* Sim::TryBuildCellCoordFrame (source/simulation/core/cell_frame.h:32-66): inclusive signed
+ * cell bounds -> frame origin and dimensions. Fails with TSP_ERR_FRAME, leaving origin/dims
+ * untouched, if any axis has min > max, a bound outside int32, or more than 2^21 cells. The
+ * neighbor search builds its frame with this rule (UpdateCellFrame, neighbor_search.cpp:1902). */
+int tsp_b200_try_build_cell_frame(const int64_t cell_min[3], const int64_t cell_max[3], int32_t origin[3],
+                                  uint32_t dims[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -57,3 +57,47 @@ def test_null_handle_is_rejected_without_gpu(lib):
     lib.tsp_b200_last_error.restype = C.c_char_p
     lib.tsp_b200_last_error.argtypes = [C.c_void_p]
     assert b"NULL" in lib.tsp_b200_last_error(None)
+
+
+# ---- cell frame rule (tests/unit/cell_frame.cpp of the reference, through the C ABI)
+def _frame(lib_abi, lo, hi, orig=(4, 5, 6), dims=(7, 8, 9)):
+    o = (C.c_int32 * 3)(*orig)
+    d = (C.c_uint32 * 3)(*dims)
+    rc = lib_abi.tsp_b200_try_build_cell_frame((C.c_int64 * 3)(*lo), (C.c_int64 * 3)(*hi), o, d)
+    return rc, tuple(o), tuple(d)
+
+
+@pytest.fixture(scope="module")
+def lib_abi():
+    if not os.path.exists(abi.LIB_PATH):
+        from turbospharticles_b200 import build
+        build.build()
+    return abi.load_library()
+
+
+def test_cell_frame_inclusive_signed_bounds(lib_abi):
+    rc, o, d = _frame(lib_abi, (-3, 5, -7), (1, 6, -7))
+    assert rc == 0 and o == (-3, 5, -7) and d == (5, 2, 1)
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_cell_frame_maximum_axis_extent(lib_abi, axis):
+    hi = [0, 0, 0]
+    hi[axis] = 2_097_151
+    rc, o, d = _frame(lib_abi, (0, 0, 0), hi)
+    want = [1, 1, 1]
+    want[axis] = 2_097_152
+    assert rc == 0 and d == tuple(want)
+
+
+@pytest.mark.parametrize("b", [
+    (1, 0, 0, 0, 0, 0), (0, 1, 0, 0, 0, 0), (0, 0, 1, 0, 0, 0),
+    (-2_147_483_649, 0, 0, -2_147_483_649, 0, 0), (0, -2_147_483_649, 0, 0, -2_147_483_649, 0),
+    (0, 0, -2_147_483_649, 0, 0, -2_147_483_649),
+    (2_147_483_648, 0, 0, 2_147_483_648, 0, 0), (0, 2_147_483_648, 0, 0, 2_147_483_648, 0),
+    (0, 0, 2_147_483_648, 0, 0, 2_147_483_648),
+    (0, 0, 0, 2_097_152, 0, 0), (0, 0, 0, 0, 2_097_152, 0), (0, 0, 0, 0, 0, 2_097_152)])
+def test_cell_frame_invalid_bounds_preserve_frame(lib_abi, b):
+    rc, o, d = _frame(lib_abi, b[:3], b[3:])
+    assert rc == -4  # TSP_ERR_FRAME
+    assert o == (4, 5, 6) and d == (7, 8, 9)

@@ -128,6 +128,8 @@ EXPORTS = {
     "tsp_b200_time_stage": (C.c_int, [_VP, C.POINTER(TspParams), _u32, _u32, _pf]),
     "tsp_b200_get_launch_count": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
     "tsp_b200_get_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
+    "tsp_b200_try_build_cell_frame": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
+                                                 C.POINTER(C.c_uint32)]),
 }
 
 

@@ -109,6 +109,19 @@ static inline int HostFloorToInt(float v) {
     const int i = (int)v;
     return (v < (float)i) ? (i - 1) : i;
 }
+// TryBuildCellCoordFrame (source/simulation/core/cell_frame.h:32-66): inclusive signed cell
+// bounds -> origin + dimensions; every axis must have min <= max, both within int32, and at
+// most 2^21 cells. On failure the frame is left unchanged.
+static bool TryBuildCellFrame(const int64_t lo[3], const int64_t hi[3], int32_t& ox, int32_t& oy, int32_t& oz,
+                              uint32_t& nx, uint32_t& ny, uint32_t& nz) {
+    for (int a = 0; a < 3; a++)
+        if (lo[a] > hi[a] || lo[a] < (int64_t)INT32_MIN || hi[a] > (int64_t)INT32_MAX ||
+            hi[a] - lo[a] + 1 > (int64_t)(1u << 21))
+            return false;
+    ox = (int32_t)lo[0]; oy = (int32_t)lo[1]; oz = (int32_t)lo[2];
+    nx = (uint32_t)(hi[0] - lo[0] + 1); ny = (uint32_t)(hi[1] - lo[1] + 1); nz = (uint32_t)(hi[2] - lo[2] + 1);
+    return true;
+}
 static inline uint32_t HostKeyBits(uint32_t nx, uint32_t ny, uint32_t nz) {  // neighbor_search.cpp:403-413
     const uint32_t m = std::max(nx, std::max(ny, nz));
     uint32_t axisBits = 1;
@@ -580,11 +593,9 @@ public:
         for (int a = 0; a < 3; a++) {
             o[a] = (int64_t)HostFloorToInt(mn[a] * fr.cellSizeInv) - margin;
             e[a] = (int64_t)HostFloorToInt(mx[a] * fr.cellSizeInv) + margin;
-            if (o[a] > e[a] || o[a] < INT32_MIN || e[a] > INT32_MAX || e[a] - o[a] + 1 > (int64_t)(1u << 21))
-                throw Error(TSP_ERR_FRAME, "Compact CLL cell frame exceeds the supported range.");
         }
-        fr.ox = (int32_t)o[0]; fr.oy = (int32_t)o[1]; fr.oz = (int32_t)o[2];
-        fr.nx = (uint32_t)(e[0] - o[0] + 1); fr.ny = (uint32_t)(e[1] - o[1] + 1); fr.nz = (uint32_t)(e[2] - o[2] + 1);
+        if (!TryBuildCellFrame(o, e, fr.ox, fr.oy, fr.oz, fr.nx, fr.ny, fr.nz))
+            throw Error(TSP_ERR_FRAME, "Compact CLL cell frame exceeds the supported range.");
         fr.keyBits = HostKeyBits(fr.nx, fr.ny, fr.nz);
         frameValid = true;
         frameRebuilds++;
@@ -1171,6 +1182,18 @@ int tsp_b200_destroy(tsp_backend* h) {
     return TSP_OK;
 }
 const char* tsp_b200_name(const tsp_backend*) { return "B200 (sm_100a) IISPH"; }
+int tsp_b200_try_build_cell_frame(const int64_t cell_min[3], const int64_t cell_max[3], int32_t origin[3],
+                                  uint32_t dims[3]) {
+    if (!cell_min || !cell_max || !origin || !dims) return TSP_ERR_INVALID;
+    int32_t o[3] = {origin[0], origin[1], origin[2]};
+    uint32_t d[3] = {dims[0], dims[1], dims[2]};
+    if (!tsp::TryBuildCellFrame(cell_min, cell_max, o[0], o[1], o[2], d[0], d[1], d[2])) {
+        g_lastError = "Compact CLL cell frame exceeds the supported range.";
+        return TSP_ERR_FRAME;
+    }
+    for (int a = 0; a < 3; a++) { origin[a] = o[a]; dims[a] = d[a]; }
+    return TSP_OK;
+}
 const char* tsp_b200_last_error(const tsp_backend* h) {
     return (h && h->b) ? h->b->lastErr.c_str() : g_lastError.c_str();
 }

@@ -235,10 +235,15 @@ def rigid_hollow_box(box: OBB, p: SimParams, density: float):
 
 def breaking_dam(container: OBB, fluid: OBB, p: SimParams, rigid=None):
     """BreakingDamScene::Build (source/simulation/scene/scenarios/breaking_dam.h:40-45):
-    container walls first, then the fluid block; optional hollow rigid boxes
+    container walls first, then the fluid block (or a list of blocks, IDs consecutive);
+    optional hollow rigid boxes
     [(OBB, density), ...]. Returns (state, domain_min, domain_max)."""
     idB, xB, yB, zB = boundary_container(container, p)
-    idF, xF, yF, zF = fluid_block(fluid, p)
+    parts, base = [], 0
+    for box in (fluid if isinstance(fluid, (list, tuple)) else [fluid]):
+        parts.append(fluid_block(box, p, id_base=base))
+        base += parts[-1][0].shape[0]
+    idF, xF, yF, zF = (np.concatenate([q[c] for q in parts]) for c in range(4))
     bodies = []
     rel = [[], [], []]
     body_of = []
@@ -327,3 +332,70 @@ def neighbor_search_scene(n, distribution="uniform", seed=1):
     st = UniversalSimState(n, 0, 0, 0, p.restDensity)
     st.xPosF[:], st.yPosF[:], st.zPosF[:] = pts[:, 0], pts[:, 1], pts[:, 2]
     return st, np.zeros(3, f32), np.ones(3, f32), p
+
+
+def _rotation(rng):
+    """Seeded uniform random rotation (unit quaternion from three uniforms, Shoemake 1992)."""
+    u1, u2, u3 = rng.random(3)
+    a, b = math.sqrt(1.0 - u1), math.sqrt(u1)
+    qw, qx, qy, qz = a * math.sin(2 * math.pi * u2), a * math.cos(2 * math.pi * u2), \
+        b * math.sin(2 * math.pi * u3), b * math.cos(2 * math.pi * u3)
+    return np.array([
+        [1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qz * qw), 2 * (qx * qz + qy * qw)],
+        [2 * (qx * qy + qz * qw), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qx * qw)],
+        [2 * (qx * qz - qy * qw), 2 * (qy * qz + qx * qw), 1 - 2 * (qx * qx + qy * qy)]])
+
+
+def rigid_dam(block=(100, 125, 80), dx=0.008, tank=(4.0, 1.5, 1.5), cubes=8, edge=0.15, dt=4e-4, seed=7):
+    """Two-sided dam with floating hollow cubes: two fluid blocks of block[0] x block[1] x
+    block[2] lattice particles (spacing dx) in opposite corners of the tank, `cubes` hollow
+    rigid cubes (edge `edge`, 2 particle layers, BuildRigidBody_OBB_Hollow) at seeded positions
+    between the blocks with seeded random orientations; the first half of the cubes have
+    density 500 kg/m^3, the rest 2000 kg/m^3. Defaults: 2,000,000 fluid particles, 8 cubes
+    of 3,088 particles."""
+    from .params import dam_params
+    p = dam_params(dx, dt)
+    p.jitterFracF = 0.01
+    p.jitterSeedF = seed
+    ext = [(n + 0.5) * dx for n in block]  # n lattice sites per axis, robust to FP32 rounding
+    container = OBB((0.0, 0.0, 0.0), tuple(tank))
+    fluids = [OBB((0.0, 0.0, 0.0), tuple(ext)),
+              OBB((tank[0] - ext[0], 0.0, tank[2] - ext[2]), tuple(ext))]
+    rng = np.random.default_rng(seed)
+    gap = (ext[0] + edge, tank[0] - ext[0] - edge)
+    cols = max(1, (cubes + 1) // 2)
+    rigid = []
+    for k in range(cubes):
+        cx = gap[0] + (gap[1] - gap[0]) * (k % cols + 0.5) / cols
+        cz = tank[2] * (0.3 if k // cols == 0 else 0.7)
+        cy = edge + rng.random() * max(tank[1] * 0.5 - edge, 0.0)
+        R = _rotation(rng)
+        u, v, w = (tuple(float(x) for x in R[:, c]) for c in range(3))
+        origin = tuple(float(c) for c in np.array([cx, cy, cz]) - R @ np.full(3, 0.5 * edge))
+        rigid.append((OBB(origin, (edge, edge, edge), u, v, w), 500.0 if k < cubes // 2 else 2000.0))
+    st, dmin, dmax = breaking_dam(container, fluids, p, rigid)
+    return st, dmin, dmax, p
+
+
+def floating_cubes(seed=5, dx=0.03, dt=1e-3):
+    """Small rigid-coupling scene: a 30 x 10 x 20 fluid slab (spacing dx) in a 0.9 x 0.6 x 0.6 m
+    tank and two hollow cubes (edge 0.18 m, densities 500 and 2000 kg/m^3, seeded random
+    orientations) resting on its surface, so fluid-rigid forces act from the first step."""
+    from .params import dam_params
+    p = dam_params(dx, dt)
+    p.jitterFracF = 0.01
+    p.jitterSeedF = seed
+    container = OBB((0.0, 0.0, 0.0), (0.9, 0.6, 0.6))
+    top = (10 + 0.5) * dx
+    fluid = OBB((0.0, 0.0, 0.0), ((30 + 0.5) * dx, top, (20 + 0.5) * dx))
+    rng = np.random.default_rng(seed)
+    rigid = []
+    edge = 0.18
+    for cx, dens in ((0.25, 500.0), (0.62, 2000.0)):
+        R = _rotation(rng)
+        c = np.array([cx, top + 0.12, 0.3])
+        origin = tuple(float(x) for x in c - R @ np.full(3, 0.5 * edge))
+        axes = (tuple(float(x) for x in R[:, j]) for j in range(3))
+        rigid.append((OBB(origin, (edge, edge, edge), *axes), dens))
+    st, dmin, dmax = breaking_dam(container, fluid, p, rigid)
+    return st, dmin, dmax, p
