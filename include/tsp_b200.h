@@ -249,6 +249,37 @@ int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count);
 int tsp_b200_try_build_cell_frame(const int64_t cell_min[3], const int64_t cell_max[3], int32_t origin[3],
                                   uint32_t dims[3]);
 
+/* ---- cell-table build without device allocation ---------------------------------------
+ * No counterpart in the reference (its cell tables are built inside the backend's neighbor
+ * search, source/simulation/CPU/backend/neighbor_search.cpp). For callers that own their
+ * particle buffers and stream and must not allocate device memory on the way: a fixed-budget
+ * embedding, or a time-critical loop where cudaMalloc / cudaFree (which synchronises the
+ * device) would stall other work. The scan scratch is a fixed array inside this library
+ * (one per device, 128 KiB); no cudaMalloc, cudaFree or allocating library call is made.
+ *
+ * Input: n Morton cell IDs sorted ascending (device memory; out-of-frame particles carry
+ * 0xFFFFFFFFFFFFFFFF and sort last, as tsp_b200_read_cell_ids returns them). Output, all
+ * device memory: d_unique_out[c] = cell ID of run c (room for n), d_start_out[c] = index of
+ * the first particle of run c plus d_start_out[num_cells] = n (room for n + 1), and
+ * *d_num_cells_out = num_cells. Outputs need not be zeroed, and nothing has to start at zero.
+ * Work is queued on `stream` (a cudaStream_t; NULL = legacy default stream); results are
+ * ready when that stream reaches them.
+ *
+ * Setup: the first call on a device looks up the scratch's device address for that device
+ * (cudaGetSymbolAddress, which may load this library's device code there). Call
+ * tsp_b200_noalloc_setup() with each device current once during setup -- before any stream
+ * capture or time-critical section -- so later calls only launch kernels.
+ * Limit: n <= TSP_NOALLOC_MAX_PARTICLES; larger n returns TSP_ERR_INVALID and queues nothing.
+ * Races: all calls on one device share the scratch, so calls must not overlap in time on that
+ * device (issue them on one stream, or order them with events).
+ * Errors: TSP_ERR_INVALID / TSP_ERR_CUDA / TSP_ERR_NO_DEVICE; message from
+ * tsp_b200_noalloc_last_error() (per host thread). */
+#define TSP_NOALLOC_MAX_PARTICLES (1u << 24)
+int tsp_b200_noalloc_setup(void);
+int tsp_b200_build_cell_table_noalloc(const uint64_t* d_cell_ids_sorted, uint32_t n, uint64_t* d_unique_out,
+                                      uint32_t* d_start_out, uint64_t* d_num_cells_out, void* stream);
+const char* tsp_b200_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
