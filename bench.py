@@ -100,12 +100,17 @@ def measured_peak_hbm():
 
 
 def profiled_traffic():
-    p = os.path.join(ROOT, "profiles", "jacobi_dam_traffic.json")
+    """DRAM bytes (read + write) of one KJacobi launch on this workload, from the ncu summary
+    committed beside the kernel's profile (line `traffic_bytes_per_launch = N`)."""
+    p = os.path.join(ROOT, "profiles", "KJacobi_iisph_dam_1M.md")
     try:
         with open(p) as f:
-            return json.load(f)
-    except (OSError, ValueError):
-        return None
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch"):
+                    return {"bytes_per_launch_scaled": int(line.split("=")[1].strip().split()[0])}
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
 
 
 def build_workload(rank=0):
