@@ -156,7 +156,7 @@ def run_b200(args):
     l0 = be.launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    step_ms, iters = [], []
+    step_ms, iters, phases = [], [], []
     with ClockSampler(local) as clk:
         e0.record(stream)
         for _ in range(args.steps):
@@ -164,6 +164,7 @@ def run_b200(args):
             s = be.stats()
             step_ms.append(s.lastStepMs)
             iters.append(s.solverIters - 1)
+            phases.append(be.phase_times())
         e1.record(stream)
         torch.cuda.synchronize(dev)
     barrier(dist, dev)
@@ -235,6 +236,8 @@ def run_b200(args):
         "p50_step_ms": round(float(q[0]), 4), "p99_step_ms": round(float(q[1]), 4),
         "jacobi_sweeps": sweeps, "jacobi_iters_per_s": round(sweeps * ws / (elapsed_ms / 1e3), 1),
         "neighbor_ms_last": round(s.lastNeighborMs, 4), "jacobi_ms_last": round(s.lastJacobiMs, 4),
+        "phase_ms_p50": {k: round(float(np.median([ph[k] for ph in phases if k in ph])), 4)
+                         for k in (phases[-1] if phases else {})},
         "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
         "clocks": clk.summary(), "impl": "b200",
     }

@@ -238,6 +238,13 @@ int tsp_b200_time_stage(tsp_backend* h, const tsp_params* params, uint32_t stage
                         float* ms_per_launch);
 /* the cudaStream_t all work of this backend runs on (for events / ordering by the caller) */
 int tsp_b200_get_stream(const tsp_backend* h, void** stream);
+/* device time (ms, CUDA events) of the phases of the last step, in this order: frame update,
+ * sort + reorder + cell tables + grids, query count, finalize + size read-back, query fill,
+ * density, non-pressure (+ rigid viscous forces), source/diagonal/init, Jacobi loop, final
+ * pressure acceleration (+ rigid pressure forces), integration (+ rigid integration), stats
+ * read-back. *n = number written (0 before the first step). Analogue of the reference's
+ * per-stage BenchOp timers (source/simulation/core/backend_sim.h:255, GetBenchOps). */
+int tsp_b200_get_phase_times(const tsp_backend* h, float* ms, uint32_t cap, uint32_t* n);
 /* number of CUDA kernels this backend launched since creation (graph nodes included) */
 int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count);
 

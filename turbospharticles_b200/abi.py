@@ -22,6 +22,9 @@ TERM_FIXED_ITERS, TERM_REL_ERR_RAW, TERM_REL_ERR_POS, TERM_REL_ERR_ABS = 0, 1, 2
 SPECIES_F, SPECIES_B, SPECIES_R = 0, 1, 2
 LIST_FF, LIST_FB, LIST_FR, LIST_RF, LIST_RB, LIST_RR = range(6)
 NOALLOC_MAX_PARTICLES = 1 << 24  # TSP_NOALLOC_MAX_PARTICLES
+PHASE_NAMES = ("frame", "sort_reorder_tables", "query_count", "finalize_readback", "query_fill", "density",
+               "non_pressure", "source_diag_init", "jacobi_loop", "pressure_acc_final", "integration",
+               "stats_readback")
 STAGE_DENSITY, STAGE_NON_PRESSURE, STAGE_SOURCE_DIAG_INIT = 1, 2, 3
 STAGE_PRESSURE_ACC, STAGE_JACOBI_UPDATE, STAGE_INTEGRATION, STAGE_BOUNDARY_VOLUMES = 4, 5, 6, 7
 (FIELD_POS, FIELD_VEL, FIELD_VEL_PRED, FIELD_ACC_PRESS, FIELD_SOURCE, FIELD_DIAG, FIELD_PRESSURE,
@@ -129,6 +132,7 @@ EXPORTS = {
     "tsp_b200_time_stage": (C.c_int, [_VP, C.POINTER(TspParams), _u32, _u32, _pf]),
     "tsp_b200_get_launch_count": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
     "tsp_b200_get_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
+    "tsp_b200_get_phase_times": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32)]),
     "tsp_b200_try_build_cell_frame": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                                  C.POINTER(C.c_uint32)]),
     "tsp_b200_noalloc_setup": (C.c_int, []),

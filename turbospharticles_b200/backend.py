@@ -183,6 +183,13 @@ class SimBackendB200:
         self._chk(self.L.tsp_b200_time_stage(self.h, self._cparams(params), stage, reps, C.byref(ms)))
         return ms.value
 
+    def phase_times(self) -> dict:
+        """Device milliseconds of the phases of the last step (empty before the first step)."""
+        buf = (C.c_float * len(abi.PHASE_NAMES))()
+        n = C.c_uint32()
+        self._chk(self.L.tsp_b200_get_phase_times(self.h, buf, len(abi.PHASE_NAMES), C.byref(n)))
+        return {abi.PHASE_NAMES[k]: float(buf[k]) for k in range(n.value)}
+
     def launch_count(self) -> int:
         n = C.c_uint64()
         self._chk(self.L.tsp_b200_get_launch_count(self.h, C.byref(n)))

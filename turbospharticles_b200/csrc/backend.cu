@@ -233,10 +233,11 @@ public:
     bool kgValid = false;  // the recorded factors belong to the current positions and lists
     DBuf<U64x2> sellTot;
     DBuf<unsigned long long> nbrTot;
-    // count-pass hit-mask record replayed by the fill pass (scratch, DICT_CAP entries per chunk)
-    static constexpr uint32_t DICT_CAP = 512;
-    DBuf<uint2> dict;
-    DBuf<uint32_t> dictCount;
+    // count-pass rows of the fluid query ([chunk][slot][lane]); rows longer than KS_* slots make
+    // the fill walk that chunk's stencil again
+    static constexpr uint32_t KS_F = 64, KS_B = 48, KS_R = 16;
+    DBuf<uint32_t> scrF, scrB, scrR;
+    DBuf<uint8_t> scrOver;
     uint64_t nNbr[3] = {0, 0, 0};
     DBuf<uint16_t> cntR[3];
     DBuf<uint64_t> offR[3];
@@ -259,6 +260,14 @@ public:
     DBuf<float> stage;  // device staging of the SoA <-> packed conversions at the state boundary (grow-only)
     size_t graphNext = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // phase boundaries of the last step: 0 start, 1 frame, 2 sort/reorder/cell tables/grids,
+    // 3 query count, 4 finalize + size read-back, 5 query fill (= neighbor build end),
+    // 6 density, 7 non-pressure (+ rigid viscous forces), 8 source/diagonal/init,
+    // 9 Jacobi loop, 10 final pressure acceleration (+ rigid pressure forces), 11 integration
+    // (+ rigid integration), 12 end
+    static constexpr int N_PHASE_EVENTS = 13;
+    cudaEvent_t pev[N_PHASE_EVENTS] = {};
+    bool phaseValid = false;
     float lastStepMs = 0.f, lastNbrMs = 0.f, lastJacMs = 0.f;
     std::string lastErr;
     uint64_t launches = 0;  // kernels launched by this backend (graph nodes included)
@@ -284,6 +293,7 @@ public:
         CK(cudaMemset(st.p, 0, sizeof(SolverState)));
         CK(cudaMemset(err.p, 0, sizeof(uint32_t)));
         for (auto& e : ev) CK(cudaEventCreate(&e));
+        for (auto& e : pev) CK(cudaEventCreate(&e));
     }
     ~Backend() {
         cudaSetDevice(device);
@@ -293,6 +303,7 @@ public:
             if (g.g) cudaGraphDestroy(g.g);
         }
         for (auto& e : ev) if (e) cudaEventDestroy(e);
+        for (auto& e : pev) if (e) cudaEventDestroy(e);
         if (hm) cudaFreeHost(hm);
         if (capStream) cudaStreamDestroy(capStream);
         if (s) cudaStreamDestroy(s);
@@ -542,6 +553,8 @@ public:
         const float span = zero ? 0.0f : (prm.kernelRadius / cs);
         const uint32_t r = zero ? 1u : std::max<uint32_t>(1u, (uint32_t)std::ceil(std::max(0.0f, span - 1e-6f)));
         if (std::fabs(cellSize - cs) > 1e-7f || reach != r) { frameValid = false; bSortedForFrame = false; }
+        if (QuerySmemBytes(r) > 227u * 1024u)
+            throw Error(TSP_ERR_UNSUPPORTED, "cell size ratio too small: query stencil exceeds shared memory");
         cellSize = cs;
         reach = r;
         fr.cellSizeInv = zero ? 0.0f : 1.0f / cs;
@@ -634,13 +647,17 @@ public:
         }
         velPred2.ensure(std::max<uint32_t>(nF, 1)); acc2.ensure(std::max<uint32_t>(nF, 1));
         srcDiag2.ensure(std::max<uint32_t>(nF, 1));
-        dict.ensure((size_t)std::max<uint32_t>(nChunks, 1) * DICT_CAP);
-        dictCount.ensure(std::max<uint32_t>(nChunks, 1));
+        scrF.ensure(std::max<size_t>(QueryScratchWords(nChunks, KS_F), 1));
+        scrB.ensure(std::max<size_t>(QueryScratchWords(nChunks, KS_B), 1));
+        scrR.ensure(std::max<size_t>(QueryScratchWords(nChunks, nR ? KS_R : 0), 1));
+        scrOver.ensure(std::max<uint32_t>(nChunks, 1));
     }
     // ReOrderParticleData + Construct + Query_Count + Finalize_Count + Query_Fill
     void NeighborBuild(bool permuteAll) {
         SetCellSize();
+        CK(cudaEventRecord(pev[0], s));
         const bool frameChanged = UpdateFrame();
+        CK(cudaEventRecord(pev[1], s));
         if (!frameValid) { listsValid = false; return; }
         EnsureNsScratch();
         SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p};
@@ -687,9 +704,11 @@ public:
         QueryArgs qa = MakeQueryArgs();
         SellMeta m0 = Meta(0), m1 = Meta(1), m2 = Meta(2);
         RigidLists rl = RLists();
+        CK(cudaEventRecord(pev[2], s));
         CK(cudaMemsetAsync(nbrTot.p, 0, 3 * sizeof(unsigned long long), s));
         LaunchQueryFluid(false, qa, m0, m1, m2, s);
         LaunchQueryRigid(false, qa, rl, s);
+        CK(cudaEventRecord(pev[3], s));
         const uint32_t nChunks = (nF + SELL_W - 1) / SELL_W;
         for (int k = 0; k < 3; k++) FinalizeSell(Meta(k), nChunks, scanScratch2.p, sellTot.p + k, s);
         for (int k = 0; k < 3; k++) FinalizeCsr(cntR[k].p, offR[k].p, nR, scanScratch.p, csrTot.p + k, s);
@@ -697,6 +716,7 @@ public:
         CK(cudaMemcpyAsync(hm->csrTot, csrTot.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(hm->nCells, nCellsDev.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(hm->nbrTot, nbrTot.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        CK(cudaEventRecord(pev[4], s));
         Sync();
         for (int k = 0; k < 3; k++) {
             nNbr[k] = nF ? hm->nbrTot[k] : 0;
@@ -713,6 +733,7 @@ public:
         rl = RLists();
         LaunchQueryFluid(true, qa, m0, m1, m2, s);
         LaunchQueryRigid(true, qa, rl, s);
+        CK(cudaEventRecord(pev[5], s));
         kgValid = false;
         launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + (nF ? 9u : 0u) + (nR ? 9u : 0u);
         listsValid = true;
@@ -724,9 +745,11 @@ public:
         qa.posR = posR.p; qa.permR = permR.p; qa.bodyR = bodyR.p; qa.nR = nR;
         qa.startF = startF.p; qa.startB = startB.p; qa.startR = startR.p;
         qa.gridF = nF ? gridF.p : nullptr; qa.gridB = nB ? gridB.p : nullptr; qa.gridR = nR ? gridR.p : nullptr;
-        qa.fr = fr; qa.r2 = prm.kernelRadiusSqu; qa.cap = QueryCap(reach); qa.err = err.p;
+        qa.fr = fr; qa.r2 = prm.kernelRadiusSqu; qa.err = err.p;
         qa.nbrTotals = nbrTot.p;
-        qa.dict = dict.p; qa.dictCount = dictCount.p; qa.dictCap = DICT_CAP;
+        qa.scrF = scrF.p; qa.scrB = scrB.p; qa.scrR = scrR.p;
+        qa.ksF = KS_F; qa.ksB = KS_B; qa.ksR = nR ? KS_R : 0u;
+        qa.scrOver = scrOver.p;
         return qa;
     }
     RigidLists RLists() {
@@ -805,6 +828,7 @@ public:
             throw Error(TSP_ERR_INVALID, "time step, particle size and kernel radius must be positive");
         if (nF == 0 && nRB == 0) return;  // empty serial sim (cpu_backend.cpp:2309-2315)
         const Consts c = MakeConsts(prm);
+        phaseValid = false;
         CK(cudaEventRecord(ev[0], s));
         NeighborBuild(false);
         CK(cudaEventRecord(ev[1], s));
@@ -812,6 +836,7 @@ public:
         RigidParticlesDev rp = RigidView(); BodyDev bd = BodyView();
         LaunchDensity(c, f, b, r, nv, s);
         if (nRB) LaunchRigidClearAddGravity(bd, prm.gravity[0], prm.gravity[1], prm.gravity[2], s);
+        CK(cudaEventRecord(pev[6], s));
         LaunchNonPressure(c, f, b, r, nv, s);
         if (nRB) {
             LaunchRigidViscousForces(c, rp, f, offR[0].p, listR[0].p, s);
@@ -819,9 +844,11 @@ public:
             LaunchRigidPredict(bd, prm.timeStep, s);
             LaunchRigidUpdateParticles(rp, bd, true, err.p, s);
         }
+        CK(cudaEventRecord(pev[7], s));
         LaunchSourceDiagInit(c, f, b, r, nv, st.p, s);
         kgValid = true;
         CK(cudaEventRecord(ev[2], s));
+        CK(cudaEventRecord(pev[8], s));
         if (nF) {
             partials.ensure(3ull * JacobiBlocks(nF) + 3);
             const SolverControl ctl = Control();
@@ -829,12 +856,14 @@ public:
             CK(cudaGraphLaunch(ex, s));
         }
         CK(cudaEventRecord(ev[3], s));
+        CK(cudaEventRecord(pev[9], s));
         LaunchPressureAcc(c, f, b, r, nv, s);
         if (nRB) {
             LaunchRigidPressureForces(c, rp, f, offR[0].p, listR[0].p, s);
             LaunchRigidClearAddGravity(bd, prm.gravity[0], prm.gravity[1], prm.gravity[2], s);
             LaunchRigidReduce(rp, bd, s);
         }
+        CK(cudaEventRecord(pev[10], s));
         LaunchIntegration(c, f, s);
         kgValid = false;
         if (nRB) {
@@ -842,18 +871,29 @@ public:
             LaunchRigidIntegrate(bd, prm.timeStep, err.p, s);
             LaunchRigidUpdateParticles(rp, bd, false, err.p, s);
         }
+        CK(cudaEventRecord(pev[11], s));
         CK(cudaMemcpyAsync(&hm->st, st.p, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
         launches += (nF ? 6u : 0u) + (nRB ? 13u : 0u);
-        cudaEvent_t evEnd;
-        CK(cudaEventCreate(&evEnd));
-        CK(cudaEventRecord(evEnd, s));
+        CK(cudaEventRecord(pev[12], s));
         CheckErrors();
         float t = 0.f;
-        cudaEventElapsedTime(&t, ev[0], evEnd); lastStepMs = t;
+        cudaEventElapsedTime(&t, ev[0], pev[12]); lastStepMs = t;
         cudaEventElapsedTime(&t, ev[0], ev[1]); lastNbrMs = t;
         cudaEventElapsedTime(&t, ev[2], ev[3]); lastJacMs = t;
-        cudaEventDestroy(evEnd);
+        phaseValid = listsValid;
         if (nF && hm->st.iters > 0) launches += 2ull * (hm->st.iters - 1u);
+    }
+
+    // device milliseconds between consecutive phase events of the last completed step
+    uint32_t PhaseTimes(float* ms, uint32_t cap) {
+        if (!phaseValid) return 0;
+        const uint32_t n = std::min<uint32_t>(cap, N_PHASE_EVENTS - 1);
+        for (uint32_t k = 0; k < n; k++) {
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, pev[k], pev[k + 1]));
+            ms[k] = t;
+        }
+        return n;
     }
 
     void NeighborSearchStandalone(const tsp_params& p) {  // ExecuteNeighborSearch (cpu_backend.cpp:1593-1624)
@@ -1406,6 +1446,12 @@ int tsp_b200_get_stream(const tsp_backend* h, void** stream) {
     if (!stream) return TSP_ERR_INVALID;
     *stream = (void*)h->b->s;
     return TSP_OK;
+}
+int tsp_b200_get_phase_times(const tsp_backend* h, float* ms, uint32_t cap, uint32_t* n) {
+    TSP_NEED(h);
+    if (!n || (cap && !ms)) return TSP_ERR_INVALID;
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, *n = hh->b->PhaseTimes(ms, cap));
 }
 int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count) {
     TSP_NEED(h);

@@ -60,12 +60,13 @@ struct QueryArgs {
     const uint32_t *gridF, *gridB, *gridR;  // NULL when the species is absent
     Frame fr;
     float r2;
-    uint32_t cap;
     uint32_t* err;
     unsigned long long* nbrTotals;  // FF, FB, FR neighbor totals (accumulated by the count pass)
-    uint2* dict;                    // per-chunk hit-mask record of the count pass (NULL: fill re-sweeps)
-    uint32_t* dictCount;            // entries per chunk, EMPTY_32 when the record overflowed
-    uint32_t dictCap;               // entries per chunk
+    // count-pass rows per chunk in [slot][lane] layout, ks* slots per lane; a chunk with a
+    // longer row sets its bit in scrOver (1 FF, 2 FB, 4 FR) and the fill walks it again
+    uint32_t *scrF, *scrB, *scrR;
+    uint32_t ksF, ksB, ksR;
+    uint8_t* scrOver;
 };
 
 struct RigidLists {
@@ -144,6 +145,8 @@ void BuildCellTable(const uint64_t* cidSorted, uint32_t n, uint64_t* unique, uin
 void BuildGrid(const uint64_t* unique, const uint64_t* nCellsDev, uint32_t nMax, const Frame& fr, uint32_t* grid,
                uint64_t gridCells, cudaStream_t s);
 uint32_t QueryCap(uint32_t reach);
+size_t QueryScratchWords(uint32_t nChunks, uint32_t ks);
+size_t QuerySmemBytes(uint32_t reach);  // dynamic shared memory of one fluid-query block
 void LaunchQueryFluid(bool fill, const QueryArgs& a, const SellMeta& ff, const SellMeta& fb, const SellMeta& fr,
                       cudaStream_t s);
 void LaunchQueryRigid(bool fill, const QueryArgs& a, const RigidLists& L, cudaStream_t s);

@@ -12,10 +12,12 @@
 //   KReorder*       gather the SoA fields through the permutation, sorted cell IDs
 //   cell table      run starts of the sorted cell IDs (device scan), count stays on device
 //   KGridScatter    dense frame grid: linear cell coordinate -> compact cell index
-//   KQueryFluid     one warp per SELL32 chunk (32 consecutive sorted fluid particles):
-//                   stencil cells of the chunk staged in shared memory and sorted by
-//                   Morton ID, so every lane's neighbors arrive in ascending index order;
-//                   warp-uniform candidate sweep (broadcast loads), per-lane hit test
+//   KQueryFluid*    one warp per SELL32 chunk (32 consecutive sorted fluid particles):
+//                   each lane walks only its own strict stencil, whose non-empty cell
+//                   ranges are looked up once per distinct cell of the chunk and ranked by
+//                   first index (= Morton order), so rows arrive in ascending index order.
+//                   The count pass keeps each row in a [slot][lane] scratch; the fill pass
+//                   encodes the scratch into the SELL32 slices (same layout, coalesced)
 //   KQueryRigid     one thread per rigid particle, CSR rows (RF, RB, RR)
 #include "kernels.h"
 #include "primitives.cuh"
@@ -280,108 +282,9 @@ struct LaneWriter {
     }
 };
 
-__device__ __forceinline__ void WarpBitonicSort(uint64_t* v, uint32_t S, uint32_t lane) {
-    for (uint32_t k = 2; k <= S; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            for (uint32_t t = lane; t < S; t += 32) {
-                const uint32_t p = t ^ j;
-                if (p > t) {
-                    const uint64_t a = v[t], b = v[p];
-                    const bool up = (t & k) == 0;
-                    if ((a > b) == up) { v[t] = b; v[p] = a; }
-                }
-            }
-            __syncwarp();
-        }
-    }
-}
-
-// per-warp record of the count pass: (candidate | species << 30, 32-lane hit mask) for every
-// candidate that is a neighbor of at least one lane, in sweep order, staged 32 entries per
-// coalesced 256 B store; the fill pass replays it instead of repeating the candidate sweep
-struct DictRec {
-    uint2* base;
-    uint32_t n, cap;
-    uint32_t pj, pm;
-    bool ok;
-    __device__ __forceinline__ void push(uint32_t tagged, uint32_t mask, uint32_t lane) {
-        if (n < cap) {
-            if (lane == (n & 31u)) { pj = tagged; pm = mask; }
-            if ((n & 31u) == 31u) base[(n & ~31u) + lane] = make_uint2(pj, pm);
-        }
-        n++;
-    }
-    __device__ __forceinline__ void finish(uint32_t lane) {
-        if (n <= cap && lane < (n & 31u)) base[(n & ~31u) + lane] = make_uint2(pj, pm);
-    }
-};
-
-struct QueryLane {
-    float4 pi;
-    int lx, ly, lz;
-    bool member;
-    uint32_t homeLo, homeHi;
-};
-
-// candidate sweep of one species over the group's sorted candidate cells (warp-uniform loop)
-template <int SP, bool FILL>
-__device__ __forceinline__ void SweepSpecies(const QueryArgs& a, const uint64_t* cells, uint32_t vol, const QueryLane& q,
-                                             uint32_t lane, LaneRefs& ref, LaneWriter& w, const SellMeta& m,
-                                             DictRec& dict) {
-    const uint32_t* grid = SP == 0 ? a.gridF : SP == 1 ? a.gridB : a.gridR;
-    const uint32_t* start = SP == 0 ? a.startF : SP == 1 ? a.startB : a.startR;
-    const float4* pos = SP == 0 ? a.posF : SP == 1 ? a.posB : a.posR;
-    if (grid == nullptr) return;
-    const int r = (int)a.fr.reach;
-    for (uint32_t cb = 0; cb < vol; cb += 32) {
-        const uint32_t t = cb + lane;
-        uint32_t b = 0, e = 0;
-        int cx = 0, cy = 0, cz = 0;
-        if (t < vol) {
-            const uint64_t mc = cells[t];
-            cx = (int)Compact21(mc); cy = (int)Compact21(mc >> 1); cz = (int)Compact21(mc >> 2);
-            const uint32_t c = grid[(uint64_t)cx + (uint64_t)a.fr.nx * ((uint64_t)cy + (uint64_t)a.fr.ny * cz)];
-            if (c != EMPTY_32) { b = start[c]; e = start[c + 1]; }
-        }
-        uint32_t nonEmpty = __ballot_sync(0xffffffffu, b < e);
-        while (nonEmpty) {
-            const int l = __ffs(nonEmpty) - 1;
-            nonEmpty &= nonEmpty - 1;
-            const uint32_t cb_ = __shfl_sync(0xffffffffu, b, l), ce = __shfl_sync(0xffffffffu, e, l);
-            const int ccx = __shfl_sync(0xffffffffu, cx, l), ccy = __shfl_sync(0xffffffffu, cy, l),
-                      ccz = __shfl_sync(0xffffffffu, cz, l);
-            // strict per-particle stencil (GatherCellQueryRanges, neighbor_search.cpp:917-947)
-            const bool ok = q.member && abs(ccx - q.lx) <= r && abs(ccy - q.ly) <= r && abs(ccz - q.lz) <= r;
-            if (!__any_sync(0xffffffffu, ok)) continue;
-            for (uint32_t k = cb_; k < ce; k++) {
-                const uint32_t j = (SP == 2) ? a.permR[k] : k;
-                const float4 pj = pos[j];
-                const bool hit = ok && IsNeighbor(q.pi.x, q.pi.y, q.pi.z, pj.x, pj.y, pj.z, a.r2);
-                if (FILL) {
-                    if (hit) w.store(m, lane, j, a.err);
-                } else {
-                    const uint32_t mask = __ballot_sync(0xffffffffu, hit);
-                    if (mask) dict.push(j < (1u << 30) ? (j | ((uint32_t)SP << 30)) : 0xffffffffu, mask, lane);
-                    if (j >= (1u << 30)) dict.ok = false;
-                    if (hit) {
-                        ref.cnt++;
-                        ref.mn = min(ref.mn, j);
-                        ref.mx = max(ref.mx, j);
-                        if (SP == 0) {
-                            if (j < q.homeLo) ref.farLoMax = max(ref.farLoMax, j);
-                            else if (j > q.homeHi) ref.farHiMin = min(ref.farHiMin, j);
-                            else ref.homeMin = min(ref.homeMin, j);
-                        }
-                    }
-                }
-            }
-        }
-    }
-}
-
 __device__ __forceinline__ void SortRowSell(const SellMeta& m, const LaneWriter& w, uint32_t lane) {
-    // rigid candidates arrive in sorted-cell order; rows are kept in ascending index order
-    // (the Delta16x2 / Abs32 codes of an FR chunk are monotonic in the index)
+    // rigid candidates arrive in sorted-cell order through the rigid permutation; rows are kept
+    // in ascending index order (the Delta16x2 / Abs32 codes of an FR chunk are monotonic in j)
     for (uint32_t x = 1; x < w.wr; x++) {
         const uint64_t at = w.off + (uint64_t)x * SELL_W + lane;
         uint32_t y = x;
@@ -403,131 +306,231 @@ __device__ __forceinline__ void SortRowSell(const SellMeta& m, const LaneWriter&
     }
 }
 
-template <bool FILL>
-__global__ void __launch_bounds__(QUERY_THREADS) KQueryFluid(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
-    extern __shared__ uint64_t qsmem[];
+// ---- per-lane stencil walk
+//
+// A chunk's lanes are grouped by their (sorted, hence contiguous) cell. For each group the
+// non-empty cells of its strict (2*reach+1)^3 stencil (GatherCellQueryRanges,
+// neighbor_search.cpp:917-947) are looked up once in the dense frame grid, and their particle
+// ranges are ranked by first index -- ascending cell ranges are ascending Morton IDs, so each
+// lane then walks exactly its own candidates in ascending index order. Groups are handled in
+// batches that fit the per-warp range staging (QueryGroupsPerBatch).
+struct QueryWarp {
+    uint2* rng;      // [RCAP] (begin, end) per stencil slot, group-major
+    uint2* srt;      // [RCAP] non-empty ranges of each group ranked by begin
+    int* gc;         // [3][32] cell coordinates of each group
+    uint32_t* nne;   // [32] non-empty ranges per group of the batch
+};
+__host__ __device__ __forceinline__ uint32_t StencilVolume(uint32_t reach) {
+    const uint32_t d = 2u * reach + 1u;
+    return d * d * d;
+}
+__host__ __device__ __forceinline__ uint32_t QueryGroupsPerBatch(uint32_t reach) {
+    const uint32_t sv = StencilVolume(reach);
+    return sv >= 256u ? 1u : 256u / sv;
+}
+__host__ __device__ __forceinline__ uint32_t QueryRangeCap(uint32_t reach) {
+    return QueryGroupsPerBatch(reach) * StencilVolume(reach);
+}
+__host__ __device__ __forceinline__ size_t QueryWarpSmemBytes(uint32_t reach) {
+    return (size_t)QueryRangeCap(reach) * 2u * sizeof(uint2) + 4u * 32u * sizeof(uint32_t);
+}
+__device__ __forceinline__ QueryWarp QueryWarpSmem(void* base, uint32_t warp, uint32_t reach) {
+    const uint32_t rcap = QueryRangeCap(reach);
+    char* p = (char*)base + (size_t)warp * QueryWarpSmemBytes(reach);
+    QueryWarp w;
+    w.rng = (uint2*)p;
+    w.srt = w.rng + rcap;
+    w.gc = (int*)(w.srt + rcap);
+    w.nne = (uint32_t*)(w.gc + 96);
+    return w;
+}
+
+struct QueryLaneInfo {
+    uint32_t i;
+    bool inRange, valid;
+    float4 pi;
+    uint32_t g;        // group (distinct cell) of a valid lane, EMPTY_32 otherwise
+    uint32_t nGroups;
+};
+
+__device__ __forceinline__ QueryLaneInfo QuerySetup(const QueryArgs& a, uint32_t chunk, uint32_t lane, const QueryWarp& w) {
+    QueryLaneInfo q;
+    q.i = chunk * SELL_W + lane;
+    q.inRange = q.i < a.nF;
+    const uint64_t cid = q.inRange ? a.cidF[q.i] : EMPTY_64;
+    q.valid = cid != EMPTY_64;
+    q.pi = q.inRange ? a.posF[q.i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    // out-of-frame particles (EMPTY cell ID) sort last, so valid lanes form a prefix of the chunk
+    const uint64_t prevCid = __shfl_up_sync(0xffffffffu, cid, 1);
+    const bool isStart = q.valid && (lane == 0 || prevCid != cid);
+    const uint32_t startMask = __ballot_sync(0xffffffffu, isStart);
+    q.nGroups = __popc(startMask);
+    q.g = q.valid ? (uint32_t)__popc(startMask & (0xffffffffu >> (31u - lane))) - 1u : EMPTY_32;
+    if (isStart) {
+        w.gc[q.g] = (int)Compact21(cid);
+        w.gc[32 + q.g] = (int)Compact21(cid >> 1);
+        w.gc[64 + q.g] = (int)Compact21(cid >> 2);
+    }
+    __syncwarp();
+    return q;
+}
+
+// stencil ranges of groups [g0, g0 + nb) of species SP, ranked by first index
+template <int SP>
+__device__ __forceinline__ void QueryRanges(const QueryArgs& a, const QueryWarp& w, uint32_t g0, uint32_t nb,
+                                            uint32_t lane) {
+    const uint32_t* grid = SP == 0 ? a.gridF : SP == 1 ? a.gridB : a.gridR;
+    const uint32_t* start = SP == 0 ? a.startF : SP == 1 ? a.startB : a.startR;
+    const int r = (int)a.fr.reach, D = 2 * r + 1;
+    const uint32_t sv = (uint32_t)(D * D * D), total = nb * sv;
+    if (lane < nb) w.nne[lane] = 0;
+    __syncwarp();
+    for (uint32_t t = lane; t < total; t += 32) {
+        const uint32_t gl = t / sv, s = t - gl * sv;
+        const int x = w.gc[g0 + gl] + (int)(s % D) - r;
+        const int y = w.gc[32 + g0 + gl] + (int)((s / D) % D) - r;
+        const int z = w.gc[64 + g0 + gl] + (int)(s / (D * D)) - r;
+        uint2 v = make_uint2(0u, 0u);
+        if (x >= 0 && x < (int)a.fr.nx && y >= 0 && y < (int)a.fr.ny && z >= 0 && z < (int)a.fr.nz) {
+            const uint32_t c = grid[(uint64_t)x + (uint64_t)a.fr.nx * ((uint64_t)y + (uint64_t)a.fr.ny * z)];
+            if (c != EMPTY_32) v = make_uint2(start[c], start[c + 1]);
+        }
+        w.rng[t] = v;
+        if (v.x < v.y) atomicAdd(&w.nne[gl], 1u);
+    }
+    __syncwarp();
+    for (uint32_t t = lane; t < total; t += 32) {
+        const uint32_t gl = t / sv;
+        const uint2 v = w.rng[t];
+        if (v.x < v.y) {
+            uint32_t rank = 0;
+            const uint2* row = w.rng + gl * sv;
+            for (uint32_t u = 0; u < sv; u++) {
+                const uint2 o = row[u];
+                rank += (o.x < o.y && o.x < v.x) ? 1u : 0u;
+            }
+            w.srt[gl * sv + rank] = v;
+        }
+    }
+    __syncwarp();
+}
+
+enum WalkMode { WALK_COUNT = 0, WALK_STATS = 1, WALK_FILL = 2 };
+
+// walk of each lane's own stencil candidates (ascending index order for F and B)
+template <int SP, int MODE>
+__device__ __forceinline__ void QueryWalk(const QueryArgs& a, const QueryWarp& w, const QueryLaneInfo& q, uint32_t g0,
+                                          uint32_t nb, uint32_t lane, uint32_t homeLo, uint32_t homeHi, LaneRefs& ref,
+                                          uint32_t* scr, uint32_t ks, LaneWriter& wr, const SellMeta& m) {
+    const float4* pos = SP == 0 ? a.posF : SP == 1 ? a.posB : a.posR;
+    const uint32_t sv = StencilVolume(a.fr.reach);
+    const bool mine = q.g != EMPTY_32 && q.g >= g0 && q.g < g0 + nb;
+    const uint32_t gl = mine ? q.g - g0 : 0u;
+    const uint32_t n = mine ? w.nne[gl] : 0u;
+    uint32_t k = 0, j = 0, e = 0;
+    bool act = n > 0;
+    if (act) { const uint2 v = w.srt[gl * sv]; j = v.x; e = v.y; }
+    while (__any_sync(0xffffffffu, act)) {
+        if (act) {
+            const uint32_t jj = SP == 2 ? a.permR[j] : j;
+            const float4 pj = pos[jj];
+            if (IsNeighbor(q.pi.x, q.pi.y, q.pi.z, pj.x, pj.y, pj.z, a.r2)) {
+                if (MODE == WALK_FILL) {
+                    wr.store(m, lane, jj, a.err);
+                } else {
+                    if (MODE == WALK_COUNT && ref.cnt < ks) scr[(uint64_t)ref.cnt * SELL_W] = jj;
+                    ref.cnt++;
+                    ref.mn = min(ref.mn, jj);
+                    ref.mx = max(ref.mx, jj);
+                    if (MODE == WALK_STATS) {
+                        if (jj < homeLo) ref.farLoMax = max(ref.farLoMax, jj);
+                        else if (jj > homeHi) ref.farHiMin = min(ref.farHiMin, jj);
+                        else ref.homeMin = min(ref.homeMin, jj);
+                    }
+                }
+            }
+            if (++j == e) {
+                if (++k < n) { const uint2 v = w.srt[gl * sv + k]; j = v.x; e = v.y; }
+                else act = false;
+            }
+        }
+    }
+}
+
+// whole-chunk walk of one species in group batches
+template <int SP, int MODE>
+__device__ __forceinline__ void QuerySpecies(const QueryArgs& a, const QueryWarp& w, const QueryLaneInfo& q,
+                                             uint32_t lane, uint32_t homeLo, uint32_t homeHi, LaneRefs& ref,
+                                             uint32_t* scr, uint32_t ks, LaneWriter& wr, const SellMeta& m) {
+    const uint32_t* grid = SP == 0 ? a.gridF : SP == 1 ? a.gridB : a.gridR;
+    if (grid == nullptr) return;
+    const uint32_t gb = QueryGroupsPerBatch(a.fr.reach);
+    for (uint32_t g0 = 0; g0 < q.nGroups; g0 += gb) {
+        const uint32_t nb = min(gb, q.nGroups - g0);
+        QueryRanges<SP>(a, w, g0, nb, lane);
+        QueryWalk<SP, MODE>(a, w, q, g0, nb, lane, homeLo, homeHi, ref, scr, ks, wr, m);
+        __syncwarp();
+    }
+}
+
+// home-window statistics of an FF row held in scratch (only needed when the chunk's index
+// span exceeds 0xffff and the Delta16x2 home/far split is tried)
+__device__ __forceinline__ void HomeStatsFromScratch(const uint32_t* scr, LaneRefs& ref, uint32_t homeLo,
+                                                     uint32_t homeHi) {
+    for (uint32_t k = 0; k < ref.cnt; k++) {
+        const uint32_t j = scr[(uint64_t)k * SELL_W];
+        if (j < homeLo) ref.farLoMax = max(ref.farLoMax, j);
+        else if (j > homeHi) ref.farHiMin = min(ref.farHiMin, j);
+        else ref.homeMin = min(ref.homeMin, j);
+    }
+}
+
+// count pass: neighbor counts, chunk compression meta, rows into the per-chunk scratch
+__global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidCount(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
+    extern __shared__ uint2 qsm[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint64_t* cells = qsmem + (uint64_t)warp * a.cap;
     const uint32_t chunk = blockIdx.x * (QUERY_THREADS / 32) + warp;
     const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
     if (chunk >= nChunks) return;  // uniform per warp
-    const uint32_t i = chunk * SELL_W + lane;
-    const bool inRange = i < a.nF;
-    const uint64_t cid = inRange ? a.cidF[i] : EMPTY_64;
-    const bool valid = cid != EMPTY_64;
-    QueryLane q;
-    q.pi = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (inRange) q.pi = a.posF[i];
-    q.lx = q.ly = q.lz = 0;
-    if (valid) { q.lx = (int)Compact21(cid); q.ly = (int)Compact21(cid >> 1); q.lz = (int)Compact21(cid >> 2); }
-    HomeWindow(chunk, q.homeLo, q.homeHi);
-    const int r = (int)a.fr.reach;
-
+    const QueryWarp w = QueryWarpSmem(qsm, warp, a.fr.reach);
+    const QueryLaneInfo q = QuerySetup(a, chunk, lane, w);
+    uint32_t homeLo, homeHi;
+    HomeWindow(chunk, homeLo, homeHi);
     LaneRefs rFF, rFB, rFR;
     rFF.init(); rFB.init(); rFR.init();
-    LaneWriter wFF, wFB, wFR;
-    if (FILL) { wFF.init(mFF, chunk); wFB.init(mFB, chunk); wFR.init(mFR, chunk); }
-    DictRec dict;
-    dict.base = a.dict ? a.dict + (uint64_t)chunk * a.dictCap : nullptr;
-    dict.n = 0; dict.cap = a.dict ? a.dictCap : 0u; dict.pj = 0; dict.pm = 0; dict.ok = a.dict != nullptr;
-
-    if (FILL && a.dict) {
-        // replay the count pass's hit masks (same order as the sweep)
-        const uint32_t nd = a.dictCount[chunk];
-        if (nd != EMPTY_32) {
-            const uint2* d = a.dict + (uint64_t)chunk * a.dictCap;
-            for (uint32_t b0 = 0; b0 < nd; b0 += 32) {
-                const uint2 mine = (b0 + lane < nd) ? d[b0 + lane] : make_uint2(0u, 0u);
-                const uint32_t cntHere = min(32u, nd - b0);
-                for (uint32_t e = 0; e < cntHere; e++) {
-                    const uint32_t tj = __shfl_sync(0xffffffffu, mine.x, e);
-                    const uint32_t tm = __shfl_sync(0xffffffffu, mine.y, e);
-                    if (!((tm >> lane) & 1u)) continue;
-                    const uint32_t sp = tj >> 30, j = tj & 0x3fffffffu;
-                    if (sp == 0) wFF.store(mFF, lane, j, a.err);
-                    else if (sp == 1) wFB.store(mFB, lane, j, a.err);
-                    else wFR.store(mFR, lane, j, a.err);
-                }
-            }
-            if (inRange && wFR.wr > 1) SortRowSell(mFR, wFR, lane);
-            return;
-        }
-    }
-
-    const uint32_t validMask = __ballot_sync(0xffffffffu, valid);
-    if (validMask) {
-        int mnx = valid ? q.lx : 0x7fffffff, mny = valid ? q.ly : 0x7fffffff, mnz = valid ? q.lz : 0x7fffffff;
-        int mxx = valid ? q.lx : -1, mxy = valid ? q.ly : -1, mxz = valid ? q.lz : -1;
+    LaneWriter none;
+    uint32_t* sF = a.scrF + (uint64_t)chunk * a.ksF * SELL_W + lane;
+    uint32_t* sB = a.scrB + (uint64_t)chunk * a.ksB * SELL_W + lane;
+    uint32_t* sR = a.scrR + (uint64_t)chunk * a.ksR * SELL_W + lane;
+    QuerySpecies<0, WALK_COUNT>(a, w, q, lane, homeLo, homeHi, rFF, sF, a.ksF, none, mFF);
+    QuerySpecies<1, WALK_COUNT>(a, w, q, lane, homeLo, homeHi, rFB, sB, a.ksB, none, mFB);
+    QuerySpecies<2, WALK_COUNT>(a, w, q, lane, homeLo, homeHi, rFR, sR, a.ksR, none, mFR);
+    const uint32_t over = (__any_sync(0xffffffffu, rFF.cnt > a.ksF) ? 1u : 0u) |
+                          (__any_sync(0xffffffffu, rFB.cnt > a.ksB) ? 2u : 0u) |
+                          (__any_sync(0xffffffffu, rFR.cnt > a.ksR) ? 4u : 0u);
+    // the FF home/far split needs per-lane window statistics only when the span exceeds 16 bits
+    uint32_t mn = rFF.mn, mx = rFF.mx;
 #pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-            mnx = min(mnx, __shfl_xor_sync(0xffffffffu, mnx, d)); mxx = max(mxx, __shfl_xor_sync(0xffffffffu, mxx, d));
-            mny = min(mny, __shfl_xor_sync(0xffffffffu, mny, d)); mxy = max(mxy, __shfl_xor_sync(0xffffffffu, mxy, d));
-            mnz = min(mnz, __shfl_xor_sync(0xffffffffu, mnz, d)); mxz = max(mxz, __shfl_xor_sync(0xffffffffu, mxz, d));
-        }
-        const uint64_t prevCid = __shfl_up_sync(0xffffffffu, cid, 1);
-        const bool isStart = valid && (lane == 0 || prevCid != cid);
-        const uint32_t startMask = __ballot_sync(0xffffffffu, isStart);
-        const uint32_t nDistinct = __popc(startMask);
-        const int bx0 = max(mnx - r, 0), by0 = max(mny - r, 0), bz0 = max(mnz - r, 0);
-        const int bx1 = min(mxx + r, (int)a.fr.nx - 1), by1 = min(mxy + r, (int)a.fr.ny - 1),
-                  bz1 = min(mxz + r, (int)a.fr.nz - 1);
-        const uint64_t boxVol = (uint64_t)(bx1 - bx0 + 1) * (uint64_t)(by1 - by0 + 1) * (uint64_t)(bz1 - bz0 + 1);
-        const uint64_t stencilVol = (uint64_t)(2 * r + 1) * (2 * r + 1) * (2 * r + 1);
-        // one box sweep when it is small (GatherChunkQueryRanges, neighbor_search.cpp:1008-1018),
-        // else one stencil box per distinct cell of the chunk
-        const bool boxMode = boxVol <= a.cap && boxVol <= (uint64_t)nDistinct * stencilVol;
-        const uint32_t nGroups = boxMode ? 1u : nDistinct;
-        uint32_t groupsLeft = startMask;
-        for (uint32_t g = 0; g < nGroups; g++) {
-            int gx0 = bx0, gy0 = by0, gz0 = bz0, gx1 = bx1, gy1 = by1, gz1 = bz1;
-            q.member = valid;
-            if (!boxMode) {
-                const int L = __ffs(groupsLeft) - 1;
-                groupsLeft &= groupsLeft - 1;
-                const uint64_t gcid = __shfl_sync(0xffffffffu, cid, L);
-                const int cx = __shfl_sync(0xffffffffu, q.lx, L), cy = __shfl_sync(0xffffffffu, q.ly, L),
-                          cz = __shfl_sync(0xffffffffu, q.lz, L);
-                q.member = valid && cid == gcid;
-                gx0 = max(cx - r, 0); gy0 = max(cy - r, 0); gz0 = max(cz - r, 0);
-                gx1 = min(cx + r, (int)a.fr.nx - 1); gy1 = min(cy + r, (int)a.fr.ny - 1); gz1 = min(cz + r, (int)a.fr.nz - 1);
-            }
-            const uint32_t ex = gx1 - gx0 + 1, ey = gy1 - gy0 + 1, ez = gz1 - gz0 + 1;
-            const uint32_t vol = ex * ey * ez;
-            if (vol > a.cap) {
-                if (lane == 0) atomicOr(a.err, ERR_QUERY_CAP);
-                continue;
-            }
-            uint32_t S = 32;
-            while (S < vol) S <<= 1;
-            for (uint32_t t = lane; t < S; t += 32) {
-                uint64_t v = 0xffffffffffffffffull;
-                if (t < vol) {
-                    const uint32_t x = gx0 + t % ex, y = gy0 + (t / ex) % ey, z = gz0 + t / (ex * ey);
-                    v = MortonLocal(x, y, z);
-                }
-                cells[t] = v;
-            }
-            __syncwarp();
-            WarpBitonicSort(cells, S, lane);
-            SweepSpecies<0, FILL>(a, cells, vol, q, lane, rFF, wFF, mFF, dict);
-            SweepSpecies<1, FILL>(a, cells, vol, q, lane, rFB, wFB, mFB, dict);
-            SweepSpecies<2, FILL>(a, cells, vol, q, lane, rFR, wFR, mFR, dict);
-            __syncwarp();
+    for (int d = 16; d > 0; d >>= 1) {
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+    }
+    if (mx >= mn && mx - mn > 0xffffu) {
+        if (!(over & 1u)) {
+            HomeStatsFromScratch(sF, rFF, homeLo, homeHi);
+        } else {
+            LaneRefs s;
+            s.init();
+            QuerySpecies<0, WALK_STATS>(a, w, q, lane, homeLo, homeHi, s, nullptr, 0, none, mFF);
+            rFF.homeMin = s.homeMin; rFF.farLoMax = s.farLoMax; rFF.farHiMin = s.farHiMin;
         }
     }
-    if (FILL) {
-        if (inRange && wFR.wr > 1) SortRowSell(mFR, wFR, lane);
-        return;
-    }
-    if (a.dict) {
-        dict.finish(lane);
-        if (lane == 0) a.dictCount[chunk] = (dict.ok && dict.n <= dict.cap) ? dict.n : EMPTY_32;
-    }
-    if (inRange) {
+    if (lane == 0) a.scrOver[chunk] = (uint8_t)over;
+    if (q.inRange) {
         if ((rFF.cnt | rFB.cnt | rFR.cnt) > 0xffffu) atomicOr(a.err, ERR_COUNT_U16);
-        mFF.counts[i] = (uint16_t)rFF.cnt;
-        mFB.counts[i] = (uint16_t)rFB.cnt;
-        mFR.counts[i] = (uint16_t)rFR.cnt;
+        mFF.counts[q.i] = (uint16_t)rFF.cnt;
+        mFB.counts[q.i] = (uint16_t)rFB.cnt;
+        mFR.counts[q.i] = (uint16_t)rFR.cnt;
     }
     {
         uint32_t t0 = rFF.cnt & 0xffffu, t1 = rFB.cnt & 0xffffu, t2 = rFR.cnt & 0xffffu;
@@ -549,26 +552,61 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluid(QueryArgs a, SellMe
     CommitChunkMeta(chunk, owner, rFR, false, mFR);
 }
 
-uint32_t QueryCap(uint32_t reach) {
-    const uint32_t stencil = (2 * reach + 1) * (2 * reach + 1) * (2 * reach + 1);
-    uint32_t cap = 512;
-    while (cap < stencil) cap <<= 1;
-    return cap;
+// encode one species' scratch rows of a chunk into its SELL32 slice (coalesced: the scratch
+// and the slice share the [slot][lane] layout)
+__device__ __forceinline__ void EncodeFromScratch(const SellMeta& m, LaneWriter& wr, const uint32_t* scr, uint32_t cnt,
+                                                  uint32_t lane, uint32_t* err) {
+    for (uint32_t k = 0; k < wr.pitch; k++)
+        if (k < cnt) wr.store(m, lane, scr[(uint64_t)k * SELL_W], err);
 }
+
+// fill pass: scratch rows -> SELL32 (a chunk whose scratch overflowed walks its stencil again)
+__global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidFill(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
+    extern __shared__ uint2 qsm[];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t chunk = blockIdx.x * (QUERY_THREADS / 32) + warp;
+    const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
+    if (chunk >= nChunks) return;
+    const uint32_t i = chunk * SELL_W + lane;
+    const bool inRange = i < a.nF;
+    const uint32_t over = a.scrOver[chunk];
+    LaneWriter wFF, wFB, wFR;
+    wFF.init(mFF, chunk); wFB.init(mFB, chunk); wFR.init(mFR, chunk);
+    const uint32_t* sF = a.scrF + (uint64_t)chunk * a.ksF * SELL_W + lane;
+    const uint32_t* sB = a.scrB + (uint64_t)chunk * a.ksB * SELL_W + lane;
+    const uint32_t* sR = a.scrR + (uint64_t)chunk * a.ksR * SELL_W + lane;
+    if (!(over & 1u)) EncodeFromScratch(mFF, wFF, sF, inRange ? mFF.counts[i] : 0u, lane, a.err);
+    if (!(over & 2u)) EncodeFromScratch(mFB, wFB, sB, inRange ? mFB.counts[i] : 0u, lane, a.err);
+    if (!(over & 4u)) EncodeFromScratch(mFR, wFR, sR, inRange ? mFR.counts[i] : 0u, lane, a.err);
+    if (over) {
+        const QueryWarp w = QueryWarpSmem(qsm, warp, a.fr.reach);
+        const QueryLaneInfo q = QuerySetup(a, chunk, lane, w);
+        LaneRefs none;
+        none.init();
+        if (over & 1u) QuerySpecies<0, WALK_FILL>(a, w, q, lane, 0u, 0u, none, nullptr, 0u, wFF, mFF);
+        if (over & 2u) QuerySpecies<1, WALK_FILL>(a, w, q, lane, 0u, 0u, none, nullptr, 0u, wFB, mFB);
+        if (over & 4u) QuerySpecies<2, WALK_FILL>(a, w, q, lane, 0u, 0u, none, nullptr, 0u, wFR, mFR);
+    }
+    if (inRange && wFR.wr > 1) SortRowSell(mFR, wFR, lane);
+}
+
+uint32_t QueryCap(uint32_t reach) { return QueryRangeCap(reach); }
+size_t QuerySmemBytes(uint32_t reach) { return QueryWarpSmemBytes(reach) * (QUERY_THREADS / 32); }
+size_t QueryScratchWords(uint32_t nChunks, uint32_t ks) { return (size_t)nChunks * ks * SELL_W; }
 
 void LaunchQueryFluid(bool fill, const QueryArgs& a, const SellMeta& ff, const SellMeta& fb, const SellMeta& fr,
                       cudaStream_t s) {
     const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
     if (nChunks == 0) return;
     const uint32_t warps = QUERY_THREADS / 32;
-    const size_t smem = (size_t)a.cap * sizeof(uint64_t) * warps;
+    const size_t smem = QueryWarpSmemBytes(a.fr.reach) * warps;
     const uint32_t blocks = (nChunks + warps - 1) / warps;
     if (fill) {
-        cudaFuncSetAttribute(KQueryFluid<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        KQueryFluid<true><<<blocks, QUERY_THREADS, smem, s>>>(a, ff, fb, fr);
+        cudaFuncSetAttribute(KQueryFluidFill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        KQueryFluidFill<<<blocks, QUERY_THREADS, smem, s>>>(a, ff, fb, fr);
     } else {
-        cudaFuncSetAttribute(KQueryFluid<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        KQueryFluid<false><<<blocks, QUERY_THREADS, smem, s>>>(a, ff, fb, fr);
+        cudaFuncSetAttribute(KQueryFluidCount, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        KQueryFluidCount<<<blocks, QUERY_THREADS, smem, s>>>(a, ff, fb, fr);
     }
 }
 

@@ -399,3 +399,47 @@ def floating_cubes(seed=5, dx=0.03, dt=1e-3):
         rigid.append((OBB(origin, (edge, edge, edge), *axes), dens))
     st, dmin, dmax = breaking_dam(container, fluid, p, rigid)
     return st, dmin, dmax, p
+
+
+@dataclasses.dataclass
+class ServedSceneSpec:
+    """One scene of the served stream: a block of nx x ny x nz fluid particles (spacing dx)
+    in the corner of a tank twice the block's extent per axis, arriving at `arrival_s`."""
+    index: int
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    dt: float
+    arrival_s: float
+    seed: int
+
+    @property
+    def n_fluid(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    def build(self):
+        from .params import dam_params
+        p = dam_params(self.dx, self.dt)
+        p.jitterFracF = 0.01
+        p.jitterSeedF = self.seed
+        ext = [(n + 0.5) * self.dx for n in (self.nx, self.ny, self.nz)]
+        container = OBB((0.0, 0.0, 0.0), tuple(2.0 * e for e in ext))
+        st, dmin, dmax = breaking_dam(container, OBB((0.0, 0.0, 0.0), tuple(ext)), p)
+        return st, dmin, dmax, p
+
+
+def served_stream(n_scenes=256, n_min=4096, n_max=262144, dx=0.01, dt=5e-4, rate_hz=64.0, seed=2024):
+    """Seeded served-stream workload: N_F log-uniform in [n_min, n_max], block aspect ratios
+    nx/ny and nz/ny uniform in [0.5, 2], Poisson arrivals at `rate_hz` scenes per second."""
+    rng = np.random.default_rng(seed)
+    specs, t = [], 0.0
+    for k in range(n_scenes):
+        n = math.exp(rng.uniform(math.log(n_min), math.log(n_max)))
+        r1, r2 = rng.uniform(0.5, 2.0, 2)
+        ny = max(2, int(round((n / (r1 * r2)) ** (1.0 / 3.0))))
+        nx = max(2, int(round(r1 * ny)))
+        nz = max(2, int(round(r2 * ny)))
+        t += rng.exponential(1.0 / rate_hz) if rate_hz > 0 else 0.0
+        specs.append(ServedSceneSpec(k, nx, ny, nz, dx, dt, t, seed * 1000 + k))
+    return specs
