@@ -96,9 +96,54 @@ __device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellV
     const uint32_t warps_ = (gridDim.x * blockDim.x) >> 5;                                 \
     for (uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < nChunks_; chunk += warps_)
 
+// L2 prefetch of the SELL32 slices a warp sweeps next. A chunk's slice of each category is
+// contiguous (pitch * 32 entries from its offset, a multiple of 32 entries, so the start is
+// 64-byte aligned and the size a multiple of 64 bytes), so one bulk prefetch per slice pulls it
+// into L2 while the warp still works on its current chunk. Lanes 0-5 each own one slice
+// (FF/FB/FR list, FF/FB/FR recorded gradient factors); the slice meta of chunk c + 2W is loaded
+// while chunk c is processed and the prefetch of c + W is issued at the start of chunk c.
+__device__ __forceinline__ void L2PrefetchBulk(const void* p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+struct SlicePrefetch {
+    uint32_t pitch, fmt;
+    uint64_t off;
+    __device__ __forceinline__ const SellView& view(const NeighborView& nv, uint32_t lane) const {
+        return lane < 2 ? nv.ff : (lane < 4 ? nv.fb : nv.fr);
+    }
+    __device__ __forceinline__ void load(const NeighborView& nv, uint32_t chunk, uint32_t nChunks, uint32_t lane) {
+        pitch = 0; fmt = 0; off = 0;
+        if (lane < 6 && chunk < nChunks) {
+            const SellView& v = view(nv, lane);
+            pitch = v.pitch[chunk]; fmt = v.format[chunk]; off = v.offset[chunk];
+        }
+    }
+    __device__ __forceinline__ void issue(const NeighborView& nv, uint32_t lane, bool kg) const {
+        if (pitch == 0) return;
+        const SellView& v = view(nv, lane);
+        const uint32_t n = pitch * SELL_W;
+        const bool d16 = fmt == FMT_DELTA16X2;
+        if ((lane & 1u) == 0u) {
+            if (d16) L2PrefetchBulk(v.list16 + off, n * 2u);
+            else L2PrefetchBulk(v.list32 + off, n * 4u);
+        } else if (kg) {
+            L2PrefetchBulk((d16 ? v.kg16 : v.kg32) + off, n * 4u);
+        }
+    }
+};
+#define FOR_EACH_CHUNK_PF(n, nv, KG)                                                            \
+    const uint32_t lane = threadIdx.x & 31;                                                     \
+    const uint32_t nChunks_ = ((n) + SELL_W - 1) / SELL_W;                                      \
+    const uint32_t warps_ = (gridDim.x * blockDim.x) >> 5;                                      \
+    SlicePrefetch pf_;                                                                          \
+    pf_.load(nv, ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) + warps_, nChunks_, lane);       \
+    for (uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < nChunks_;       \
+         chunk += warps_)                                                                       \
+        if (pf_.issue(nv, lane, KG), pf_.load(nv, chunk + 2u * warps_, nChunks_, lane), true)
+
 // ----------------------------------------------------------------------------- density
 __global__ void __launch_bounds__(SPH_THREADS) KDensity(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv) {
-    FOR_EACH_CHUNK(f.n) {
+    FOR_EACH_CHUNK_PF(f.n, nv, false) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = i < f.n;
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -123,7 +168,7 @@ __global__ void __launch_bounds__(SPH_THREADS) KDensity(Consts c, FluidDev f, Bo
 // ----------------------------------------------------------------------------- non-pressure
 __global__ void __launch_bounds__(SPH_THREADS, 4) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
-    FOR_EACH_CHUNK(f.n) {
+    FOR_EACH_CHUNK_PF(f.n, nv, false) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = i < f.n;
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -174,7 +219,7 @@ __global__ void __launch_bounds__(SPH_THREADS, 4) KNonPressure(Consts c, FluidDe
 // ----------------------------------------------------------------------------- source / diagonal / init
 __global__ void __launch_bounds__(SPH_THREADS, 4) KSourceDiagInit(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                             NeighborView nv) {
-    FOR_EACH_CHUNK(f.n) {
+    FOR_EACH_CHUNK_PF(f.n, nv, false) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = i < f.n;
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -239,7 +284,7 @@ __global__ void __launch_bounds__(SPH_THREADS, 4) KSourceDiagInit(Consts c, Flui
 // ----------------------------------------------------------------------------- pressure acceleration
 __global__ void __launch_bounds__(SPH_THREADS, 4) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
-    FOR_EACH_CHUNK(f.n) {
+    FOR_EACH_CHUNK_PF(f.n, nv, true) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = i < f.n;
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -288,7 +333,7 @@ __global__ void __launch_bounds__(SPH_THREADS, 4) KJacobi(Consts c, FluidDev f, 
                                                     SolverControl ctl, SolverState* st, double* partials,
                                                     cudaGraphConditionalHandle cond, int hasCond) {
     double eRaw = 0.0, ePos = 0.0, eAbs = 0.0;  // per-lane FP64 sums over the warp's chunks
-    FOR_EACH_CHUNK(f.n) {
+    FOR_EACH_CHUNK_PF(f.n, nv, true) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = i < f.n;
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
