@@ -248,6 +248,34 @@ int tsp_b200_get_phase_times(const tsp_backend* h, float* ms, uint32_t cap, uint
 /* number of CUDA kernels this backend launched since creation (graph nodes included) */
 int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count);
 
+/* ---- served batch ------------------------------------------------------------------------
+ * No counterpart in the reference (its SimulationMgr runs one scene per backend). A batch keeps
+ * many independent scenes of one physics setup resident on one GPU and advances all of them
+ * per substep over one scene-offset fluid array: one sort, one neighbor build, one solver pass
+ * for all scenes; the Jacobi loop drops each scene as it converges. A scene's results do not
+ * depend on the other scenes in the batch. Scenes are fluid + boundary (no rigid bodies).
+ * Admission charges an estimate of the scene's device memory (tsp_b200_batch_scene_bytes)
+ * against the budget given at creation and fails with TSP_ERR_OVERFLOW when it does not fit;
+ * admissions and retirements take effect at the next substep. */
+typedef struct tsp_batch tsp_batch;
+int tsp_b200_batch_create(const tsp_params* params, int device, uint64_t hbm_budget_bytes, tsp_batch** out);
+int tsp_b200_batch_destroy(tsp_batch* b);
+const char* tsp_b200_batch_last_error(const tsp_batch* b);
+/* admits one scene (PullFromUniversalSimState analogue; boundary volumes/psi taken from the view,
+ * defaults when NULL) with its sim domain; *slot identifies it until it is retired */
+int tsp_b200_admit(tsp_batch* b, const tsp_state_view* scene, const float domain_min[3],
+                   const float domain_max[3], uint32_t* slot);
+/* retires a scene; when out != NULL its state is pushed first (PushToUniversalSimState) */
+int tsp_b200_retire(tsp_batch* b, uint32_t slot, tsp_state_view* out);
+/* advances every admitted scene by n steps (ExecuteFullSimStep of each, fused) */
+int tsp_b200_substep_all(tsp_batch* b, const tsp_params* params, uint32_t n);
+int tsp_b200_batch_push(tsp_batch* b, uint32_t slot, tsp_state_view* out);
+int tsp_b200_batch_stats(const tsp_batch* b, uint32_t slot, tsp_step_stats* out);
+int tsp_b200_batch_info(const tsp_batch* b, uint32_t* scenes, uint64_t* fluid_particles, uint64_t* bytes_used,
+                        uint64_t* bytes_budget, float* last_substep_ms, uint64_t* launches);
+/* device bytes a scene is charged at admission (host arithmetic, no GPU work) */
+uint64_t tsp_b200_batch_scene_bytes(uint32_t n_fluid, uint32_t n_boundary, uint64_t grid_cells);
+
 /* ---- host helpers (no GPU work) -------------------------------------------------------- */
 /* Sim::TryBuildCellCoordFrame (source/simulation/core/cell_frame.h:32-66): inclusive signed
  * cell bounds -> frame origin and dimensions. Fails with TSP_ERR_FRAME, leaving origin/dims

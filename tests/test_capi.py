@@ -15,7 +15,7 @@ def declared_entry_points():
     for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
         if h.endswith(".h"):
             text = open(os.path.join(ROOT, "include", h)).read()
-            names += re.findall(r"^\s*(?:int|const char\*)\s+(tsp_b200_\w+)\s*\(", text, re.M)
+            names += re.findall(r"^\s*(?:int|const char\*|uint64_t)\s+(tsp_b200_\w+)\s*\(", text, re.M)
     return names
 
 
@@ -101,3 +101,13 @@ def test_cell_frame_invalid_bounds_preserve_frame(lib_abi, b):
     rc, o, d = _frame(lib_abi, b[:3], b[3:])
     assert rc == -4  # TSP_ERR_FRAME
     assert o == (4, 5, 6) and d == (7, 8, 9)
+
+
+def test_batch_scene_bytes_is_host_arithmetic(lib_abi):
+    f = lib_abi.tsp_b200_batch_scene_bytes
+    a = f(4096, 5000, 100_000)
+    assert a > 0
+    assert f(8192, 5000, 100_000) > a          # more fluid costs more
+    assert f(4096, 10000, 100_000) > a         # more boundary costs more
+    assert f(4096, 5000, 200_000) > a          # a larger frame costs more
+    assert f(4095, 5000, 100_000) == a         # fluid is charged in whole 32-particle chunks

@@ -135,6 +135,17 @@ EXPORTS = {
     "tsp_b200_get_phase_times": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32)]),
     "tsp_b200_try_build_cell_frame": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                                  C.POINTER(C.c_uint32)]),
+    "tsp_b200_batch_create": (C.c_int, [C.POINTER(TspParams), C.c_int, C.c_uint64, C.POINTER(_VP)]),
+    "tsp_b200_batch_destroy": (C.c_int, [_VP]),
+    "tsp_b200_batch_last_error": (C.c_char_p, [_VP]),
+    "tsp_b200_admit": (C.c_int, [_VP, C.POINTER(TspStateView), _pf, _pf, C.POINTER(C.c_uint32)]),
+    "tsp_b200_retire": (C.c_int, [_VP, C.c_uint32, C.POINTER(TspStateView)]),
+    "tsp_b200_substep_all": (C.c_int, [_VP, C.POINTER(TspParams), C.c_uint32]),
+    "tsp_b200_batch_push": (C.c_int, [_VP, C.c_uint32, C.POINTER(TspStateView)]),
+    "tsp_b200_batch_stats": (C.c_int, [_VP, C.c_uint32, C.POINTER(TspStepStats)]),
+    "tsp_b200_batch_info": (C.c_int, [_VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                      C.POINTER(C.c_uint64), C.POINTER(C.c_float), C.POINTER(C.c_uint64)]),
+    "tsp_b200_batch_scene_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint64]),
     "tsp_b200_noalloc_setup": (C.c_int, []),
     "tsp_b200_build_cell_table_noalloc": (C.c_int, [_VP, C.c_uint32, _VP, _VP, _VP, _VP]),
     "tsp_b200_noalloc_last_error": (C.c_char_p, []),

@@ -204,3 +204,89 @@ class SimBackendB200:
         v = np.ascontiguousarray(values, np.float32).ravel()
         k = FIELD_COMPONENTS[field]
         self._chk(self.L.tsp_b200_write_field(self.h, field, _p(v), v.size // k))
+
+
+class ServedBatchB200:
+    """Served batch over the C ABI (`tsp_b200_batch_*`): independent fluid + boundary scenes of
+    one physics setup, resident on one GPU and advanced together per substep. `admit` returns a
+    slot (raises TspError with TSP_ERR_OVERFLOW when the scene does not fit the memory budget);
+    admissions and retirements take effect at the next `substep`."""
+
+    def __init__(self, params: SimParams, budget_bytes: int, device: int = -1):
+        self.L = abi.load_library()
+        self.params = params
+        self._cp = params.to_c()
+        h = C.c_void_p()
+        rc = self.L.tsp_b200_batch_create(C.byref(self._cp), device, int(budget_bytes), C.byref(h))
+        if rc != 0:
+            raise TspError(rc, self.L.tsp_b200_batch_last_error(None).decode())
+        self.h = h
+        self.counts = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.tsp_b200_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise TspError(rc, self.L.tsp_b200_batch_last_error(self.h).decode())
+
+    def admit(self, state: UniversalSimState, dmin, dmax) -> int:
+        v = state.view()
+        a = np.ascontiguousarray(dmin, np.float32)
+        b = np.ascontiguousarray(dmax, np.float32)
+        slot = C.c_uint32()
+        self._chk(self.L.tsp_b200_admit(self.h, C.byref(v), a.ctypes.data_as(C.POINTER(C.c_float)),
+                                        b.ctypes.data_as(C.POINTER(C.c_float)), C.byref(slot)))
+        self.counts[slot.value] = (state.N_F, state.N_B)
+        return slot.value
+
+    def retire(self, slot: int, push: bool = False):
+        st = None
+        if push:
+            st = UniversalSimState(self.counts[slot][0], self.counts[slot][1], 0, 0)
+            v = st.view()
+            self._chk(self.L.tsp_b200_retire(self.h, slot, C.byref(v)))
+            st.step, st.time = int(v.step), float(v.time)
+        else:
+            self._chk(self.L.tsp_b200_retire(self.h, slot, None))
+        self.counts.pop(slot, None)
+        return st
+
+    def substep(self, n: int = 1, params: SimParams | None = None):
+        if params is not None:
+            self.params = params
+            self._cp = params.to_c()
+        self._chk(self.L.tsp_b200_substep_all(self.h, C.byref(self._cp), n))
+
+    def push(self, slot: int) -> UniversalSimState:
+        st = UniversalSimState(self.counts[slot][0], self.counts[slot][1], 0, 0)
+        v = st.view()
+        self._chk(self.L.tsp_b200_batch_push(self.h, slot, C.byref(v)))
+        st.step, st.time = int(v.step), float(v.time)
+        return st
+
+    def stats(self, slot: int) -> TspStepStats:
+        s = TspStepStats()
+        self._chk(self.L.tsp_b200_batch_stats(self.h, slot, C.byref(s)))
+        return s
+
+    def info(self) -> dict:
+        sc, nf, used, budget, launches = C.c_uint32(), C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        ms = C.c_float()
+        self._chk(self.L.tsp_b200_batch_info(self.h, C.byref(sc), C.byref(nf), C.byref(used), C.byref(budget),
+                                             C.byref(ms), C.byref(launches)))
+        return {"scenes": sc.value, "fluid_particles": nf.value, "bytes_used": used.value,
+                "bytes_budget": budget.value, "last_substep_ms": ms.value, "launches": launches.value}
+
+
+def batch_scene_bytes(n_fluid: int, n_boundary: int, grid_cells: int) -> int:
+    """Device bytes a served scene is charged at admission (host arithmetic)."""
+    return int(abi.load_library().tsp_b200_batch_scene_bytes(n_fluid, n_boundary, grid_cells))

@@ -14,8 +14,8 @@ import sys
 from .abi import LIB_PATH, PKG_DIR
 
 CSRC = os.path.join(PKG_DIR, "csrc")
-SOURCES = ["backend.cu", "ns_kernels.cu", "sph_kernels.cu", "rigid_kernels.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "kernels.h", "primitives.cuh"]
+SOURCES = ["backend.cu", "ns_kernels.cu", "sph_kernels.cu", "rigid_kernels.cu", "noalloc.cu", "batch.cu"]
+HEADERS = ["common.cuh", "kernels.h", "primitives.cuh", "host_common.h"]
 INCLUDE = os.path.join(os.path.dirname(PKG_DIR), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",

@@ -1,0 +1,123 @@
+// host_common.h -- host-side helpers shared by the one-scene backend and the served batch:
+// status-carrying exception, device buffers, the cell-frame rule and the solver constants.
+#pragma once
+
+#include <algorithm>
+#include <climits>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "../../include/tsp_b200.h"
+#include "kernels.h"
+
+namespace tsp {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+#define CK(x)                                                                                       \
+    do {                                                                                            \
+        cudaError_t e_ = (x);                                                                       \
+        if (e_ != cudaSuccess) throw Error(TSP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    void ensure(size_t n) {  // contents are not preserved
+        if (n <= cap && (p || n == 0)) return;
+        release();
+        if (n == 0) return;
+        CK(cudaMalloc(&p, n * sizeof(T)));
+        cap = n;
+    }
+    void grow(size_t n, double slack) {
+        if (n <= cap && p) return;
+        ensure((size_t)((double)n * slack) + 16);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    ~DBuf() { release(); }
+};
+template <typename T> inline void Swap(DBuf<T>& a, DBuf<T>& b) { std::swap(a.p, b.p); std::swap(a.cap, b.cap); }
+
+inline unsigned G(uint32_t n) { return (n + 255) / 256; }
+
+// ------------------------------------------------------------------------------ helpers
+inline int HostFloorToInt(float v) {
+    const int i = (int)v;
+    return (v < (float)i) ? (i - 1) : i;
+}
+// TryBuildCellCoordFrame (source/simulation/core/cell_frame.h:32-66): inclusive signed cell
+// bounds -> origin + dimensions; every axis must have min <= max, both within int32, and at
+// most 2^21 cells. On failure the frame is left unchanged.
+inline bool TryBuildCellFrame(const int64_t lo[3], const int64_t hi[3], int32_t& ox, int32_t& oy, int32_t& oz,
+                              uint32_t& nx, uint32_t& ny, uint32_t& nz) {
+    for (int a = 0; a < 3; a++)
+        if (lo[a] > hi[a] || lo[a] < (int64_t)INT32_MIN || hi[a] > (int64_t)INT32_MAX ||
+            hi[a] - lo[a] + 1 > (int64_t)(1u << 21))
+            return false;
+    ox = (int32_t)lo[0]; oy = (int32_t)lo[1]; oz = (int32_t)lo[2];
+    nx = (uint32_t)(hi[0] - lo[0] + 1); ny = (uint32_t)(hi[1] - lo[1] + 1); nz = (uint32_t)(hi[2] - lo[2] + 1);
+    return true;
+}
+inline uint32_t HostKeyBits(uint32_t nx, uint32_t ny, uint32_t nz) {  // neighbor_search.cpp:403-413
+    const uint32_t m = std::max(nx, std::max(ny, nz));
+    uint32_t axisBits = 1;
+    if (m >= 2) axisBits = 32u - (uint32_t)__builtin_clz(m - 1u);
+    return 3u * axisBits + 1u;
+}
+
+// solver constants exactly as the reference derives them (see common.cuh: Consts)
+inline Consts MakeConsts(const tsp_params& p) {
+    Consts c{};
+    const double h = (double)p.particleSizeF, hInv = 1.0 / h, rho = (double)p.restDensity;
+    c.sizeInv = (float)hInv;
+    c.sizeSqu = (float)(h * h);
+    c.alpha = p.cubicSplineAlphaOverride > 0.0f ? p.cubicSplineAlphaOverride
+                                                : (float)(hInv * hInv * hInv / (4.0 * 3.14159265358979323846));
+    c.restDensitySquInv = (float)(1.0 / (rho * rho));
+    c.radSqu = p.kernelRadiusSqu;
+    c.dt = p.timeStep;
+    c.dt2 = p.timeStep * p.timeStep;
+    c.kSize = 1.0f / c.sizeInv;
+    c.kTwoSize = 2.0f / c.sizeInv;
+    c.kInnerSlope = 9.0f * c.alpha * c.sizeInv * c.sizeInv * c.sizeInv;
+    c.kInnerOffset = -12.0f * c.alpha * c.sizeInv * c.sizeInv;
+    c.kOuterScale = -3.0f * c.alpha * c.sizeInv * c.sizeInv * c.sizeInv;
+    c.massF = p.massF;
+    c.restDensity = p.restDensity;
+    c.densInvSqu = 1.0f / (p.restDensity * p.restDensity);
+    c.hEps = 0.01f * c.sizeSqu;
+    c.visFacF = 10.0f * p.viscosityF;
+    c.visFacB = 10.0f * p.viscosityB;
+    c.gx = p.gravity[0]; c.gy = p.gravity[1]; c.gz = p.gravity[2];
+    c.cTermFacF = -p.massF * c.restDensitySquInv;
+    c.cTermFacB = -2.0f * p.pressGamma * c.restDensitySquInv;
+    c.diagBFac = -p.massF * c.restDensitySquInv;
+    c.omega = p.jacobiOmega;
+    c.warmStart = p.jacobiWarmStart;
+    c.warm = p.jacobiWarmStart > 0.0f ? 1 : 0;
+    c.accCoeffB = 2.0f * p.pressGamma * c.densInvSqu;
+    return c;
+}
+
+
+// pack / unpack kernels of the state boundary (defined in backend.cu)
+void LaunchPack4(const float* a, const float* b, const float* c, const float* d, float dDefault, float4* out,
+                 uint32_t n, cudaStream_t s);
+void LaunchUnpack4(const float4* in, float* a, float* b, float* c, float* d, uint32_t n, cudaStream_t s);
+void LaunchPack2(const float* a, const float* b, float2* out, uint32_t n, cudaStream_t s);
+void LaunchUnpack2(const float2* in, float* a, float* b, uint32_t n, cudaStream_t s);
+
+}  // namespace tsp

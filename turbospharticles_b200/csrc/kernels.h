@@ -67,6 +67,15 @@ struct QueryArgs {
     uint32_t *scrF, *scrB, *scrR;
     uint32_t ksF, ksB, ksR;
     uint8_t* scrOver;
+    // served batch only (NULL for one scene): valid lanes and scene of each chunk, and per
+    // scene its frame and the offsets of its dense grids inside gridF / gridB
+    const uint8_t* chunkLen;
+    const uint32_t* chunkScene;
+    const struct SceneGeom* scenes;
+};
+struct SceneGeom {
+    Frame fr;
+    uint64_t gridOffF, gridOffB;
 };
 
 struct RigidLists {
@@ -92,6 +101,19 @@ struct SolverControl {
     uint32_t nF;
 };
 
+// TerminationConditionSatisfied (source/simulation/CPU/backend/sph_solver.cpp:686-732)
+__device__ __forceinline__ bool Terminated(const SolverControl& ctl, uint32_t iters, const float* avg) {
+    if (iters < ctl.minIters) return false;
+    if (iters >= ctl.maxIters) return true;
+    switch (ctl.cond) {
+        case 0: return iters >= ctl.fixedIters;
+        case 1: return avg[0] <= ctl.target;
+        case 2: return avg[1] <= ctl.target;
+        case 3: return avg[2] <= ctl.target;
+        default: return iters >= 3;
+    }
+}
+
 // fluid SoA on the device (Morton order)
 struct FluidDev {
     float4* posP;     // x, y, z, pressure
@@ -100,7 +122,21 @@ struct FluidDev {
     float4* acc;      // a^p x, y, z, -
     float2* srcDiag;  // source term, diagonal a_ii
     uint32_t n;
+    // served batch only (all NULL for one scene): the particle array holds several scenes, each
+    // padded to whole SELL32 chunks; chunkLen = valid lanes of a chunk, chunkScene = its scene,
+    // sceneActive = scenes still iterating in the Jacobi loop (converged scenes are skipped),
+    // chunkPartials = per-chunk FP64 residual sums (raw, pos, abs) of a Jacobi sweep
+    const uint8_t* chunkLen;
+    const uint32_t* chunkScene;
+    const uint32_t* sceneActive;
+    double* chunkPartials;
 };
+__device__ __forceinline__ bool LaneActive(const FluidDev& f, uint32_t chunk, uint32_t lane, uint32_t i) {
+    return f.chunkLen ? lane < (uint32_t)f.chunkLen[chunk] : i < f.n;
+}
+__device__ __forceinline__ bool ChunkSkipped(const FluidDev& f, uint32_t chunk) {
+    return f.sceneActive != nullptr && f.sceneActive[f.chunkScene[chunk]] == 0u;
+}
 struct BoundaryDev {
     const float4* pos;  // x, y, z, psi
     const float* vol;

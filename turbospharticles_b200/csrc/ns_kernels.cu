@@ -345,6 +345,26 @@ __device__ __forceinline__ QueryWarp QueryWarpSmem(void* base, uint32_t warp, ui
     return w;
 }
 
+// frame and grids the warp's chunk is queried against (its scene's, in a served batch)
+struct QueryScene {
+    Frame fr;
+    const uint32_t *gridF, *gridB, *gridR;
+};
+__device__ __forceinline__ QueryScene ResolveScene(const QueryArgs& a, uint32_t chunk) {
+    QueryScene sc;
+    if (a.scenes) {
+        const SceneGeom& g = a.scenes[a.chunkScene[chunk]];
+        sc.fr = g.fr;
+        sc.gridF = a.gridF ? a.gridF + g.gridOffF : nullptr;
+        sc.gridB = a.gridB ? a.gridB + g.gridOffB : nullptr;
+        sc.gridR = nullptr;
+    } else {
+        sc.fr = a.fr;
+        sc.gridF = a.gridF; sc.gridB = a.gridB; sc.gridR = a.gridR;
+    }
+    return sc;
+}
+
 struct QueryLaneInfo {
     uint32_t i;
     bool inRange, valid;
@@ -356,7 +376,7 @@ struct QueryLaneInfo {
 __device__ __forceinline__ QueryLaneInfo QuerySetup(const QueryArgs& a, uint32_t chunk, uint32_t lane, const QueryWarp& w) {
     QueryLaneInfo q;
     q.i = chunk * SELL_W + lane;
-    q.inRange = q.i < a.nF;
+    q.inRange = a.chunkLen ? lane < (uint32_t)a.chunkLen[chunk] : q.i < a.nF;
     const uint64_t cid = q.inRange ? a.cidF[q.i] : EMPTY_64;
     q.valid = cid != EMPTY_64;
     q.pi = q.inRange ? a.posF[q.i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -377,11 +397,11 @@ __device__ __forceinline__ QueryLaneInfo QuerySetup(const QueryArgs& a, uint32_t
 
 // stencil ranges of groups [g0, g0 + nb) of species SP, ranked by first index
 template <int SP>
-__device__ __forceinline__ void QueryRanges(const QueryArgs& a, const QueryWarp& w, uint32_t g0, uint32_t nb,
-                                            uint32_t lane) {
-    const uint32_t* grid = SP == 0 ? a.gridF : SP == 1 ? a.gridB : a.gridR;
+__device__ __forceinline__ void QueryRanges(const QueryArgs& a, const QueryScene& sc, const QueryWarp& w, uint32_t g0,
+                                            uint32_t nb, uint32_t lane) {
+    const uint32_t* grid = SP == 0 ? sc.gridF : SP == 1 ? sc.gridB : sc.gridR;
     const uint32_t* start = SP == 0 ? a.startF : SP == 1 ? a.startB : a.startR;
-    const int r = (int)a.fr.reach, D = 2 * r + 1;
+    const int r = (int)sc.fr.reach, D = 2 * r + 1;
     const uint32_t sv = (uint32_t)(D * D * D), total = nb * sv;
     if (lane < nb) w.nne[lane] = 0;
     __syncwarp();
@@ -391,8 +411,8 @@ __device__ __forceinline__ void QueryRanges(const QueryArgs& a, const QueryWarp&
         const int y = w.gc[32 + g0 + gl] + (int)((s / D) % D) - r;
         const int z = w.gc[64 + g0 + gl] + (int)(s / (D * D)) - r;
         uint2 v = make_uint2(0u, 0u);
-        if (x >= 0 && x < (int)a.fr.nx && y >= 0 && y < (int)a.fr.ny && z >= 0 && z < (int)a.fr.nz) {
-            const uint32_t c = grid[(uint64_t)x + (uint64_t)a.fr.nx * ((uint64_t)y + (uint64_t)a.fr.ny * z)];
+        if (x >= 0 && x < (int)sc.fr.nx && y >= 0 && y < (int)sc.fr.ny && z >= 0 && z < (int)sc.fr.nz) {
+            const uint32_t c = grid[(uint64_t)x + (uint64_t)sc.fr.nx * ((uint64_t)y + (uint64_t)sc.fr.ny * z)];
             if (c != EMPTY_32) v = make_uint2(start[c], start[c + 1]);
         }
         w.rng[t] = v;
@@ -419,56 +439,61 @@ enum WalkMode { WALK_COUNT = 0, WALK_STATS = 1, WALK_FILL = 2 };
 
 // walk of each lane's own stencil candidates (ascending index order for F and B)
 template <int SP, int MODE>
-__device__ __forceinline__ void QueryWalk(const QueryArgs& a, const QueryWarp& w, const QueryLaneInfo& q, uint32_t g0,
-                                          uint32_t nb, uint32_t lane, uint32_t homeLo, uint32_t homeHi, LaneRefs& ref,
-                                          uint32_t* scr, uint32_t ks, LaneWriter& wr, const SellMeta& m) {
+__device__ __forceinline__ void QueryWalk(const QueryArgs& a, const QueryScene& sc, const QueryWarp& w,
+                                          const QueryLaneInfo& q, uint32_t g0, uint32_t nb, uint32_t lane,
+                                          uint32_t homeLo, uint32_t homeHi, LaneRefs& ref, uint32_t* scr, uint32_t ks,
+                                          LaneWriter& wr, const SellMeta& m) {
     const float4* pos = SP == 0 ? a.posF : SP == 1 ? a.posB : a.posR;
-    const uint32_t sv = StencilVolume(a.fr.reach);
+    const uint32_t sv = StencilVolume(sc.fr.reach);
     const bool mine = q.g != EMPTY_32 && q.g >= g0 && q.g < g0 + nb;
     const uint32_t gl = mine ? q.g - g0 : 0u;
     const uint32_t n = mine ? w.nne[gl] : 0u;
+    const uint2* rows = w.srt + gl * sv;
     uint32_t k = 0, j = 0, e = 0;
-    bool act = n > 0;
-    if (act) { const uint2 v = w.srt[gl * sv]; j = v.x; e = v.y; }
-    while (__any_sync(0xffffffffu, act)) {
-        if (act) {
-            const uint32_t jj = SP == 2 ? a.permR[j] : j;
-            const float4 pj = pos[jj];
-            if (IsNeighbor(q.pi.x, q.pi.y, q.pi.z, pj.x, pj.y, pj.z, a.r2)) {
-                if (MODE == WALK_FILL) {
-                    wr.store(m, lane, jj, a.err);
-                } else {
-                    if (MODE == WALK_COUNT && ref.cnt < ks) scr[(uint64_t)ref.cnt * SELL_W] = jj;
-                    ref.cnt++;
-                    ref.mn = min(ref.mn, jj);
-                    ref.mx = max(ref.mx, jj);
-                    if (MODE == WALK_STATS) {
-                        if (jj < homeLo) ref.farLoMax = max(ref.farLoMax, jj);
-                        else if (jj > homeHi) ref.farHiMin = min(ref.farHiMin, jj);
-                        else ref.homeMin = min(ref.homeMin, jj);
-                    }
-                }
+    if (n > 0) { const uint2 v = rows[0]; j = v.x; e = v.y; }
+    // count mode: rows go to the scratch through a running pointer (slot cnt of this lane);
+    // min/max of F and B rows are their first/last entries (ascending), taken after the walk
+    uint32_t* sp = scr + (uint64_t)ref.cnt * SELL_W;
+    while (k < n) {
+        const uint32_t jj = SP == 2 ? a.permR[j] : j;
+        const float4 pj = pos[jj];
+        const bool hit = IsNeighbor(q.pi.x, q.pi.y, q.pi.z, pj.x, pj.y, pj.z, a.r2);
+        if (MODE == WALK_FILL) {
+            if (hit) wr.store(m, lane, jj, a.err);
+        } else if (MODE == WALK_COUNT) {
+            if (hit && ref.cnt < ks) *sp = jj;
+            if (hit) { sp += SELL_W; ref.cnt++; }
+            if (SP == 2 && hit) { ref.mn = min(ref.mn, jj); ref.mx = max(ref.mx, jj); }
+            if (SP != 2 && hit) ref.mx = jj;
+        } else {
+            if (hit) {
+                ref.cnt++;
+                ref.mn = min(ref.mn, jj);
+                ref.mx = max(ref.mx, jj);
+                if (jj < homeLo) ref.farLoMax = max(ref.farLoMax, jj);
+                else if (jj > homeHi) ref.farHiMin = min(ref.farHiMin, jj);
+                else ref.homeMin = min(ref.homeMin, jj);
             }
-            if (++j == e) {
-                if (++k < n) { const uint2 v = w.srt[gl * sv + k]; j = v.x; e = v.y; }
-                else act = false;
-            }
+        }
+        if (++j == e) {
+            if (++k < n) { const uint2 v = rows[k]; j = v.x; e = v.y; }
         }
     }
 }
 
 // whole-chunk walk of one species in group batches
 template <int SP, int MODE>
-__device__ __forceinline__ void QuerySpecies(const QueryArgs& a, const QueryWarp& w, const QueryLaneInfo& q,
-                                             uint32_t lane, uint32_t homeLo, uint32_t homeHi, LaneRefs& ref,
-                                             uint32_t* scr, uint32_t ks, LaneWriter& wr, const SellMeta& m) {
-    const uint32_t* grid = SP == 0 ? a.gridF : SP == 1 ? a.gridB : a.gridR;
+__device__ __forceinline__ void QuerySpecies(const QueryArgs& a, const QueryScene& sc, const QueryWarp& w,
+                                             const QueryLaneInfo& q, uint32_t lane, uint32_t homeLo, uint32_t homeHi,
+                                             LaneRefs& ref, uint32_t* scr, uint32_t ks, LaneWriter& wr,
+                                             const SellMeta& m) {
+    const uint32_t* grid = SP == 0 ? sc.gridF : SP == 1 ? sc.gridB : sc.gridR;
     if (grid == nullptr) return;
-    const uint32_t gb = QueryGroupsPerBatch(a.fr.reach);
+    const uint32_t gb = QueryGroupsPerBatch(sc.fr.reach);
     for (uint32_t g0 = 0; g0 < q.nGroups; g0 += gb) {
         const uint32_t nb = min(gb, q.nGroups - g0);
-        QueryRanges<SP>(a, w, g0, nb, lane);
-        QueryWalk<SP, MODE>(a, w, q, g0, nb, lane, homeLo, homeHi, ref, scr, ks, wr, m);
+        QueryRanges<SP>(a, sc, w, g0, nb, lane);
+        QueryWalk<SP, MODE>(a, sc, w, q, g0, nb, lane, homeLo, homeHi, ref, scr, ks, wr, m);
         __syncwarp();
     }
 }
@@ -492,6 +517,7 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidCount(QueryArgs a, S
     const uint32_t chunk = blockIdx.x * (QUERY_THREADS / 32) + warp;
     const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
     if (chunk >= nChunks) return;  // uniform per warp
+    const QueryScene sc = ResolveScene(a, chunk);
     const QueryWarp w = QueryWarpSmem(qsm, warp, a.fr.reach);
     const QueryLaneInfo q = QuerySetup(a, chunk, lane, w);
     uint32_t homeLo, homeHi;
@@ -502,9 +528,12 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidCount(QueryArgs a, S
     uint32_t* sF = a.scrF + (uint64_t)chunk * a.ksF * SELL_W + lane;
     uint32_t* sB = a.scrB + (uint64_t)chunk * a.ksB * SELL_W + lane;
     uint32_t* sR = a.scrR + (uint64_t)chunk * a.ksR * SELL_W + lane;
-    QuerySpecies<0, WALK_COUNT>(a, w, q, lane, homeLo, homeHi, rFF, sF, a.ksF, none, mFF);
-    QuerySpecies<1, WALK_COUNT>(a, w, q, lane, homeLo, homeHi, rFB, sB, a.ksB, none, mFB);
-    QuerySpecies<2, WALK_COUNT>(a, w, q, lane, homeLo, homeHi, rFR, sR, a.ksR, none, mFR);
+    QuerySpecies<0, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFF, sF, a.ksF, none, mFF);
+    QuerySpecies<1, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFB, sB, a.ksB, none, mFB);
+    QuerySpecies<2, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFR, sR, a.ksR, none, mFR);
+    // F and B rows are ascending: the minimum is the first stored entry
+    if (rFF.cnt) rFF.mn = sF[0];
+    if (rFB.cnt) rFB.mn = sB[0];
     const uint32_t over = (__any_sync(0xffffffffu, rFF.cnt > a.ksF) ? 1u : 0u) |
                           (__any_sync(0xffffffffu, rFB.cnt > a.ksB) ? 2u : 0u) |
                           (__any_sync(0xffffffffu, rFR.cnt > a.ksR) ? 4u : 0u);
@@ -521,7 +550,7 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidCount(QueryArgs a, S
         } else {
             LaneRefs s;
             s.init();
-            QuerySpecies<0, WALK_STATS>(a, w, q, lane, homeLo, homeHi, s, nullptr, 0, none, mFF);
+            QuerySpecies<0, WALK_STATS>(a, sc, w, q, lane, homeLo, homeHi, s, nullptr, 0, none, mFF);
             rFF.homeMin = s.homeMin; rFF.farLoMax = s.farLoMax; rFF.farHiMin = s.farHiMin;
         }
     }
@@ -556,8 +585,15 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidCount(QueryArgs a, S
 // and the slice share the [slot][lane] layout)
 __device__ __forceinline__ void EncodeFromScratch(const SellMeta& m, LaneWriter& wr, const uint32_t* scr, uint32_t cnt,
                                                   uint32_t lane, uint32_t* err) {
-    for (uint32_t k = 0; k < wr.pitch; k++)
-        if (k < cnt) wr.store(m, lane, scr[(uint64_t)k * SELL_W], err);
+    constexpr uint32_t U = 8;  // loads of U slots in flight before their stores
+    for (uint32_t k0 = 0; k0 < wr.pitch; k0 += U) {
+        uint32_t v[U];
+#pragma unroll
+        for (uint32_t u = 0; u < U; u++) v[u] = (k0 + u < cnt) ? __ldcs(scr + (uint64_t)(k0 + u) * SELL_W) : 0u;
+#pragma unroll
+        for (uint32_t u = 0; u < U; u++)
+            if (k0 + u < cnt) wr.store(m, lane, v[u], err);
+    }
 }
 
 // fill pass: scratch rows -> SELL32 (a chunk whose scratch overflowed walks its stencil again)
@@ -568,7 +604,7 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidFill(QueryArgs a, Se
     const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
     if (chunk >= nChunks) return;
     const uint32_t i = chunk * SELL_W + lane;
-    const bool inRange = i < a.nF;
+    const bool inRange = a.chunkLen ? lane < (uint32_t)a.chunkLen[chunk] : i < a.nF;
     const uint32_t over = a.scrOver[chunk];
     LaneWriter wFF, wFB, wFR;
     wFF.init(mFF, chunk); wFB.init(mFB, chunk); wFR.init(mFR, chunk);
@@ -579,13 +615,14 @@ __global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidFill(QueryArgs a, Se
     if (!(over & 2u)) EncodeFromScratch(mFB, wFB, sB, inRange ? mFB.counts[i] : 0u, lane, a.err);
     if (!(over & 4u)) EncodeFromScratch(mFR, wFR, sR, inRange ? mFR.counts[i] : 0u, lane, a.err);
     if (over) {
+        const QueryScene sc = ResolveScene(a, chunk);
         const QueryWarp w = QueryWarpSmem(qsm, warp, a.fr.reach);
         const QueryLaneInfo q = QuerySetup(a, chunk, lane, w);
         LaneRefs none;
         none.init();
-        if (over & 1u) QuerySpecies<0, WALK_FILL>(a, w, q, lane, 0u, 0u, none, nullptr, 0u, wFF, mFF);
-        if (over & 2u) QuerySpecies<1, WALK_FILL>(a, w, q, lane, 0u, 0u, none, nullptr, 0u, wFB, mFB);
-        if (over & 4u) QuerySpecies<2, WALK_FILL>(a, w, q, lane, 0u, 0u, none, nullptr, 0u, wFR, mFR);
+        if (over & 1u) QuerySpecies<0, WALK_FILL>(a, sc, w, q, lane, 0u, 0u, none, nullptr, 0u, wFF, mFF);
+        if (over & 2u) QuerySpecies<1, WALK_FILL>(a, sc, w, q, lane, 0u, 0u, none, nullptr, 0u, wFB, mFB);
+        if (over & 4u) QuerySpecies<2, WALK_FILL>(a, sc, w, q, lane, 0u, 0u, none, nullptr, 0u, wFR, mFR);
     }
     if (inRange && wFR.wr > 1) SortRowSell(mFR, wFR, lane);
 }

@@ -14,6 +14,13 @@
 namespace tsp {
 
 constexpr uint32_t SPH_THREADS = 256;
+// tuning of the neighbor sweeps: FF slots in flight per lane, minimum resident blocks per SM
+#ifndef TSP_SPH_FF_SLOTS
+#define TSP_SPH_FF_SLOTS 4
+#endif
+#ifndef TSP_SPH_MIN_BLOCKS
+#define TSP_SPH_MIN_BLOCKS 4
+#endif
 
 struct ChunkCursor {
     uint32_t pitch, cnt, base, base2;
@@ -145,12 +152,12 @@ struct SlicePrefetch {
 __global__ void __launch_bounds__(SPH_THREADS) KDensity(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv) {
     FOR_EACH_CHUNK_PF(f.n, nv, false) {
         const uint32_t i = chunk * SELL_W + lane;
-        const bool act = i < f.n;
+        const bool act = LaneActive(f, chunk, lane, i);
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         float dF = 0.f, dB = 0.f, dR = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<4, false>(cur, nv.ff, lane, f.posP, nullptr, [&](uint32_t, uint32_t, const float4& pj, const float4&) {
+        SweepSlots<TSP_SPH_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](uint32_t, uint32_t, const float4& pj, const float4&) {
             dF = fmaf(c.massF, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dF);
         });
         cur.load(nv.fb, chunk, i, act);
@@ -166,17 +173,17 @@ __global__ void __launch_bounds__(SPH_THREADS) KDensity(Consts c, FluidDev f, Bo
 }
 
 // ----------------------------------------------------------------------------- non-pressure
-__global__ void __launch_bounds__(SPH_THREADS, 4) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+__global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
     FOR_EACH_CHUNK_PF(f.n, nv, false) {
         const uint32_t i = chunk * SELL_W + lane;
-        const bool act = i < f.n;
+        const bool act = LaneActive(f, chunk, lane, i);
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 vi = act ? f.velRho[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         float fx = 0.f, fy = 0.f, fz = 0.f, bx = 0.f, by = 0.f, bz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<4, true>(cur, nv.ff, lane, f.posP, f.velRho, [&](uint32_t, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<TSP_SPH_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velRho, [&](uint32_t, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -217,18 +224,18 @@ __global__ void __launch_bounds__(SPH_THREADS, 4) KNonPressure(Consts c, FluidDe
 }
 
 // ----------------------------------------------------------------------------- source / diagonal / init
-__global__ void __launch_bounds__(SPH_THREADS, 4) KSourceDiagInit(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+__global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagInit(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                             NeighborView nv) {
     FOR_EACH_CHUNK_PF(f.n, nv, false) {
         const uint32_t i = chunk * SELL_W + lane;
-        const bool act = i < f.n;
+        const bool act = LaneActive(f, chunk, lane, i);
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 vi = act ? f.velPred[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         float sF = 0.f, sB = 0.f, sR = 0.f, cxF = 0.f, cyF = 0.f, czF = 0.f, g2 = 0.f;
         float cxB = 0.f, cyB = 0.f, czB = 0.f, cxR = 0.f, cyR = 0.f, czR = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<4, true>(cur, nv.ff, lane, f.posP, f.velPred, [&](uint32_t k, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<TSP_SPH_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velPred, [&](uint32_t k, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -282,17 +289,18 @@ __global__ void __launch_bounds__(SPH_THREADS, 4) KSourceDiagInit(Consts c, Flui
 }
 
 // ----------------------------------------------------------------------------- pressure acceleration
-__global__ void __launch_bounds__(SPH_THREADS, 4) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+__global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
     FOR_EACH_CHUNK_PF(f.n, nv, true) {
+        if (ChunkSkipped(f, chunk)) continue;  // converged scene of a batch
         const uint32_t i = chunk * SELL_W + lane;
-        const bool act = i < f.n;
+        const bool act = LaneActive(f, chunk, lane, i);
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float fOuter = c.massF * pi.w * c.densInvSqu;
         float ax = 0.f, ay = 0.f, az = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsKg<4, false>(cur, nv.ff, lane, f.posP, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsKg<TSP_SPH_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float a = (fOuter + c.massF * pj.w * c.densInvSqu) * kg;
             ax = fmaf(a, dx, ax); ay = fmaf(a, dy, ay); az = fmaf(a, dz, az);
@@ -316,32 +324,22 @@ __global__ void __launch_bounds__(SPH_THREADS, 4) KPressureAcc(Consts c, FluidDe
 }
 
 // ----------------------------------------------------------------------------- relaxed Jacobi sweep
-__device__ __forceinline__ bool Terminated(const SolverControl& ctl, uint32_t iters, const float* avg) {
-    // TerminationConditionSatisfied (sph_solver.cpp:686-732)
-    if (iters < ctl.minIters) return false;
-    if (iters >= ctl.maxIters) return true;
-    switch (ctl.cond) {
-        case 0: return iters >= ctl.fixedIters;
-        case 1: return avg[0] <= ctl.target;
-        case 2: return avg[1] <= ctl.target;
-        case 3: return avg[2] <= ctl.target;
-        default: return iters >= 3;
-    }
-}
 
-__global__ void __launch_bounds__(SPH_THREADS, 4) KJacobi(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv,
+__global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KJacobi(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv,
                                                     SolverControl ctl, SolverState* st, double* partials,
                                                     cudaGraphConditionalHandle cond, int hasCond) {
     double eRaw = 0.0, ePos = 0.0, eAbs = 0.0;  // per-lane FP64 sums over the warp's chunks
     FOR_EACH_CHUNK_PF(f.n, nv, true) {
+        if (ChunkSkipped(f, chunk)) continue;  // converged scene of a batch
+        double cRaw = 0.0, cPos = 0.0, cAbs = 0.0;  // this chunk's contribution of the lane
         const uint32_t i = chunk * SELL_W + lane;
-        const bool act = i < f.n;
+        const bool act = LaneActive(f, chunk, lane, i);
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 ai = act ? f.acc[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         float sF = 0.f, sB = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsKg<4, true>(cur, nv.ff, lane, f.posP, f.acc, [&](float kg, const float4& pj, const float4& aj) {
+        SweepSlotsKg<TSP_SPH_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.acc, [&](float kg, const float4& pj, const float4& aj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
             const float sv = fmaf(dax, dx, fmaf(day, dy, daz * dz));
@@ -372,12 +370,31 @@ __global__ void __launch_bounds__(SPH_THREADS, 4) KJacobi(Consts c, FluidDev f, 
             reinterpret_cast<float*>(f.posP)[4ull * i + 3] = pn;
             if (valid) {
                 const double re = (double)(err / c.restDensity);
-                eRaw += re;
-                ePos += re > 0.0 ? re : 0.0;
-                eAbs += fabs(re);
+                cRaw = re;
+                cPos = re > 0.0 ? re : 0.0;
+                cAbs = fabs(re);
             }
         }
+        if (f.chunkPartials) {
+            // batch: fixed-order per-chunk sums, reduced per scene by a separate kernel
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                cRaw += __shfl_xor_sync(0xffffffffu, cRaw, d);
+                cPos += __shfl_xor_sync(0xffffffffu, cPos, d);
+                cAbs += __shfl_xor_sync(0xffffffffu, cAbs, d);
+            }
+            if (lane == 0) {
+                f.chunkPartials[3ull * chunk + 0] = cRaw;
+                f.chunkPartials[3ull * chunk + 1] = cPos;
+                f.chunkPartials[3ull * chunk + 2] = cAbs;
+            }
+        } else {
+            eRaw += cRaw;
+            ePos += cPos;
+            eAbs += cAbs;
+        }
     }
+    if (f.chunkPartials) return;
     // FP64 block reduction (fixed order), last block folds the partials in fixed order
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
@@ -447,11 +464,11 @@ __global__ void __launch_bounds__(SPH_THREADS) KGradFactors(Consts c, FluidDev f
                                                          NeighborView nv) {
     FOR_EACH_CHUNK(f.n) {
         const uint32_t i = chunk * SELL_W + lane;
-        const bool act = i < f.n;
+        const bool act = LaneActive(f, chunk, lane, i);
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<4, false>(cur, nv.ff, lane, f.posP, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
+        SweepSlots<TSP_SPH_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             *cur.kgSlot(nv.ff, k, lane) = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
         });
@@ -480,6 +497,7 @@ __global__ void KSolverReset(SolverState* st, uint32_t nF) {
 __global__ void __launch_bounds__(256) KIntegration(Consts c, FluidDev f) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= f.n) return;
+    if (f.chunkLen && (i & 31u) >= (uint32_t)f.chunkLen[i >> 5]) return;  // padding of a batched scene
     const float4 vp = f.velPred[i];
     const float4 a = f.acc[i];
     const float4 p = f.posP[i];
@@ -562,7 +580,7 @@ void LaunchNonPressure(const Consts& c, const FluidDev& f, const BoundaryDev& b,
 void LaunchSourceDiagInit(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
                           const NeighborView& nv, SolverState* st, cudaStream_t s) {
     if (f.n) KSourceDiagInit<<<PersistentBlocks(KSourceDiagInit, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
-    KSolverReset<<<1, 1, 0, s>>>(st, f.n);
+    if (st) KSolverReset<<<1, 1, 0, s>>>(st, f.n);
 }
 void LaunchSolverReset(SolverState* st, uint32_t nF, cudaStream_t s) { KSolverReset<<<1, 1, 0, s>>>(st, nF); }
 void LaunchGradFactors(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,

@@ -1,0 +1,143 @@
+"""Served mixed-size stream: continuous batching of independent dam-break scenes on one GPU.
+
+Request loop: scenes arrive (seeded Poisson process, `scene.served_stream`), wait in a FIFO
+queue, and are admitted into the batch when the batch's device-memory budget has room; every
+loop iteration advances all admitted scenes by one step (`ServedBatchB200.substep`); a scene
+that has run its steps is retired and its slot and memory are reused. Arrival times are
+compared with the loop's own clock (device-timed substeps), so arrivals that happen while
+other scenes are on the GPU are admitted at the next substep.
+
+The comparison path runs the same scenes one at a time on the one-scene backend
+(`SimBackendB200`), the plain path; to bound its run time it times a sample of steps of every
+scene and charges each scene its full step count at the sampled per-step time.
+
+    python -m turbospharticles_b200.serve --scenes 256 --steps 500        # the full stream
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import abi, scene as S
+from .backend import ServedBatchB200, SimBackendB200, TspError
+
+
+def prepare(specs):
+    """Builds every scene and computes its boundary volumes once (ComputeParticleCoefficients,
+    which the reference runs when it builds a scene)."""
+    out = []
+    for sp in specs:
+        st, dmin, dmax, p = sp.build()
+        be = SimBackendB200(p)
+        be.set_sim_domain_bounds(dmin, dmax)
+        be.pull(st, p)
+        be.run_stage(abi.STAGE_BOUNDARY_VOLUMES, p)
+        st = be.push()
+        be.close()
+        out.append((sp, st, dmin, dmax, p))
+    return out
+
+
+def run_served(prepared, steps, budget_bytes, max_substeps=None):
+    """Continuous batching of the prepared scenes; returns throughput and latency figures."""
+    p = prepared[0][4]
+    batch = ServedBatchB200(p, budget_bytes)
+    queue = list(range(len(prepared)))
+    queue.sort(key=lambda k: prepared[k][0].arrival_s)
+    active = {}   # slot -> (scene index, steps done)
+    clock_s = 0.0
+    sub_ms, n_active, particles_per_sub = [], [], []
+    done_updates = 0
+    refused = 0
+    it = 0
+    t0 = time.perf_counter()
+    while queue or active:
+        # admit arrived scenes in arrival order while they fit
+        while queue and (prepared[queue[0]][0].arrival_s <= clock_s or not active):
+            k = queue[0]
+            sp, st, dmin, dmax, _ = prepared[k]
+            try:
+                slot = batch.admit(st, dmin, dmax)
+            except TspError as e:
+                if e.status != -3 or not active:
+                    raise
+                refused += 1
+                break
+            active[slot] = [k, 0]
+            queue.pop(0)
+        batch.substep(1)
+        info = batch.info()
+        ms = info["last_substep_ms"]
+        sub_ms.append(ms)
+        clock_s += ms / 1e3
+        nf = sum(prepared[k][0].n_fluid for k, _ in active.values())
+        particles_per_sub.append(nf)
+        n_active.append(len(active))
+        done_updates += nf
+        for slot in list(active):
+            active[slot][1] += 1
+            if active[slot][1] >= steps:
+                batch.retire(slot)
+                del active[slot]
+        it += 1
+        if max_substeps and it >= max_substeps:
+            break
+    wall_s = time.perf_counter() - t0
+    batch.close()
+    dev_s = float(np.sum(sub_ms)) / 1e3
+    q = np.percentile(sub_ms, [50, 99])
+    return {"particle_updates": int(done_updates), "device_s": round(dev_s, 4), "wall_s": round(wall_s, 3),
+            "value": round(done_updates / dev_s, 1), "value_wall": round(done_updates / wall_s, 1),
+            "substeps": it, "p50_step_ms": round(float(q[0]), 4), "p99_step_ms": round(float(q[1]), 4),
+            "mean_active_scenes": round(float(np.mean(n_active)), 1), "max_active_scenes": int(np.max(n_active)),
+            "admissions_deferred": refused, "budget_bytes": int(budget_bytes)}
+
+
+def run_plain(prepared, steps, sample_steps=10, warmup=2):
+    """The same scenes one at a time on the one-scene backend (device time per step)."""
+    total_updates, total_s, step_ms = 0, 0.0, []
+    for sp, st, dmin, dmax, p in prepared:
+        be = SimBackendB200(p)
+        be.set_sim_domain_bounds(dmin, dmax)
+        be.pull(st, p)
+        for _ in range(warmup):
+            be.step(p)
+        ms = []
+        for _ in range(sample_steps):
+            be.step(p)
+            ms.append(be.stats().lastStepMs)
+        be.close()
+        per = float(np.mean(ms))
+        step_ms.extend(ms)
+        total_updates += sp.n_fluid * steps
+        total_s += per * steps / 1e3
+    q = np.percentile(step_ms, [50, 99])
+    return {"particle_updates": int(total_updates), "device_s": round(total_s, 4),
+            "value": round(total_updates / total_s, 1), "p50_step_ms": round(float(q[0]), 4),
+            "p99_step_ms": round(float(q[1]), 4), "sampled_steps_per_scene": sample_steps}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--scenes", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--rate", type=float, default=64.0, help="Poisson arrival rate, scenes per second")
+    ap.add_argument("--budget-gb", type=float, default=16.0)
+    ap.add_argument("--plain-sample", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=2024)
+    args = ap.parse_args()
+    specs = S.served_stream(args.scenes, rate_hz=args.rate, seed=args.seed)
+    prepared = prepare(specs)
+    served = run_served(prepared, args.steps, int(args.budget_gb * (1 << 30)))
+    plain = run_plain(prepared, args.steps, args.plain_sample)
+    print(json.dumps({"workload": "served_stream", "scenes": args.scenes, "steps_per_scene": args.steps,
+                      "rate_hz": args.rate, "n_fluid_total": int(sum(s.n_fluid for s in specs)),
+                      "served": served, "plain": plain,
+                      "served_over_plain": round(served["value"] / plain["value"], 3)}))
+
+
+if __name__ == "__main__":
+    main()
