@@ -14,6 +14,9 @@ replicas (one scene per GPU, no inter-GPU traffic) -> weak scaling.
 e2e: the same metric through the C ABI with pinned host buffers: per step pull_state (H2D of
 the step's particle state) + step + push_state (D2H of positions, velocities, pressure,
 density).
+served: the seeded mixed-size served stream (continuous batching, turbospharticles_b200.serve;
+64 scenes x 100 steps by default, --served-scenes 256 --served-steps 500 for the full stream)
+against the same scenes one at a time on the plain one-scene path, both device-timed.
 --impl reference: the CPU restatement of the reference step (oracle/, OpenMP over all host
 threads) on the same workload; the reference's own CPU backend cannot be built here.
 """
@@ -220,6 +223,11 @@ def run_b200(args):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline_from(be, p, dmin, dmax)
+    # ---- served mixed-size stream (continuous batching) vs the same scenes one at a time
+    served = None
+    if rank == 0 and ws == 1 and args.served_scenes > 0:
+        be.close()
+        served = served_stream_measure(args.served_scenes, args.served_steps)
     if dist is not None:
         dist.destroy_process_group()
     if rank != 0:
@@ -239,9 +247,26 @@ def run_b200(args):
         "phase_ms_p50": {k: round(float(np.median([ph[k] for ph in phases if k in ph])), 4)
                          for k in (phases[-1] if phases else {})},
         "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
-        "clocks": clk.summary(), "impl": "b200",
+        "clocks": clk.summary(), "served": served, "impl": "b200",
     }
     print(json.dumps(line), flush=True)
+
+
+def served_stream_measure(n_scenes, steps):
+    """Served-stream figures (turbospharticles_b200.serve): the seeded mixed-size stream
+    (N_F log-uniform in [4,096, 262,144], Poisson arrivals at 64 scenes/s, 16 GB budget) run
+    with continuous batching, and the same scenes one at a time on the plain path."""
+    from turbospharticles_b200 import scene as S, serve
+    specs = S.served_stream(n_scenes)
+    prepared = serve.prepare(specs)
+    sv = serve.run_served(prepared, steps, 16 << 30)
+    pl = serve.run_plain(prepared, steps)
+    return {"workload": f"served_stream_{n_scenes}x{steps}", "scenes": n_scenes, "steps_per_scene": steps,
+            "n_fluid_total": int(sum(sp.n_fluid for sp in specs)), "unit": UNIT,
+            "value": sv["value"], "value_wall": sv["value_wall"], "p50_step_ms": sv["p50_step_ms"],
+            "p99_step_ms": sv["p99_step_ms"], "mean_active_scenes": sv["mean_active_scenes"],
+            "plain_value": pl["value"], "plain_p50_step_ms": pl["p50_step_ms"],
+            "plain_p99_step_ms": pl["p99_step_ms"], "served_over_plain": round(sv["value"] / pl["value"], 3)}
 
 
 def cpu_baseline_from(be, p, dmin, dmax):
@@ -252,13 +277,17 @@ def cpu_baseline_from(be, p, dmin, dmax):
     o = OracleBackend(p, threads=threads)
     o.set_sim_domain_bounds(dmin, dmax)
     o.pull(st, p)
+    # bounded sample: whole steps until about 12 s of CPU work (at least 3 steps)
     t0 = time.perf_counter()
-    o.step(p)
+    steps, sweeps = 0, 0
+    while steps < 3 or time.perf_counter() - t0 < 12.0:
+        o.step(p)
+        steps += 1
+        sweeps += o.stats().solverIters - 1
     dt = time.perf_counter() - t0
-    iters = o.stats().solverIters - 1
-    return {"value": round(st.N_F / dt, 1), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"1 IISPH step of the 1M dam from the GPU state after warm-up ({iters} Jacobi sweeps, "
-                      f"{dt:.2f} s, oracle/ CPU restatement, OpenMP)"}
+    return {"value": round(st.N_F * steps / dt, 1), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} IISPH steps of the 1M dam from the GPU state after warm-up ({sweeps} Jacobi "
+                      f"sweeps, {dt:.1f} s, oracle/ CPU restatement, OpenMP over {threads} threads)"}
 
 
 def run_reference(args):
@@ -312,6 +341,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--served-scenes", type=int, default=64,
+                    help="scenes of the served-stream sub-measure (0: skip; 256 = the full stream)")
+    ap.add_argument("--served-steps", type=int, default=100)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     if args.impl == "reference":
