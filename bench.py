@@ -48,31 +48,46 @@ def init_dist(ws, backend):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 100 ms; sampling starts before the
+    timed region (the first sample is awaited) and only samples received inside the region
+    (`mark_start` .. `mark_end`, plus one interval of read-out lag) are summarised."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_S = 0.1
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.rows = []
         self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(int(self.INTERVAL_S * 1000))], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.perf_counter() + 3.0
+            while not self.rows and time.perf_counter() < deadline:
+                time.sleep(0.01)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            self.rows.append((time.perf_counter(), [x.strip() for x in line.split(",")]))
+
+    def mark_start(self):
+        self.t0 = time.perf_counter()
+
+    def mark_end(self):
+        self.t1 = time.perf_counter()
+        time.sleep(self.INTERVAL_S * 1.5)  # let the sample covering the end arrive
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -83,14 +98,18 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        lo = self.t0 if self.t0 is not None else float("-inf")
+        hi = (self.t1 + self.INTERVAL_S) if self.t1 is not None else float("inf")
+        inside = [r for t, r in self.rows if lo <= t <= hi]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        rows = inside
+        sm = [float(r[1]) for r in rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4) if r[5 + k] == "Active"})
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows)}
 
 
 def measured_peak_hbm():
@@ -153,14 +172,15 @@ def run_b200(args):
     stream = torch.cuda.ExternalStream(be.stream_handle(), device=dev)
     for _ in range(args.warmup):
         be.step(p)
-    # ---- device-timed region
-    barrier(dist, dev)
-    torch.cuda.synchronize(dev)
-    l0 = be.launch_count()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    # ---- device-timed region (clock sampling already running when it starts)
     step_ms, iters, phases = [], [], []
     with ClockSampler(local) as clk:
+        barrier(dist, dev)
+        torch.cuda.synchronize(dev)
+        l0 = be.launch_count()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        clk.mark_start()
         e0.record(stream)
         for _ in range(args.steps):
             be.step(p)
@@ -170,6 +190,7 @@ def run_b200(args):
             phases.append(be.phase_times())
         e1.record(stream)
         torch.cuda.synchronize(dev)
+        clk.mark_end()
     barrier(dist, dev)
     elapsed_ms = max_over_ranks(dist, e0.elapsed_time(e1), dev)
     launches = be.launch_count() - l0
@@ -336,7 +357,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")

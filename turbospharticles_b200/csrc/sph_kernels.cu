@@ -21,6 +21,15 @@ constexpr uint32_t SPH_THREADS = 256;
 #ifndef TSP_SPH_MIN_BLOCKS
 #define TSP_SPH_MIN_BLOCKS 4
 #endif
+// 1: grid of resident blocks only (warps loop over chunks); 0: one warp per chunk
+#ifndef TSP_SPH_PERSISTENT
+#define TSP_SPH_PERSISTENT 1
+#endif
+// 1: the list entries and gradient factors of the next slot group are loaded before the
+// gathers of the current group (one group of loads always in flight)
+#ifndef TSP_SPH_PIPELINE
+#define TSP_SPH_PIPELINE 0
+#endif
 
 struct ChunkCursor {
     uint32_t pitch, cnt, base, base2;
@@ -68,6 +77,45 @@ __device__ __forceinline__ void SweepSlots(const ChunkCursor& cur, const SellVie
 }
 
 // as SweepSlots, also loading each slot's recorded kernel-gradient factor (no sqrt / division)
+#if TSP_SPH_PIPELINE
+template <int U, bool TWO, typename Body>
+__device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellView& v, uint32_t lane,
+                                             const float4* A, const float4* B, Body&& body) {
+    uint32_t jn[U];
+    float kn[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const bool ok = (uint32_t)u < cur.cnt;
+        jn[u] = ok ? cur.nbr(v, u, lane) : EMPTY_32;
+        kn[u] = ok ? *cur.kgSlot(v, u, lane) : 0.0f;
+    }
+    for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
+        uint32_t j[U];
+        float kg[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) { j[u] = jn[u]; kg[u] = kn[u]; }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool ok = k0 + U + u < cur.cnt;
+            jn[u] = ok ? cur.nbr(v, k0 + U + u, lane) : EMPTY_32;
+            kn[u] = ok ? *cur.kgSlot(v, k0 + U + u, lane) : 0.0f;
+        }
+        float4 a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            a[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+            b[u] = a[u];
+            if (j[u] != EMPTY_32) {
+                a[u] = A[j[u]];
+                if (TWO) b[u] = B[j[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (j[u] != EMPTY_32) body(kg[u], a[u], b[u]);
+    }
+}
+#else
 template <int U, bool TWO, typename Body>
 __device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellView& v, uint32_t lane,
                                              const float4* A, const float4* B, Body&& body) {
@@ -95,6 +143,7 @@ __device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellV
             if (j[u] != EMPTY_32) body(kg[u], a[u], b[u]);
     }
 }
+#endif
 
 // persistent warps: warp w of the grid handles chunks w, w + W, w + 2W, ...
 #define FOR_EACH_CHUNK(n)                                                                  \
@@ -564,6 +613,7 @@ static uint32_t PersistentBlocks(K kernel, uint32_t n) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, SPH_THREADS, 0);
     if (perSM <= 0) perSM = 1;
     const uint32_t need = (n + SPH_THREADS - 1) / SPH_THREADS;
+    if (!TSP_SPH_PERSISTENT) return std::max(1u, need);
     return std::max(1u, std::min(need, (uint32_t)perSM * g_numSMs));
 }
 static inline uint32_t SphBlocks(uint32_t n) { return (n + SPH_THREADS - 1) / SPH_THREADS; }
