@@ -72,7 +72,11 @@ typedef struct tsp_params {
     float gridCellSizeRatio;
     uint32_t boundaryLayers;
     float cubicSplineAlphaOverride;   /* <= 0: derive from particleSizeF */
-    uint32_t reserved[4];
+    /* rigid contact solver (SolveRigidContacts, rigid_solver.cpp:602-799; parameters_sim.h:100-101);
+     * both 0 selects the reference defaults 0.001 and 100 */
+    float rigidContactDensityDevTarget;
+    uint32_t rigidContactMaxSolverIters;
+    uint32_t reserved[2];
 } tsp_params;
 
 /*
@@ -137,6 +141,19 @@ typedef struct tsp_step_stats {
     float lastJacobiMs;            /* of which Jacobi loop                              */
     uint32_t reserved1;
 } tsp_step_stats;
+
+/* CPU::RigidContactReport (source/simulation/CPU/backend/rigid_solver.h:25-30) of the last
+ * step's rigid contact solve, plus its contact counts (rigid particles with a contact after the
+ * per-body relaxation count + boundary particles in contact; boundary particles referenced by
+ * rigid neighbor rows) */
+typedef struct tsp_contact_report {
+    uint32_t solverIters;
+    float avgDensityError;
+    uint32_t converged;            /* 1 also when there was no contact */
+    uint32_t reserved;
+    uint64_t nContacts;
+    uint64_t nContactBoundary;
+} tsp_contact_report;
 
 typedef struct tsp_backend tsp_backend;
 
@@ -245,6 +262,8 @@ int tsp_b200_get_stream(const tsp_backend* h, void** stream);
  * read-back. *n = number written (0 before the first step). Analogue of the reference's
  * per-stage BenchOp timers (source/simulation/core/backend_sim.h:255, GetBenchOps). */
 int tsp_b200_get_phase_times(const tsp_backend* h, float* ms, uint32_t cap, uint32_t* n);
+/* SimBackend_CPU::GetRigidContactReport (cpu_backend.h:132) */
+int tsp_b200_get_contact_report(const tsp_backend* h, tsp_contact_report* out);
 /* number of CUDA kernels this backend launched since creation (graph nodes included) */
 int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count);
 

@@ -53,6 +53,12 @@ public:
         Check(tsp_b200_get_stats(h_, &s));
         return s;
     }
+    // SimBackend_CPU::GetRigidContactReport (source/simulation/CPU/backend/cpu_backend.h:132)
+    tsp_contact_report GetRigidContactReport() const {
+        tsp_contact_report r{};
+        Check(tsp_b200_get_contact_report(h_, &r));
+        return r;
+    }
     tsp_backend* Handle() const { return h_; }
 
 private:

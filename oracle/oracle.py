@@ -12,7 +12,7 @@ import subprocess
 
 import numpy as np
 
-from turbospharticles_b200.abi import (TspParams, TspStateView, TspStepStats, FIELD_COMPONENTS,
+from turbospharticles_b200.abi import (TspParams, TspStateView, TspStepStats, TspContactReport, FIELD_COMPONENTS,
                                        FIELD_BODY_FT)
 from turbospharticles_b200.state import UniversalSimState
 
@@ -43,6 +43,7 @@ def lib():
             "orc_neighbor_search": (C.c_int, [vp, C.POINTER(TspParams)]),
             "orc_step": (C.c_int, [vp, C.POINTER(TspParams), C.c_uint32]),
             "orc_get_stats": (C.c_int, [vp, C.POINTER(TspStepStats)]),
+            "orc_get_contact_report": (C.c_int, [vp, C.POINTER(TspContactReport)]),
             "orc_read_cell_ids": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32]),
             "orc_read_permutation": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32]),
             "orc_read_cell_table": (C.c_int, [vp, C.c_uint32, vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]),
@@ -122,6 +123,11 @@ class OracleBackend:
         s = TspStepStats()
         self._chk(self.L.orc_get_stats(self.h, C.byref(s)))
         return s
+
+    def contact_report(self) -> TspContactReport:
+        r = TspContactReport()
+        self._chk(self.L.orc_get_contact_report(self.h, C.byref(r)))
+        return r
 
     def cell_ids(self, species):
         n = self.counts[species]

@@ -43,6 +43,7 @@
 #include <stdexcept>
 #include <string>
 #include <vector>
+#include <unordered_map>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -274,6 +275,15 @@ template <typename T> struct Oracle {
     CSR rows[6];
     // solver state
     uint32_t iters = 0; T avgRaw = 0, avgPos = 0, avgAbs = 0; double eRaw = 0, ePos = 0, eAbs = 0;
+    // rigid contact solver state (rigid_solver.cpp)
+    std::vector<uint32_t> cLocalB;                 // contact boundary particle -> boundary index
+    std::vector<uint64_t> cOffRB, cOffBR;
+    std::vector<uint32_t> cIdxRB, cIdxBR;          // RB: contact indices; BR: rigid indices
+    std::vector<T> cRelWx, cRelWy, cRelWz, cIw[9];
+    std::vector<T> cDensR, cDiagR, cPresR, cSrcR, cErrR, cOmegaR, cFxR, cFyR, cFzR, cVxR, cVyR, cVzR;
+    std::vector<T> cDensB, cDiagB, cPresB, cSrcB, cErrB, cOmegaB;
+    std::vector<T> cFx, cFy, cFz, cTx, cTy, cTz;   // per body contact force / torque
+    uint32_t contactIters = 0; T contactAvgErr = 0; bool contactConverged = false; uint64_t contactCount = 0;
 
     T alpha() const {
         if (prm.cubicSplineAlphaOverride > 0.0f) return (T)prm.cubicSplineAlphaOverride;
@@ -896,12 +906,322 @@ template <typename T> struct Oracle {
         }
     }
 
+    // ------------------------------------------------------------------ rigid contacts
+    // RIGID_CONTACT_VOLUME_FACTOR (rigid_solver.h:23)
+    static constexpr float kContactVol = 0.7f;
+    // ContactKernel (rigid_solver.cpp:51-63): cubic-spline weight and scalar gradient
+    T ContactKernel(T dx, T dy, T dz, T& gx, T& gy, T& gz) const {
+        const T sInv = sizeInv(), r2 = (T)prm.kernelRadiusSqu, a = alpha();
+        const T d2 = fmaT(dx, dx, fmaT(dy, dy, dz * dz));
+        if (d2 >= r2) { gx = gy = gz = T(0); return T(0); }
+        const T q = std::sqrt(d2) * sInv;
+        const T t1 = std::max(T(1) - q, T(0)), t2 = std::max(T(2) - q, T(0));
+        GradScalar(dx, dy, dz, sInv, r2, a, gx, gy, gz);
+        return a * (t2 * t2 * t2 - T(4) * t1 * t1 * t1);
+    }
+    // BuildRigidBoundaryNeighbors (rigid_solver.cpp:90-149): contact boundary particles in order
+    // of first reference by the rigid particles' RB rows, RB rows as contact indices, BR rows
+    bool BuildContactNeighbors() {
+        cLocalB.clear(); cOffRB.clear(); cIdxRB.clear(); cOffBR.clear(); cIdxBR.clear();
+        std::unordered_map<uint32_t, uint32_t> toContact;
+        bool any = false;
+        const CSR& RB = rows[4];
+        const CSR& RR = rows[5];
+        for (uint32_t i = 0; i < NR; i++) {
+            const uint64_t b0 = RB.off[i], b1 = RB.off[i + 1];
+            if (cOffRB.empty()) {
+                if (b0 == b1) { any = any || RR.off[i + 1] > RR.off[i]; continue; }
+                cOffRB.assign((size_t)NR + 1, 0);
+                cOffBR.push_back(0);
+            }
+            for (uint64_t k = b0; k < b1; k++) {
+                const uint32_t b = RB.idx[k];
+                auto ins = toContact.emplace(b, (uint32_t)cLocalB.size());
+                if (ins.second) { cLocalB.push_back(b); cOffBR.push_back(0); }
+                const uint32_t c = ins.first->second;
+                cIdxRB.push_back(c);
+                cOffBR[c + 1]++;
+            }
+            cOffRB[i + 1] = cIdxRB.size();
+        }
+        if (cOffRB.empty()) return any;
+        const uint32_t nc = (uint32_t)cLocalB.size();
+        for (uint32_t c = 0; c < nc; c++) cOffBR[c + 1] += cOffBR[c];
+        cIdxBR.assign(cOffBR.back(), 0);
+        std::vector<uint64_t> w(cOffBR.begin(), cOffBR.end() - 1);
+        for (uint32_t i = 0; i < NR; i++)
+            for (uint64_t k = cOffRB[i]; k < cOffRB[i + 1]; k++) cIdxBR[w[cIdxRB[k]]++] = i;
+        return true;
+    }
+    // ForEachContactNeighbor (rigid_solver.cpp:22-48): BR row of a boundary contact; RR then RB
+    // row of a rigid particle. f(j, neighborIsBoundary) with j a rigid or contact index.
+    template <class Fn> void ForEachContact(bool boundary, uint32_t i, const Fn& f) const {
+        if (boundary) {
+            for (uint64_t k = cOffBR[i]; k < cOffBR[i + 1]; k++) f(cIdxBR[k], false);
+            return;
+        }
+        const CSR& RR = rows[5];
+        for (uint64_t k = RR.off[i]; k < RR.off[i + 1]; k++) f(RR.idx[k], false);
+        if (!cOffRB.empty())
+            for (uint64_t k = cOffRB[i]; k < cOffRB[i + 1]; k++) f(cIdxRB[k], true);
+    }
+    T CPosX(bool boundary, uint32_t j) const { return boundary ? xB[cLocalB[j]] : xR[j]; }
+    T CPosY(bool boundary, uint32_t j) const { return boundary ? yB[cLocalB[j]] : yR[j]; }
+    T CPosZ(bool boundary, uint32_t j) const { return boundary ? zB[cLocalB[j]] : zR[j]; }
+    T CVol(bool boundary, uint32_t j) const { return boundary ? volB[cLocalB[j]] : volR[j]; }
+    // RigidContactGeometry (rigid_solver.cpp:151-227)
+    void ContactGeometry() {
+        for (int k = 0; k < 9; k++) cIw[k].assign(NRB, T(0));
+        for (uint32_t b = 0; b < NRB; b++) {
+            T t[9];
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++)
+                    t[r * 3 + c] = A[r * 3 + 0][b] * Ib[0 * 3 + c][b] + A[r * 3 + 1][b] * Ib[1 * 3 + c][b] +
+                                   A[r * 3 + 2][b] * Ib[2 * 3 + c][b];
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++)
+                    cIw[r * 3 + c][b] = t[r * 3 + 0] * A[c * 3 + 0][b] + t[r * 3 + 1] * A[c * 3 + 1][b] +
+                                        t[r * 3 + 2] * A[c * 3 + 2][b];
+        }
+        cRelWx.assign(NR, T(0)); cRelWy.assign(NR, T(0)); cRelWz.assign(NR, T(0));
+        for (uint32_t i = 0; i < NR; i++) {
+            const uint32_t b = bodyR[i];
+            const T lx = xRel[i], ly = yRel[i], lz = zRel[i];
+            cRelWx[i] = fmaT(A[0][b], lx, fmaT(A[1][b], ly, A[2][b] * lz));
+            cRelWy[i] = fmaT(A[3][b], lx, fmaT(A[4][b], ly, A[5][b] * lz));
+            cRelWz[i] = fmaT(A[6][b], lx, fmaT(A[7][b], ly, A[8][b] * lz));
+        }
+    }
+    struct BodyGrad { uint32_t b; T x, y, z, tx, ty, tz; };
+    static void AddBodyGrad(std::vector<BodyGrad>& g, uint32_t b, T x, T y, T z, T rx, T ry, T rz) {
+        auto it = std::find_if(g.begin(), g.end(), [&](const BodyGrad& e) { return e.b == b; });
+        if (it == g.end()) { g.push_back({b, T(0), T(0), T(0), T(0), T(0), T(0)}); it = g.end() - 1; }
+        it->x += x; it->y += y; it->z += z;
+        it->tx += ry * z - rz * y;
+        it->ty += rz * x - rx * z;
+        it->tz += rx * y - ry * x;
+    }
+    // RigidContactDensityAndDiagonal (rigid_solver.cpp:229-344)
+    void ContactDensityAndDiagonal(bool boundary) {
+        const uint32_t N = boundary ? (uint32_t)cLocalB.size() : NR;
+        auto& dens = boundary ? cDensB : cDensR;
+        auto& diag = boundary ? cDiagB : cDiagR;
+        auto& pres = boundary ? cPresB : cPresR;
+        auto& src = boundary ? cSrcB : cSrcR;
+        auto& omg = boundary ? cOmegaB : cOmegaR;
+        dens.assign(N, T(0)); diag.assign(N, T(0)); pres.assign(N, T(0)); src.assign(N, T(0)); omg.assign(N, T(0));
+        const T dt = (T)prm.timeStep;
+        std::vector<BodyGrad> g;
+        for (uint32_t i = 0; i < N; i++) {
+            g.clear();
+            const T volRest = T(kContactVol) * CVol(boundary, i);
+            T rho = T(kContactVol);
+            bool has = false;
+            const T px = CPosX(boundary, i), py = CPosY(boundary, i), pz = CPosZ(boundary, i);
+            ForEachContact(boundary, i, [&](uint32_t j, bool nb) {
+                T gx, gy, gz;
+                const T w = ContactKernel(px - CPosX(nb, j), py - CPosY(nb, j), pz - CPosZ(nb, j), gx, gy, gz);
+                if (!(w > T(0))) return;
+                has = true;
+                const T nv = T(kContactVol) * CVol(nb, j);
+                rho += nv * w;
+                gx *= nv; gy *= nv; gz *= nv;
+                if (!boundary) AddBodyGrad(g, bodyR[i], gx, gy, gz, cRelWx[i], cRelWy[i], cRelWz[i]);
+                if (!nb) AddBodyGrad(g, bodyR[j], -gx, -gy, -gz, cRelWx[j], cRelWy[j], cRelWz[j]);
+            });
+            double d = 0.0;
+            for (const BodyGrad& e : g) {
+                const uint32_t b = e.b;
+                const T wx = cIw[0][b] * e.tx + cIw[1][b] * e.ty + cIw[2][b] * e.tz;
+                const T wy = cIw[3][b] * e.tx + cIw[4][b] * e.ty + cIw[5][b] * e.tz;
+                const T wz = cIw[6][b] * e.tx + cIw[7][b] * e.ty + cIw[8][b] * e.tz;
+                d += (double)(massInv[b] * (e.x * e.x + e.y * e.y + e.z * e.z) + e.tx * wx + e.ty * wy + e.tz * wz);
+            }
+            const double dv = (double)dt * (double)dt * (double)volRest / (double)(rho * rho) * d;
+            diag[i] = (T)dv;
+            if (!std::isfinite((double)diag[i]) || diag[i] < T(0))
+                throw std::runtime_error("Invalid rigid contact diagonal.");
+            dens[i] = rho; pres[i] = T(0); src[i] = rho - T(1); omg[i] = has ? T(0.5f) : T(0);
+        }
+    }
+    // RigidContactRelaxation (rigid_solver.cpp:346-407)
+    uint64_t ContactRelaxation() {
+        uint64_t n = 0;
+        for (uint32_t b = 0; b < NRB; b++) {
+            uint32_t count = 0;
+            for (uint32_t w = byBodyOff[b]; w < byBodyOff[b + 1]; w++) count += cOmegaR[byBodyIdx[w]] > T(0);
+            if (count == 0) continue;
+            for (uint32_t w = byBodyOff[b]; w < byBodyOff[b + 1]; w++) cOmegaR[byBodyIdx[w]] /= (T)count;
+            n += count;
+        }
+        const uint32_t NC = (uint32_t)cLocalB.size();
+        if (NC == 0) return n;
+        std::vector<uint32_t> perBody(NRB, 0), last(NRB, NC);
+        for (uint32_t c = 0; c < NC; c++) {
+            if (cOmegaB[c] <= T(0)) continue;
+            n++;
+            if (cDiagB[c] <= T(0)) continue;
+            for (uint64_t k = cOffBR[c]; k < cOffBR[c + 1]; k++) {
+                const uint32_t b = bodyR[cIdxBR[k]];
+                if (massInv[b] <= T(0) || last[b] == c) continue;
+                last[b] = c;
+                perBody[b]++;
+            }
+        }
+        for (uint32_t c = 0; c < NC; c++) {
+            if (cOmegaB[c] <= T(0) || cDiagB[c] <= T(0)) continue;
+            uint32_t mx = 0;
+            for (uint64_t k = cOffBR[c]; k < cOffBR[c + 1]; k++) mx = std::max(mx, perBody[bodyR[cIdxBR[k]]]);
+            if (mx > 0) cOmegaB[c] /= (T)mx;
+        }
+        return n;
+    }
+    // RigidContactPressureForces (rigid_solver.cpp:409-460)
+    void ContactPressureForces() {
+        cFxR.assign(NR, T(0)); cFyR.assign(NR, T(0)); cFzR.assign(NR, T(0));
+        for (uint32_t i = 0; i < NR; i++) {
+            T fx = 0, fy = 0, fz = 0;
+            const T pi = cPresR[i] / (cDensR[i] * cDensR[i]);
+            ForEachContact(false, i, [&](uint32_t j, bool nb) {
+                T gx, gy, gz;
+                const T w = ContactKernel(xR[i] - CPosX(nb, j), yR[i] - CPosY(nb, j), zR[i] - CPosZ(nb, j), gx, gy, gz);
+                if (!(w > T(0))) return;
+                const T rho = nb ? cDensB[j] : cDensR[j];
+                const T pj = (nb ? cPresB[j] : cPresR[j]) / (rho * rho);
+                const T c = -T(kContactVol) * volR[i] * T(kContactVol) * CVol(nb, j) * (pi + pj);
+                fx += c * gx; fy += c * gy; fz += c * gz;
+            });
+            cFxR[i] = fx; cFyR[i] = fy; cFzR[i] = fz;
+        }
+    }
+    // ReduceRigidParticleForcesToBody(Contact) (cpu_backend.cpp:2089-2172)
+    void ReduceContactForces() {
+        cFx.assign(NRB, T(0)); cFy.assign(NRB, T(0)); cFz.assign(NRB, T(0));
+        cTx.assign(NRB, T(0)); cTy.assign(NRB, T(0)); cTz.assign(NRB, T(0));
+        for (uint32_t b = 0; b < NRB; b++) {
+            T fx = 0, fy = 0, fz = 0, tx = 0, ty = 0, tz = 0;
+            for (uint32_t w = byBodyOff[b]; w < byBodyOff[b + 1]; w++) {
+                const uint32_t i = byBodyIdx[w];
+                const T lx = xRel[i], ly = yRel[i], lz = zRel[i];
+                const T rx = fmaT(A[0][b], lx, fmaT(A[1][b], ly, A[2][b] * lz));
+                const T ry = fmaT(A[3][b], lx, fmaT(A[4][b], ly, A[5][b] * lz));
+                const T rz = fmaT(A[6][b], lx, fmaT(A[7][b], ly, A[8][b] * lz));
+                fx += cFxR[i]; fy += cFyR[i]; fz += cFzR[i];
+                tx += ry * cFzR[i] - rz * cFyR[i]; ty += rz * cFxR[i] - rx * cFzR[i]; tz += rx * cFyR[i] - ry * cFxR[i];
+            }
+            cFx[b] += fx; cFy[b] += fy; cFz[b] += fz; cTx[b] += tx; cTy[b] += ty; cTz[b] += tz;
+        }
+    }
+    // RigidContactParticleVelocities (rigid_solver.cpp:462-506)
+    void ContactParticleVelocities() {
+        const T dt = (T)prm.timeStep;
+        cVxR.assign(NR, T(0)); cVyR.assign(NR, T(0)); cVzR.assign(NR, T(0));
+        for (uint32_t i = 0; i < NR; i++) {
+            const uint32_t b = bodyR[i];
+            const T tx = cTx[b], ty = cTy[b], tz = cTz[b];
+            const T wx = cIw[0][b] * tx + cIw[1][b] * ty + cIw[2][b] * tz;
+            const T wy = cIw[3][b] * tx + cIw[4][b] * ty + cIw[5][b] * tz;
+            const T wz = cIw[6][b] * tx + cIw[7][b] * ty + cIw[8][b] * tz;
+            const T rx = cRelWx[i], ry = cRelWy[i], rz = cRelWz[i];
+            cVxR[i] = dt * (massInv[b] * cFx[b] + wy * rz - wz * ry);
+            cVyR[i] = dt * (massInv[b] * cFy[b] + wz * rx - wx * rz);
+            cVzR[i] = dt * (massInv[b] * cFz[b] + wx * ry - wy * rx);
+        }
+    }
+    // RigidContactDensityError (rigid_solver.cpp:508-579), velocities of rigid particles given
+    double ContactDensityError(const std::vector<T>& vxr, const std::vector<T>& vyr, const std::vector<T>& vzr) {
+        const T dt = (T)prm.timeStep;
+        double sum = 0.0;
+        for (int pass = 0; pass < 2; pass++) {
+            const bool boundary = pass == 1;
+            const uint32_t N = boundary ? (uint32_t)cLocalB.size() : NR;
+            const auto& src = boundary ? cSrcB : cSrcR;
+            const auto& pres = boundary ? cPresB : cPresR;
+            auto& err = boundary ? cErrB : cErrR;
+            err.assign(N, T(0));
+            for (uint32_t i = 0; i < N; i++) {
+                const T vx = boundary ? T(0) : vxr[i], vy = boundary ? T(0) : vyr[i], vz = boundary ? T(0) : vzr[i];
+                const T px = CPosX(boundary, i), py = CPosY(boundary, i), pz = CPosZ(boundary, i);
+                T res = src[i];
+                ForEachContact(boundary, i, [&](uint32_t j, bool nb) {
+                    T gx, gy, gz;
+                    const T w = ContactKernel(px - CPosX(nb, j), py - CPosY(nb, j), pz - CPosZ(nb, j), gx, gy, gz);
+                    if (!(w > T(0))) return;
+                    const T dvx = (nb ? T(0) : vxr[j]) - vx, dvy = (nb ? T(0) : vyr[j]) - vy, dvz = (nb ? T(0) : vzr[j]) - vz;
+                    const T div = dt * (dvx * gx + dvy * gy + dvz * gz);
+                    res -= T(kContactVol) * CVol(nb, j) * div;
+                });
+                if (!std::isfinite((double)res)) throw std::runtime_error("Non-finite rigid contact density error.");
+                err[i] = res;
+                sum += pres[i] > T(0) ? std::abs((double)res) : std::max((double)res, 0.0);
+            }
+        }
+        return sum;
+    }
+    // RigidContactPressureRelaxedJacobi (rigid_solver.cpp:581-600)
+    static void ContactJacobi(const std::vector<T>& err, const std::vector<T>& diag, const std::vector<T>& omg,
+                              std::vector<T>& pres) {
+        for (size_t i = 0; i < pres.size(); i++) {
+            if (!(diag[i] > T(0))) continue;
+            const T p = pres[i] + omg[i] * err[i] / diag[i];
+            if (!std::isfinite((double)p)) throw std::runtime_error("Non-finite rigid contact pressure.");
+            pres[i] = std::max(T(0), p);
+        }
+    }
+    T ContactTarget() const {
+        return (prm.rigidContactDensityDevTarget == 0.0f && prm.rigidContactMaxSolverIters == 0)
+                   ? T(0.001f) : (T)prm.rigidContactDensityDevTarget;
+    }
+    uint32_t ContactMaxIters() const {
+        return (prm.rigidContactDensityDevTarget == 0.0f && prm.rigidContactMaxSolverIters == 0)
+                   ? 100u : prm.rigidContactMaxSolverIters;
+    }
+    // SolveRigidContacts (rigid_solver.cpp:602-799)
+    void SolveRigidContacts() {
+        const T target = ContactTarget();
+        const uint32_t maxIters = ContactMaxIters();
+        if (!std::isfinite((double)target) || target <= T(0) || maxIters == 0)
+            throw std::runtime_error("Invalid rigid contact solver tolerance or iteration limit.");
+        contactIters = 0; contactAvgErr = T(0); contactConverged = true; contactCount = 0;
+        const bool has = BuildContactNeighbors();
+        const uint32_t NC = (uint32_t)cLocalB.size();
+        cDensB.assign(NC, T(0)); cDiagB.assign(NC, T(0)); cPresB.assign(NC, T(0)); cSrcB.assign(NC, T(0));
+        cErrB.assign(NC, T(0)); cOmegaB.assign(NC, T(0));
+        if (!has) return;
+        ContactGeometry();
+        ContactDensityAndDiagonal(false);
+        ContactDensityAndDiagonal(true);
+        contactCount = ContactRelaxation();
+        // source motion: external and fluid forces, no contact forces
+        PredictBodies();
+        UpdateRigidParticles(true);
+        (void)ContactDensityError(vpxR, vpyR, vpzR);
+        cSrcR.swap(cErrR);
+        cSrcB.swap(cErrB);
+        for (;;) {
+            ContactPressureForces();
+            ReduceContactForces();
+            ContactParticleVelocities();
+            const double e = ContactDensityError(cVxR, cVyR, cVzR);
+            contactAvgErr = contactCount > 0 ? (T)(float)(e / (double)contactCount) : T(0);
+            contactConverged = contactAvgErr <= target;
+            if (contactConverged || contactIters == maxIters) break;
+            ContactJacobi(cErrR, cDiagR, cOmegaR, cPresR);
+            ContactJacobi(cErrB, cDiagB, cOmegaB, cPresB);
+            contactIters++;
+        }
+        for (uint32_t b = 0; b < NRB; b++) {
+            Fx[b] += cFx[b]; Fy[b] += cFy[b]; Fz[b] += cFz[b];
+            Tx[b] += cTx[b]; Ty[b] += cTy[b]; Tz[b] += cTz[b];
+        }
+    }
+
     // ------------------------------------------------------------------ drivers
     void NeighborSearch() {  // cpu_backend.cpp:1593-1624
         ReorderAndConstruct(true);
         Query();
     }
-    void Step() {  // sph_solver.cpp:34-319 (serial, no contact solve)
+    void Step() {  // sph_solver.cpp:34-319 (serial)
         if (NF == 0 && NRB == 0) { return; }
         ReorderAndConstruct(false);
         Query();
@@ -938,6 +1258,7 @@ template <typename T> struct Oracle {
         }
         Integration();
         if (NRB > 0) {
+            SolveRigidContacts();
             PredictBodies();
             IntegrateBodies();
             UpdateRigidParticles(false);
@@ -1141,6 +1462,16 @@ int orc_step(orc_handle* h, const tsp_params* p, uint32_t n) {
     ORC_TRY(h, ORC_DISPATCH(h, {
         O.prm = *p;
         for (uint32_t s = 0; s < n; s++) { O.Step(); O.step += 1; O.time += (double)p->timeStep; }
+    }))
+}
+int orc_get_contact_report(orc_handle* h, tsp_contact_report* r) {
+    ORC_TRY(h, ORC_DISPATCH(h, {
+        std::memset(r, 0, sizeof(*r));
+        r->solverIters = O.contactIters;
+        r->avgDensityError = (float)O.contactAvgErr;
+        r->converged = O.contactConverged ? 1u : 0u;
+        r->nContacts = O.contactCount;
+        r->nContactBoundary = O.cLocalB.size();
     }))
 }
 int orc_get_stats(orc_handle* h, tsp_step_stats* st) {

@@ -88,3 +88,61 @@ def test_gpu_rigid_free_fall_known_answer():
     from turbospharticles_b200.params import dam_params
     p = dam_params(0.02, 1e-3)
     check_free_fall(SimBackendB200(p), p, lone_cube(p))
+
+
+# ---- rigid contact solver (SolveRigidContacts, rigid_solver.cpp:602-799)
+def test_gpu_contact_idle_without_contact():
+    from test_oracle_rigid import lone_cube
+    from turbospharticles_b200.params import dam_params
+    p = dam_params(0.02, 1e-3)
+    g = SimBackendB200(p)
+    g.pull(lone_cube(p), p)
+    g.step(p)
+    r = g.contact_report()
+    assert r.solverIters == 0 and r.converged == 1 and r.nContacts == 0
+
+
+def test_gpu_contact_pair_conserves_momentum():
+    from test_oracle_rigid import pressed_pair, run_pair
+    from turbospharticles_b200.params import dam_params
+    p = dam_params(0.02, 1e-3)
+    p.gravity = (0.0, 0.0, 0.0)
+    st = pressed_pair(p)
+    out, reports = run_pair(SimBackendB200(p), p, st)
+    o_out, o_rep = run_pair(OracleBackend(p), p, st)
+    assert all(abs(a.solverIters - b.solverIters) <= 1 for a, b in zip(reports, o_rep))
+    assert reports[0].nContacts == o_rep[0].nContacts
+    m = st.massRB.astype(np.float64)
+    px = float(np.sum(m * out.xVelRB))
+    assert abs(px) <= 1e-5 * float(np.max(np.abs(m * out.xVelRB)))
+    assert out.xVelRB[0] < 0.0 < out.xVelRB[1]
+    close(out.xVelRB, o_out.xVelRB, 2e-3, "separation velocities vs oracle")
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_gpu_contact_matches_oracle(fp64):
+    """Stacked cubes pressed into the floor and each other: per-step contact iteration counts
+    (within one of the oracle's), the contact set of the first step, and the body states after
+    four steps against the FP32 and the FP64 oracle."""
+    st, dmin, dmax, p = S.stacked_cubes()
+    g, o = SimBackendB200(p), OracleBackend(p, fp64=fp64)
+    for be in (g, o):
+        be.set_sim_domain_bounds(dmin, dmax)
+        be.pull(st, p)
+        be.run_stage(abi.STAGE_BOUNDARY_VOLUMES, p)
+    iters_g, iters_o = [], []
+    for k in range(4):
+        g.step(p)
+        o.step(p)
+        rg, ro = g.contact_report(), o.contact_report()
+        if k == 0:
+            assert rg.nContactBoundary == ro.nContactBoundary
+            assert rg.nContacts == ro.nContacts
+        iters_g.append(rg.solverIters)
+        iters_o.append(ro.solverIters)
+    assert max(iters_o) > 0
+    assert all(abs(a - b) <= 1 for a, b in zip(iters_g, iters_o)), (iters_g, iters_o)
+    gs, os_ = g.push(), o.push()
+    for n, tol in (("xCM", 1e-5), ("yCM", 1e-4), ("zCM", 1e-5), ("xVelRB", 2e-2), ("yVelRB", 2e-2),
+                   ("zOmegaRB", 2e-2)):
+        close(getattr(gs, n), getattr(os_, n), tol, n)

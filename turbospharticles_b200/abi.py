@@ -51,7 +51,8 @@ class TspParams(C.Structure):
         ("jacobiWarmStart", _f), ("densityDevTarget", _f),
         ("fixedIters", _u32), ("minSolverIters", _u32), ("maxSolverIters", _u32),
         ("solverTerminationCond", _u32), ("gridCellSizeRatio", _f), ("boundaryLayers", _u32),
-        ("cubicSplineAlphaOverride", _f), ("reserved", _u32 * 4),
+        ("cubicSplineAlphaOverride", _f), ("rigidContactDensityDevTarget", _f),
+        ("rigidContactMaxSolverIters", _u32), ("reserved", _u32 * 2),
     ]
 
 
@@ -104,6 +105,12 @@ class TspStepStats(C.Structure):
 
 
 # every exported entry point of include/tsp_b200.h, with its ctypes signature
+class TspContactReport(C.Structure):
+    """tsp_contact_report (CPU::RigidContactReport, rigid_solver.h:25-30, + contact counts)."""
+    _fields_ = [("solverIters", _u32), ("avgDensityError", _f), ("converged", _u32), ("reserved", _u32),
+                ("nContacts", C.c_uint64), ("nContactBoundary", C.c_uint64)]
+
+
 _VP = C.c_void_p
 EXPORTS = {
     "tsp_b200_create": (C.c_int, [C.POINTER(TspParams), C.c_int, C.POINTER(_VP)]),
@@ -132,6 +139,7 @@ EXPORTS = {
     "tsp_b200_time_stage": (C.c_int, [_VP, C.POINTER(TspParams), _u32, _u32, _pf]),
     "tsp_b200_get_launch_count": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
     "tsp_b200_get_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
+    "tsp_b200_get_contact_report": (C.c_int, [_VP, C.POINTER(TspContactReport)]),
     "tsp_b200_get_phase_times": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32)]),
     "tsp_b200_try_build_cell_frame": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                                  C.POINTER(C.c_uint32)]),

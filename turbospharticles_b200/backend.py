@@ -183,6 +183,12 @@ class SimBackendB200:
         self._chk(self.L.tsp_b200_time_stage(self.h, self._cparams(params), stage, reps, C.byref(ms)))
         return ms.value
 
+    def contact_report(self):
+        """Rigid contact solve of the last step (GetRigidContactReport, cpu_backend.h:132)."""
+        r = abi.TspContactReport()
+        self._chk(self.L.tsp_b200_get_contact_report(self.h, C.byref(r)))
+        return r
+
     def phase_times(self) -> dict:
         """Device milliseconds of the phases of the last step (empty before the first step)."""
         buf = (C.c_float * len(abi.PHASE_NAMES))()

@@ -88,6 +88,8 @@ struct HostMirror {
     uint64_t nCells[3];
     SolverState st;
     uint32_t err;
+    ContactState contact;
+    uint64_t contactTot[2];
 };
 
 class Backend {
@@ -174,6 +176,19 @@ public:
         cudaGraphExec_t ex = nullptr;
     };
     std::vector<JacobiGraph> graphs;
+    // rigid contact solver (rigid_solver.cpp): per rigid particle, per contact boundary particle
+    // (capacity contactCap, grow-only), per body; the contact loop runs in its own WHILE graph
+    DBuf<uint32_t> cOfB, cLocalB, cIdxRB, cIdxBR, cCurBR, cPerBody;
+    DBuf<uint64_t> cOffBR, cTot;
+    DBuf<float4> cRelW, cForce, cVel;
+    DBuf<float> cIw, cDensR, cDiagR, cPresR, cSrcR, cErrR, cOmegaR;
+    DBuf<float> cDensB, cDiagB, cPresB, cSrcB, cErrB, cOmegaB;
+    DBuf<double> cFT, cContrib;
+    DBuf<ContactState> cState;
+    uint32_t contactCap = 0, lastContactB = 0;
+    bool contactRan = false;
+    std::vector<JacobiGraph> cgraphs;
+    size_t cgraphNext = 0;
     DBuf<float> stage;  // device staging of the SoA <-> packed conversions at the state boundary (grow-only)
     size_t graphNext = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -215,10 +230,11 @@ public:
     ~Backend() {
         cudaSetDevice(device);
         if (s) cudaStreamSynchronize(s);
-        for (auto& g : graphs) {
-            if (g.ex) cudaGraphExecDestroy(g.ex);
-            if (g.g) cudaGraphDestroy(g.g);
-        }
+        for (auto* gs : {&graphs, &cgraphs})
+            for (auto& g : *gs) {
+                if (g.ex) cudaGraphExecDestroy(g.ex);
+                if (g.g) cudaGraphDestroy(g.g);
+            }
         for (auto& e : ev) if (e) cudaEventDestroy(e);
         for (auto& e : pev) if (e) cudaEventDestroy(e);
         if (hm) cudaFreeHost(hm);
@@ -236,6 +252,10 @@ public:
         if (e & (ERR_RIGID_ORIENT | ERR_RIGID_ATTACH))
             throw Error(TSP_ERR_RIGID, (e & ERR_RIGID_ORIENT) ? "Degenerate rigid body orientation."
                                                                : "Invalid rigid particle attachment.");
+        if (e & ERR_CONTACT_INVALID)
+            throw Error(TSP_ERR_RIGID, "Invalid rigid contact diagonal, density error or pressure.");
+        if (e & ERR_CONTACT_BODIES)
+            throw Error(TSP_ERR_UNSUPPORTED, "a rigid contact particle touches more than 8 bodies");
         if (e & ERR_QUERY_CAP) throw Error(TSP_ERR_UNSUPPORTED, "query stencil exceeds the shared-memory staging");
         if (e & ERR_COUNT_U16) throw Error(TSP_ERR_OVERFLOW, "a neighbor count exceeds uint16 storage");
         throw Error(TSP_ERR_NEIGHBOR_LIST, "SELL32 neighbor-list fill overflow / delta range error");
@@ -734,6 +754,128 @@ public:
         return ex;
     }
 
+    // -------------------------------------------------------------------------- rigid contacts
+    ContactDev ContactView() {
+        ContactDev d{};
+        d.nR = nR; d.nRB = nRB;
+        d.nContactB = reinterpret_cast<const uint32_t*>(cTot.p);  // low word of the scan total
+        d.offRR = offR[2].p; d.listRR = listR[2].p; d.offRB = offR[1].p; d.listRB = listR[1].p;
+        d.idxRB = cIdxRB.p; d.contactOfB = cOfB.p; d.localB = cLocalB.p;
+        d.offBR = cOffBR.p; d.idxBR = cIdxBR.p; d.curBR = cCurBR.p;
+        d.posR = posR.p; d.relR = relR.p; d.bodyR = bodyR.p; d.byBodyOff = byBodyOff.p; d.byBodyIdx = byBodyIdx.p;
+        d.posB = posB.p; d.volB = volB.p; d.bodyState = bodyState.p; d.bodyFT = bodyFT.p;
+        d.relW = cRelW.p; d.iw = cIw.p;
+        d.densR = cDensR.p; d.diagR = cDiagR.p; d.presR = cPresR.p; d.srcR = cSrcR.p; d.errR = cErrR.p;
+        d.omegaR = cOmegaR.p; d.forceC = cForce.p; d.velC = cVel.p;
+        d.densB = cDensB.p; d.diagB = cDiagB.p; d.presB = cPresB.p; d.srcB = cSrcB.p; d.errB = cErrB.p;
+        d.omegaB = cOmegaB.p;
+        d.ftC = cFT.p; d.perBody = cPerBody.p; d.contrib = cContrib.p; d.st = cState.p; d.err = err.p;
+        return d;
+    }
+    std::vector<uint64_t> ContactKey(const Consts& c) {
+        std::vector<uint64_t> k;
+        const ContactDev d = ContactView();
+        const uint64_t* w = reinterpret_cast<const uint64_t*>(&d);
+        static_assert(sizeof(ContactDev) % 8 == 0, "ContactDev holds 8-byte fields only after its two counts");
+        for (size_t i = 0; i < sizeof(ContactDev) / 8; i++) k.push_back(w[i]);
+        const uint32_t* cw = reinterpret_cast<const uint32_t*>(&c);
+        for (size_t i = 0; i < sizeof(Consts) / 4; i++) k.push_back(cw[i]);
+        k.push_back(contactCap);
+        return k;
+    }
+    cudaGraphExec_t ContactGraphFor(const Consts& c) {
+        std::vector<uint64_t> key = ContactKey(c);
+        for (auto& g : cgraphs)
+            if (g.ex && g.key == key) return g.ex;
+        cudaGraph_t graph;
+        CK(cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle handle;
+        CK(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamBeginCaptureToGraph(capStream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        LaunchContactIteration(ContactView(), c, contactCap, (unsigned long long)handle, capStream);
+        cudaGraph_t captured;
+        CK(cudaStreamEndCapture(capStream, &captured));
+        cudaGraphExec_t ex;
+        CK(cudaGraphInstantiate(&ex, graph, 0));
+        if (cgraphs.size() < 2) cgraphs.push_back({});
+        JacobiGraph& slot = cgraphs[cgraphNext % cgraphs.size()];
+        cgraphNext++;
+        if (slot.ex) cudaGraphExecDestroy(slot.ex);
+        if (slot.g) cudaGraphDestroy(slot.g);
+        slot.key = std::move(key); slot.g = graph; slot.ex = ex;
+        return ex;
+    }
+    // SolveRigidContacts (rigid_solver.cpp:602-799), between the fluid integration and the rigid
+    // predictor/integrator of the step
+    void SolveRigidContacts(const Consts& c, const RigidParticlesDev& rp, const BodyDev& bd) {
+        const bool defaults = prm.rigidContactDensityDevTarget == 0.0f && prm.rigidContactMaxSolverIters == 0;
+        const float target = defaults ? 0.001f : prm.rigidContactDensityDevTarget;
+        const uint32_t maxIters = defaults ? 100u : prm.rigidContactMaxSolverIters;
+        if (!std::isfinite(target) || target <= 0.0f || maxIters == 0)
+            throw Error(TSP_ERR_INVALID, "Invalid rigid contact solver tolerance or iteration limit.");
+        if (maxIters > MAX_JACOBI_SWEEPS) throw Error(TSP_ERR_UNSUPPORTED, "contact iteration limit above 100000");
+        contactRan = false;
+        lastContactB = 0;
+        std::memset(&hm->contact, 0, sizeof(ContactState));
+        hm->contact.converged = 1u;
+        const uint64_t nRBe = csrN[1], nRRe = csrN[2];
+        if (nRBe == 0 && nRRe == 0) return;  // BuildRigidBoundaryNeighbors found no contact
+        // contact set: boundary particles referenced by rigid RB rows, ascending
+        cOfB.ensure(std::max<uint32_t>(nB, 1)); cLocalB.ensure(std::max<uint32_t>(nB, 1));
+        cIdxRB.ensure(std::max<uint64_t>(nRBe, 1)); cIdxBR.ensure(std::max<uint64_t>(nRBe, 1));
+        cTot.ensure(2);
+        CK(cudaMemsetAsync(cTot.p, 0, 2 * sizeof(uint64_t), s));
+        ContactDev d0 = ContactView();
+        if (nB) LaunchContactSetup(d0, nRBe, nB, scanScratch.p, cTot.p, s);
+        CK(cudaMemcpyAsync(hm->contactTot, cTot.p, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        Sync();
+        const uint32_t nc = (uint32_t)hm->contactTot[0];
+        if (nc > contactCap || !cDensB.p) {
+            contactCap = std::max<uint32_t>(nc + nc / 2 + 64, contactCap);
+            for (auto* b : {&cDensB, &cDiagB, &cPresB, &cSrcB, &cErrB, &cOmegaB}) b->ensure(contactCap);
+            cCurBR.ensure(contactCap); cOffBR.ensure(contactCap + 1ull);
+        }
+        const uint32_t nr1 = std::max<uint32_t>(nR, 1), nb1 = std::max<uint32_t>(nRB, 1);
+        cRelW.ensure(nr1); cForce.ensure(nr1); cVel.ensure(nr1);
+        for (auto* b : {&cDensR, &cDiagR, &cPresR, &cSrcR, &cErrR, &cOmegaR}) b->ensure(nr1);
+        cIw.ensure(9ull * nb1); cFT.ensure(6ull * nb1); cPerBody.ensure(nb1);
+        cContrib.ensure((uint64_t)nR + contactCap);
+        cState.ensure(1);
+        ContactDev d = ContactView();
+        LaunchContactLists(d, nRBe, nc, scanScratch.p, cTot.p + 1, s);
+        LaunchContactPrepare(d, c, nc, target, maxIters, s);
+        // predicted motion from external and fluid loads, no contact loads
+        LaunchRigidPredict(bd, prm.timeStep, s);
+        LaunchRigidUpdateParticles(rp, bd, true, err.p, s);
+        LaunchContactInitialError(d, c, nc, velPredR.p, s);
+        // the predicted-motion error becomes the source term (the reference swaps the vectors)
+        Swap(cSrcR, cErrR);
+        Swap(cSrcB, cErrB);
+        CK(cudaGraphLaunch(ContactGraphFor(c), s));
+        LaunchContactAddLoads(ContactView(), s);
+        CK(cudaMemcpyAsync(&hm->contact, cState.p, sizeof(ContactState), cudaMemcpyDeviceToHost, s));
+        contactRan = true;
+        lastContactB = nc;
+        launches += 16;
+    }
+    void ContactReport(tsp_contact_report& o) {
+        Sync();
+        o = tsp_contact_report{};
+        o.solverIters = hm->contact.iters;
+        o.avgDensityError = hm->contact.avgErr;
+        o.converged = contactRan ? hm->contact.converged : 1u;
+        o.nContacts = hm->contact.nContacts;
+        o.nContactBoundary = lastContactB;
+    }
+
     // -------------------------------------------------------------------------- step
     void Step(const tsp_params& p) {  // Step_IISPH (sph_solver.cpp:34-319) without the contact solve
         CK(cudaSetDevice(device));
@@ -784,6 +926,7 @@ public:
         LaunchIntegration(c, f, s);
         kgValid = false;
         if (nRB) {
+            SolveRigidContacts(c, rp, bd);
             LaunchRigidPredict(bd, prm.timeStep, s);
             LaunchRigidIntegrate(bd, prm.timeStep, err.p, s);
             LaunchRigidUpdateParticles(rp, bd, false, err.p, s);
@@ -1363,6 +1506,12 @@ int tsp_b200_get_stream(const tsp_backend* h, void** stream) {
     if (!stream) return TSP_ERR_INVALID;
     *stream = (void*)h->b->s;
     return TSP_OK;
+}
+int tsp_b200_get_contact_report(const tsp_backend* h, tsp_contact_report* out) {
+    TSP_NEED(h);
+    if (!out) return TSP_ERR_INVALID;
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, hh->b->ContactReport(*out));
 }
 int tsp_b200_get_phase_times(const tsp_backend* h, float* ms, uint32_t cap, uint32_t* n) {
     TSP_NEED(h);

@@ -23,6 +23,9 @@ constexpr uint32_t ERR_COUNT_U16 = 1u << 3;        // a neighbor count above uin
 constexpr uint32_t ERR_QUERY_CAP = 1u << 4;        // query stencil larger than the shared staging
 constexpr uint32_t ERR_RIGID_ORIENT = 1u << 5;     // degenerate rigid orientation (cpu_backend.cpp:46-58)
 constexpr uint32_t ERR_RIGID_ATTACH = 1u << 6;     // rigid particle attached to a missing body
+constexpr uint32_t ERR_CONTACT_BODIES = 1u << 7;   // a contact element touches too many bodies
+constexpr uint32_t ERR_CONTACT_INVALID = 1u << 8;  // invalid contact diagonal / non-finite error or pressure
+                                                   // (rigid_solver.cpp:332-336, 567, 595)
 
 // cell frame of the compact cell-linked list (source/simulation/core/cell_frame.h:18-26)
 struct Frame {

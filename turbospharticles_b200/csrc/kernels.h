@@ -234,6 +234,54 @@ struct RigidParticlesDev {
 };
 void LaunchRigidUpdateParticles(const RigidParticlesDev& r, const BodyDev& b, bool predicted, uint32_t* err,
                                 cudaStream_t s);
+
+// ---- contact_kernels.cu: rigid contact solver (rigid_solver.cpp:90-799)
+struct ContactState {
+    double errSum;
+    unsigned long long nContacts;  // N_contacts of RigidContactRelaxation
+    uint32_t iters, maxIters, converged, doUpdate;
+    float avgErr, target;
+};
+struct ContactDev {
+    uint32_t nR, nRB;
+    const uint32_t* nContactB;     // device count of contact boundary particles
+    const uint64_t *offRR, *offRB;
+    const uint32_t *listRR, *listRB;  // RR rows (rigid indices), RB rows (boundary indices)
+    uint32_t* idxRB;               // RB rows as contact indices
+    uint32_t* contactOfB;          // [nB] boundary -> contact index
+    uint32_t* localB;              // contact -> boundary index
+    uint64_t* offBR;
+    uint32_t *idxBR, *curBR;
+    const float4* posR;            // world x, y, z, psi
+    const float4* relR;            // body-frame x, y, z, vol
+    const uint32_t* bodyR;
+    const uint32_t *byBodyOff, *byBodyIdx;
+    const float4* posB;
+    const float* volB;
+    const double* bodyState;
+    double* bodyFT;
+    float4* relW;                  // world lever arms
+    float* iw;                     // world inverse inertia, 9 per body
+    float *densR, *diagR, *presR, *srcR, *errR, *omegaR;
+    float4 *forceC, *velC;
+    float *densB, *diagB, *presB, *srcB, *errB, *omegaB;
+    double* ftC;                   // contact force / torque, 6 per body
+    uint32_t* perBody;
+    double* contrib;               // per-element error-sum contributions
+    ContactState* st;
+    uint32_t* err;
+};
+void LaunchContactSetup(const ContactDev& d, uint64_t nEntriesRB, uint32_t nB, uint64_t* scanScratch,
+                        uint64_t* ncTotal, cudaStream_t s);
+void LaunchContactLists(const ContactDev& d, uint64_t nEntriesRB, uint32_t nc, uint64_t* scanScratch,
+                        uint64_t* totalScratch, cudaStream_t s);
+void LaunchContactPrepare(const ContactDev& d, const Consts& c, uint32_t nc, float target, uint32_t maxIters,
+                          cudaStream_t s);
+void LaunchContactInitialError(const ContactDev& d, const Consts& c, uint32_t nc, const float4* velPredR,
+                               cudaStream_t s);
+void LaunchContactIteration(const ContactDev& d, const Consts& c, uint32_t ncCap, unsigned long long cond,
+                            cudaStream_t s);
+void LaunchContactAddLoads(const ContactDev& d, cudaStream_t s);
 void LaunchRigidClearAddGravity(const BodyDev& b, float gx, float gy, float gz, cudaStream_t s);
 void LaunchRigidViscousForces(const Consts& c, const RigidParticlesDev& r, const FluidDev& f, const uint64_t* offRF,
                               const uint32_t* listRF, cudaStream_t s);

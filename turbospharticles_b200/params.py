@@ -40,6 +40,8 @@ class SimParams:
     gridCellSizeRatio: float = 1.0
     boundaryLayers: int = 2
     cubicSplineAlphaOverride: float = 0.0
+    rigidContactDensityDevTarget: float = 0.001   # parameters_sim.h:100
+    rigidContactMaxSolverIters: int = 100         # parameters_sim.h:101
     # scene-building parameters (builder.cpp; not read by the step)
     jitterFracF: float = 0.0
     jitterSeedF: int = 42
@@ -68,7 +70,8 @@ class SimParams:
                   "restDensity", "massF", "massB", "viscosityF", "viscosityB", "pressGamma",
                   "jacobiOmega", "jacobiWarmStart", "densityDevTarget", "fixedIters",
                   "minSolverIters", "maxSolverIters", "solverTerminationCond",
-                  "gridCellSizeRatio", "boundaryLayers", "cubicSplineAlphaOverride"):
+                  "gridCellSizeRatio", "boundaryLayers", "cubicSplineAlphaOverride",
+                  "rigidContactDensityDevTarget", "rigidContactMaxSolverIters"):
             setattr(p, f, getattr(self, f))
         for a in range(3):
             p.gravity[a] = self.gravity[a]

@@ -443,3 +443,30 @@ def served_stream(n_scenes=256, n_min=4096, n_max=262144, dx=0.01, dt=5e-4, rate
         t += rng.exponential(1.0 / rate_hz) if rate_hz > 0 else 0.0
         specs.append(ServedSceneSpec(k, nx, ny, nz, dx, dt, t, seed * 1000 + k))
     return specs
+
+
+def stacked_cubes(dx=0.02, dt=1e-3, edge=0.16, seed=9, tilt_deg=6.0, overlap=0.008, drop_speed=0.5):
+    """Rigid-contact scene: a hollow cube pressed `overlap` into the tank floor and a second,
+    slightly tilted one pressed into it and moving down at `drop_speed` (2 particle layers each,
+    densities 1000 and 700 kg/m^3), in a 0.6 m tank with a small fluid block in a far corner.
+    The contact density exceeds 1 from the first step, so the rigid contact solver
+    (rigid_solver.cpp:602) iterates every step."""
+    from .params import dam_params
+    p = dam_params(dx, dt)
+    p.jitterFracF = 0.01
+    p.jitterSeedF = seed
+    container = OBB((0.0, 0.0, 0.0), (0.6, 0.6, 0.6))
+    fluid = OBB((0.0, 0.0, 0.0), (6.5 * dx, 4.5 * dx, 6.5 * dx))
+    half = 0.5 * edge
+    t = math.radians(tilt_deg)
+    R = np.array([[math.cos(t), -math.sin(t), 0.0], [math.sin(t), math.cos(t), 0.0], [0.0, 0.0, 1.0]])
+    rigid = []
+    for c, Rm, dens in ((np.array([0.36, half - overlap, 0.36]), np.eye(3), 1000.0),
+                        (np.array([0.37, edge + half - 2.0 * overlap, 0.36]), R, 700.0)):
+        origin = tuple(float(x) for x in c - Rm @ np.full(3, half))
+        axes = (tuple(float(x) for x in Rm[:, j]) for j in range(3))
+        rigid.append((OBB(origin, (edge, edge, edge), *axes), dens))
+    st, dmin, dmax = breaking_dam(container, fluid, p, rigid)
+    st.yVelRB[1] = -float(drop_speed)
+    st.yAngMomRB[:] = 0.0
+    return st, dmin, dmax, p
