@@ -262,6 +262,50 @@ int tsp_b200_get_stream(const tsp_backend* h, void** stream);
  * read-back. *n = number written (0 before the first step). Analogue of the reference's
  * per-stage BenchOp timers (source/simulation/core/backend_sim.h:255, GetBenchOps). */
 int tsp_b200_get_phase_times(const tsp_backend* h, float* ms, uint32_t cap, uint32_t* n);
+/* Stats::StatMetric (source/eval/stats/metrics.h:23-86): index of each value in the record
+ * tsp_b200_fill_statistics writes (same order and meaning as the reference's enum) */
+#define TSP_STAT_NUM_F                       0
+#define TSP_STAT_NUM_B                       1
+#define TSP_STAT_NUM_R                       2
+#define TSP_STAT_NUM_NBR_FF_AVG             3
+#define TSP_STAT_NUM_NBR_FF_MIN             4
+#define TSP_STAT_NUM_NBR_FF_MAX             5
+#define TSP_STAT_NUM_NBR_FF_P99             6
+#define TSP_STAT_NUM_NBR_FB_AVG             7
+#define TSP_STAT_NUM_NBR_FB_MIN             8
+#define TSP_STAT_NUM_NBR_FB_MAX             9
+#define TSP_STAT_NUM_NBR_FB_P99             10
+#define TSP_STAT_NUM_NBR_FR_AVG             11
+#define TSP_STAT_NUM_NBR_FR_MIN             12
+#define TSP_STAT_NUM_NBR_FR_MAX             13
+#define TSP_STAT_NUM_NBR_FR_P99             14
+#define TSP_STAT_NUM_NBR_RF_AVG             15
+#define TSP_STAT_NUM_NBR_RF_MIN             16
+#define TSP_STAT_NUM_NBR_RF_MAX             17
+#define TSP_STAT_NUM_NBR_RF_P99             18
+#define TSP_STAT_NUM_NBR_RB_AVG             19
+#define TSP_STAT_NUM_NBR_RB_MIN             20
+#define TSP_STAT_NUM_NBR_RB_MAX             21
+#define TSP_STAT_NUM_NBR_RB_P99             22
+#define TSP_STAT_NUM_NBR_RR_AVG             23
+#define TSP_STAT_NUM_NBR_RR_MIN             24
+#define TSP_STAT_NUM_NBR_RR_MAX             25
+#define TSP_STAT_NUM_NBR_RR_P99             26
+#define TSP_STAT_DENS_REL_ERROR_RAW_AVG      27
+#define TSP_STAT_DENS_REL_ERROR_POS_AVG      28
+#define TSP_STAT_DENS_REL_ERROR_ABS_AVG      29
+#define TSP_STAT_NUM_SOLVER_ITERS            30
+#define TSP_STAT_CFL_NUMBER                  31
+#define TSP_STAT_VEL_MAG_AVG                 32
+#define TSP_STAT_VEL_MAG_MIN                 33
+#define TSP_STAT_VEL_MAG_MAX                 34
+#define TSP_STAT_COUNT                       35
+/* I_SimBackend::FillStatisticsRecord (backend_sim.h:243; GPU backend gpu_backend.cpp:1067-1203)
+ * of the last step or neighbor search: particle counts, neighbor-count average / min / max /
+ * 99th percentile per relation, average relative density errors, solver iterations, CFL
+ * number and velocity magnitude average / min / max. `record` receives min(n, TSP_STAT_COUNT)
+ * doubles. */
+int tsp_b200_fill_statistics(const tsp_backend* h, const tsp_params* params, double* record, uint32_t n);
 /* SimBackend_CPU::GetRigidContactReport (cpu_backend.h:132) */
 int tsp_b200_get_contact_report(const tsp_backend* h, tsp_contact_report* out);
 /* number of CUDA kernels this backend launched since creation (graph nodes included) */

@@ -44,6 +44,7 @@ def lib():
             "orc_step": (C.c_int, [vp, C.POINTER(TspParams), C.c_uint32]),
             "orc_get_stats": (C.c_int, [vp, C.POINTER(TspStepStats)]),
             "orc_get_contact_report": (C.c_int, [vp, C.POINTER(TspContactReport)]),
+            "orc_fill_statistics": (C.c_int, [vp, C.POINTER(TspParams), C.POINTER(C.c_double)]),
             "orc_read_cell_ids": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32]),
             "orc_read_permutation": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32]),
             "orc_read_cell_table": (C.c_int, [vp, C.c_uint32, vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]),
@@ -123,6 +124,14 @@ class OracleBackend:
         s = TspStepStats()
         self._chk(self.L.orc_get_stats(self.h, C.byref(s)))
         return s
+
+    def statistics(self, params=None) -> dict:
+        """FillStatisticsRecord of the last step (names of Stats::StatMetric)."""
+        from turbospharticles_b200.abi import STAT_NAMES
+        buf = (C.c_double * len(STAT_NAMES))()
+        cp = (params or self.params).to_c()
+        self._chk(self.L.orc_fill_statistics(self.h, C.byref(cp), buf))
+        return dict(zip(STAT_NAMES, list(buf)))
 
     def contact_report(self) -> TspContactReport:
         r = TspContactReport()

@@ -1428,6 +1428,45 @@ template <typename T> static void Push(Oracle<T>& O, tsp_state_view& s) {
     Store(O.mass, s.massRB, O.NRB); Store(O.massInv, s.massInvRB, O.NRB);
 }
 
+namespace orc {
+// FillStatisticsRecord (gpu_backend.cpp:1067-1203): same record layout as tsp_b200_fill_statistics
+template <typename T> static void FillStats(const Oracle<T>& O, const tsp_params& p, double* r) {
+    std::memset(r, 0, sizeof(double) * TSP_STAT_COUNT);
+    r[TSP_STAT_NUM_F] = O.NF; r[TSP_STAT_NUM_B] = O.NB; r[TSP_STAT_NUM_R] = O.NR;
+    for (int k = 0; k < 6; k++) {
+        const CSR& c = O.rows[k];
+        const uint32_t n = k < 3 ? O.NF : O.NR;
+        if (n == 0 || c.off.size() != (size_t)n + 1) continue;
+        std::vector<uint32_t> cnt(n);
+        for (uint32_t i = 0; i < n; i++) cnt[i] = (uint32_t)(c.off[i + 1] - c.off[i]);
+        std::vector<uint32_t> srt = cnt;
+        std::sort(srt.begin(), srt.end());
+        r[TSP_STAT_NUM_NBR_FF_AVG + 4 * k] = (double)c.total() / (double)n;
+        r[TSP_STAT_NUM_NBR_FF_MIN + 4 * k] = srt.front();
+        r[TSP_STAT_NUM_NBR_FF_MAX + 4 * k] = srt.back();
+        r[TSP_STAT_NUM_NBR_FF_P99 + 4 * k] = srt[(99ull * (uint64_t)(n - 1)) / 100ull];
+    }
+    double raw = 0, pos = 0, ab = 0, vs = 0;
+    float vmin = 3.402823466e38f, vmax = 0.0f;
+    for (uint32_t i = 0; i < O.NF; i++) {
+        const float rel = ((float)O.densF[i] / p.restDensity) - 1.0f;
+        raw += rel; pos += std::max(0.0f, rel); ab += std::fabs(rel);
+        const float vx = (float)O.vxF[i], vy = (float)O.vyF[i], vz = (float)O.vzF[i];
+        const float mag = std::sqrt(vx * vx + vy * vy + vz * vz);
+        vs += mag; vmin = std::min(vmin, mag); vmax = std::max(vmax, mag);
+    }
+    const double inv = O.NF ? 1.0 / (double)O.NF : 0.0;
+    r[TSP_STAT_DENS_REL_ERROR_RAW_AVG] = raw * inv;
+    r[TSP_STAT_DENS_REL_ERROR_POS_AVG] = pos * inv;
+    r[TSP_STAT_DENS_REL_ERROR_ABS_AVG] = ab * inv;
+    r[TSP_STAT_NUM_SOLVER_ITERS] = O.iters;
+    r[TSP_STAT_CFL_NUMBER] = (O.NF ? vmax : 0.0f) * p.timeStep / p.particleSizeF;
+    r[TSP_STAT_VEL_MAG_AVG] = vs * inv;
+    r[TSP_STAT_VEL_MAG_MIN] = O.NF ? vmin : 0.0f;
+    r[TSP_STAT_VEL_MAG_MAX] = O.NF ? vmax : 0.0f;
+}
+}  // namespace orc
+
 extern "C" {
 
 orc_handle* orc_create(const tsp_params* p, int fp64) {
@@ -1463,6 +1502,9 @@ int orc_step(orc_handle* h, const tsp_params* p, uint32_t n) {
         O.prm = *p;
         for (uint32_t s = 0; s < n; s++) { O.Step(); O.step += 1; O.time += (double)p->timeStep; }
     }))
+}
+int orc_fill_statistics(orc_handle* h, const tsp_params* p, double* r) {
+    ORC_TRY(h, ORC_DISPATCH(h, orc::FillStats(O, *p, r)))
 }
 int orc_get_contact_report(orc_handle* h, tsp_contact_report* r) {
     ORC_TRY(h, ORC_DISPATCH(h, {

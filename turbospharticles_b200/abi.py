@@ -22,6 +22,8 @@ TERM_FIXED_ITERS, TERM_REL_ERR_RAW, TERM_REL_ERR_POS, TERM_REL_ERR_ABS = 0, 1, 2
 SPECIES_F, SPECIES_B, SPECIES_R = 0, 1, 2
 LIST_FF, LIST_FB, LIST_FR, LIST_RF, LIST_RB, LIST_RR = range(6)
 NOALLOC_MAX_PARTICLES = 1 << 24  # TSP_NOALLOC_MAX_PARTICLES
+# Stats::StatMetric (source/eval/stats/metrics.h:23-86), the record of tsp_b200_fill_statistics
+STAT_NAMES = ("NumF", "NumB", "NumR", "NumNbrFF_Avg", "NumNbrFF_Min", "NumNbrFF_Max", "NumNbrFF_P99", "NumNbrFB_Avg", "NumNbrFB_Min", "NumNbrFB_Max", "NumNbrFB_P99", "NumNbrFR_Avg", "NumNbrFR_Min", "NumNbrFR_Max", "NumNbrFR_P99", "NumNbrRF_Avg", "NumNbrRF_Min", "NumNbrRF_Max", "NumNbrRF_P99", "NumNbrRB_Avg", "NumNbrRB_Min", "NumNbrRB_Max", "NumNbrRB_P99", "NumNbrRR_Avg", "NumNbrRR_Min", "NumNbrRR_Max", "NumNbrRR_P99", "DensRelError_Raw_Avg", "DensRelError_Pos_Avg", "DensRelError_Abs_Avg", "NumSolverIters", "CFL_Number", "VelMag_Avg", "VelMag_Min", "VelMag_Max")
 PHASE_NAMES = ("frame", "sort_reorder_tables", "query_count", "finalize_readback", "query_fill", "density",
                "non_pressure", "source_diag_init", "jacobi_loop", "pressure_acc_final", "integration",
                "stats_readback")
@@ -139,6 +141,7 @@ EXPORTS = {
     "tsp_b200_time_stage": (C.c_int, [_VP, C.POINTER(TspParams), _u32, _u32, _pf]),
     "tsp_b200_get_launch_count": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
     "tsp_b200_get_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
+    "tsp_b200_fill_statistics": (C.c_int, [_VP, C.POINTER(TspParams), C.POINTER(C.c_double), C.c_uint32]),
     "tsp_b200_get_contact_report": (C.c_int, [_VP, C.POINTER(TspContactReport)]),
     "tsp_b200_get_phase_times": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32)]),
     "tsp_b200_try_build_cell_frame": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),

@@ -183,6 +183,15 @@ class SimBackendB200:
         self._chk(self.L.tsp_b200_time_stage(self.h, self._cparams(params), stage, reps, C.byref(ms)))
         return ms.value
 
+    def FillStatisticsRecord(self, params: SimParams | None = None) -> dict:
+        """Statistics of the last step (I_SimBackend::FillStatisticsRecord, backend_sim.h:243),
+        keyed by the reference's Stats::StatMetric names."""
+        buf = (C.c_double * len(abi.STAT_NAMES))()
+        self._chk(self.L.tsp_b200_fill_statistics(self.h, self._cparams(params), buf, len(abi.STAT_NAMES)))
+        return dict(zip(abi.STAT_NAMES, list(buf)))
+
+    statistics = FillStatisticsRecord
+
     def contact_report(self):
         """Rigid contact solve of the last step (GetRigidContactReport, cpu_backend.h:132)."""
         r = abi.TspContactReport()

@@ -866,6 +866,52 @@ public:
         lastContactB = nc;
         launches += 16;
     }
+    // FillStatisticsRecord (gpu_backend.cpp:1067-1203) of the last step / neighbor search
+    DBuf<uint32_t> statHist, statOut;
+    DBuf<double> statPart, statF;
+    DBuf<float> statMM;
+    void Statistics(const tsp_params& p, double* rec, uint32_t n) {
+        CK(cudaSetDevice(device));
+        double r[TSP_STAT_COUNT] = {};
+        r[TSP_STAT_NUM_F] = nF; r[TSP_STAT_NUM_B] = nB; r[TSP_STAT_NUM_R] = nR;
+        statHist.ensure(65536); statOut.ensure(18); statF.ensure(6);
+        const uint32_t blocks = StatFieldBlocks(nF);
+        statPart.ensure(4ull * blocks); statMM.ensure(2ull * blocks);
+        uint32_t cnt[18] = {};
+        double fld[6] = {};
+        if (listsValid) {
+            const uint16_t* counts[6] = {sell[0].counts.p, sell[1].counts.p, sell[2].counts.p,
+                                         cntR[0].p, cntR[1].p, cntR[2].p};
+            const uint32_t srcN[6] = {nF, nF, nF, nR, nR, nR};
+            for (int k = 0; k < 6; k++)
+                LaunchStatNeighborCounts(srcN[k] ? counts[k] : nullptr, srcN[k], statHist.p, statOut.p + 3 * k, s);
+            CK(cudaMemcpyAsync(cnt, statOut.p, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+        }
+        if (nF) {
+            LaunchStatFields(velRho.p, nF, p.restDensity, statPart.p, statMM.p, statF.p, s);
+            CK(cudaMemcpyAsync(fld, statF.p, sizeof(fld), cudaMemcpyDeviceToHost, s));
+        }
+        Sync();
+        const double invNF = nF ? 1.0 / (double)nF : 0.0, invNR = nR ? 1.0 / (double)nR : 0.0;
+        const uint64_t tot[6] = {nNbr[0], nNbr[1], nNbr[2], csrN[0], csrN[1], csrN[2]};
+        for (int k = 0; k < 6 && listsValid; k++) {
+            const double inv = k < 3 ? invNF : invNR;
+            r[TSP_STAT_NUM_NBR_FF_AVG + 4 * k] = (double)tot[k] * inv;
+            r[TSP_STAT_NUM_NBR_FF_MIN + 4 * k] = cnt[3 * k];
+            r[TSP_STAT_NUM_NBR_FF_MAX + 4 * k] = cnt[3 * k + 1];
+            r[TSP_STAT_NUM_NBR_FF_P99 + 4 * k] = cnt[3 * k + 2];
+        }
+        r[TSP_STAT_DENS_REL_ERROR_RAW_AVG] = fld[0] * invNF;
+        r[TSP_STAT_DENS_REL_ERROR_POS_AVG] = fld[1] * invNF;
+        r[TSP_STAT_DENS_REL_ERROR_ABS_AVG] = fld[2] * invNF;
+        r[TSP_STAT_NUM_SOLVER_ITERS] = hm->st.iters;
+        const float vmax = nF ? (float)fld[5] : 0.0f;
+        r[TSP_STAT_CFL_NUMBER] = vmax * p.timeStep / p.particleSizeF;
+        r[TSP_STAT_VEL_MAG_AVG] = fld[3] * invNF;
+        r[TSP_STAT_VEL_MAG_MIN] = nF ? fld[4] : 0.0;
+        r[TSP_STAT_VEL_MAG_MAX] = vmax;
+        for (uint32_t k = 0; k < n && k < (uint32_t)TSP_STAT_COUNT; k++) rec[k] = r[k];
+    }
     void ContactReport(tsp_contact_report& o) {
         Sync();
         o = tsp_contact_report{};
@@ -1506,6 +1552,12 @@ int tsp_b200_get_stream(const tsp_backend* h, void** stream) {
     if (!stream) return TSP_ERR_INVALID;
     *stream = (void*)h->b->s;
     return TSP_OK;
+}
+int tsp_b200_fill_statistics(const tsp_backend* h, const tsp_params* p, double* record, uint32_t n) {
+    TSP_NEED(h);
+    if (!p || (n && !record)) return TSP_ERR_INVALID;
+    tsp_backend* hh = const_cast<tsp_backend*>(h);
+    TSP_GUARD(hh, hh->b->Statistics(*p, record, n));
 }
 int tsp_b200_get_contact_report(const tsp_backend* h, tsp_contact_report* out) {
     TSP_NEED(h);

@@ -235,6 +235,12 @@ struct RigidParticlesDev {
 void LaunchRigidUpdateParticles(const RigidParticlesDev& r, const BodyDev& b, bool predicted, uint32_t* err,
                                 cudaStream_t s);
 
+// ---- stats_kernels.cu: statistics record (gpu_backend.cpp:1067-1203)
+uint32_t StatFieldBlocks(uint32_t n);
+void LaunchStatNeighborCounts(const uint16_t* counts, uint32_t n, uint32_t* hist, uint32_t* out, cudaStream_t s);
+void LaunchStatFields(const float4* velRho, uint32_t n, float rho0, double* partials, float* mm, double* out,
+                      cudaStream_t s);
+
 // ---- contact_kernels.cu: rigid contact solver (rigid_solver.cpp:90-799)
 struct ContactState {
     double errSum;
