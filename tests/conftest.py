@@ -10,5 +10,9 @@ for p in (ROOT, os.path.join(ROOT, "oracle"), os.path.dirname(os.path.abspath(__
 
 
 def pytest_configure(config):
+    # temporary files of the tests (state files, built adapters) stay inside the checkout
+    if not config.option.basetemp:
+        os.makedirs(os.path.join(ROOT, "_build"), exist_ok=True)
+        config.option.basetemp = os.path.join(ROOT, "_build", "pytest_tmp")
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: full-size parity cases")

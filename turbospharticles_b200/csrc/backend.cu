@@ -659,12 +659,12 @@ public:
             nNbr[k] = nF ? hm->nbrTot[k] : 0;
             sell[k].n16 = hm->sellTot[k].a;
             sell[k].n32 = hm->sellTot[k].b;
-            sell[k].l16.grow(sell[k].n16, 1.04);
-            sell[k].l32.grow(sell[k].n32, 1.04);
+            sell[k].l16.grow(sell[k].n16, LIST_GROWTH);
+            sell[k].l32.grow(sell[k].n32, LIST_GROWTH);
             sell[k].kg16.ensure(sell[k].l16.cap);
             sell[k].kg32.ensure(sell[k].l32.cap);
             csrN[k] = hm->csrTot[k];
-            listR[k].grow(csrN[k], 1.04);
+            listR[k].grow(csrN[k], LIST_GROWTH);
         }
         m0 = Meta(0); m1 = Meta(1); m2 = Meta(2);
         rl = RLists();

@@ -964,7 +964,7 @@ public:
         Sync();
         for (int k = 0; k < 3; k++) {
             sell[k].n16 = tot[k].a; sell[k].n32 = tot[k].b;
-            sell[k].l16.grow(tot[k].a, 1.1); sell[k].l32.grow(tot[k].b, 1.1);
+            sell[k].l16.grow(tot[k].a, LIST_GROWTH); sell[k].l32.grow(tot[k].b, LIST_GROWTH);
             sell[k].kg16.ensure(sell[k].l16.cap); sell[k].kg32.ensure(sell[k].l32.cap);
         }
         LaunchQueryFluid(true, qa, Meta(0), Meta(1), Meta(2), s);

@@ -53,6 +53,12 @@ template <typename T> inline void Swap(DBuf<T>& a, DBuf<T>& b) { std::swap(a.p, 
 
 inline unsigned G(uint32_t n) { return (n + 255) / 256; }
 
+// Growth factor of the neighbor-list buffers. A list outgrowing its buffer costs a free and an
+// allocation (both synchronise the device) plus a new capture of the Jacobi graph, whose nodes
+// hold the buffer addresses; a flow that compresses or spreads grows its lists by a few percent
+// per hundred steps, so the buffers grow in large steps and never shrink.
+constexpr double LIST_GROWTH = 1.25;
+
 // ------------------------------------------------------------------------------ helpers
 inline int HostFloorToInt(float v) {
     const int i = (int)v;
