@@ -76,7 +76,10 @@ typedef struct tsp_params {
      * both 0 selects the reference defaults 0.001 and 100 */
     float rigidContactDensityDevTarget;
     uint32_t rigidContactMaxSolverIters;
-    uint32_t reserved[2];
+    /* export surface classification (parameters_sim.h:167-170): fewer fluid neighbors than this
+     * marks a fluid particle near-surface; 0 selects the reference default 27 */
+    uint32_t surfaceNbrCountThreshold;
+    uint32_t reserved[1];
 } tsp_params;
 
 /*
@@ -310,6 +313,33 @@ int tsp_b200_fill_statistics(const tsp_backend* h, const tsp_params* params, dou
 int tsp_b200_get_contact_report(const tsp_backend* h, tsp_contact_report* out);
 /* number of CUDA kernels this backend launched since creation (graph nodes included) */
 int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count);
+
+/*
+ * Host view of Sync::ExportSnapshot (source/simulation/sync/snapshots.h:37-66): the particles
+ * an export writes. Fluid: only the surface particles (near-surface particles and their fluid
+ * neighbors), positions and velocity magnitudes, in the backend's particle order; boundary:
+ * positions, volumes and mesh flags; rigid: world positions, volumes, body indices. Each
+ * non-NULL array must hold the backend's full count of its population (tsp_b200_get_counts);
+ * NULL arrays are skipped. The N_* fields receive the exported counts.
+ */
+typedef struct tsp_export_snapshot {
+    uint64_t simStep;
+    double simTime;
+    uint32_t N_F, N_B, N_R, reserved;
+    float *xPosF, *yPosF, *zPosF, *velMagF;
+    float *xPosB, *yPosB, *zPosB, *volB;
+    uint8_t* isMeshB;
+    uint32_t* bodyIdR;
+    float *xPosR, *yPosR, *zPosR, *volR;
+} tsp_export_snapshot;
+#define TSP_NO_MESH_ID UINT64_MAX
+/* I_SimBackend::PackExportSnapshot (backend_sim.h:215; GPU backend gpu_backend.cpp:346-540):
+ * classification and compaction run on the device, so only the exported particles are copied
+ * to the host. `include_b` = 0 exports no boundary particles; boundary particles with an ID
+ * >= `mesh_id_begin_b` are mesh particles (TSP_NO_MESH_ID: none). Before the first neighbor
+ * search no neighbor counts exist and no fluid particle is exported (as SimBackend_CPU). */
+int tsp_b200_pack_export_snapshot(tsp_backend* h, const tsp_params* params, int include_b,
+                                  uint64_t mesh_id_begin_b, tsp_export_snapshot* snap);
 
 /* ---- served batch ------------------------------------------------------------------------
  * No counterpart in the reference (its SimulationMgr runs one scene per backend). A batch keeps

@@ -59,6 +59,12 @@ public:
         Check(tsp_b200_get_contact_report(h_, &r));
         return r;
     }
+    // I_SimBackend::PackExportSnapshot (backend_sim.h:215); the snapshot's non-NULL arrays must
+    // hold the backend's full population counts, its N_* fields receive the exported counts
+    void PackExportSnapshot(tsp_export_snapshot& snap, const tsp_params& params, bool includeB,
+                            uint64_t meshIdBeginB = TSP_NO_MESH_ID) {
+        Check(tsp_b200_pack_export_snapshot(h_, &params, includeB ? 1 : 0, meshIdBeginB, &snap));
+    }
     tsp_backend* Handle() const { return h_; }
 
 private:

@@ -12,9 +12,9 @@ import subprocess
 
 import numpy as np
 
-from turbospharticles_b200.abi import (TspParams, TspStateView, TspStepStats, TspContactReport, FIELD_COMPONENTS,
-                                       FIELD_BODY_FT)
-from turbospharticles_b200.state import UniversalSimState
+from turbospharticles_b200.abi import (TspParams, TspStateView, TspStepStats, TspContactReport, TspExportSnapshot,
+                                       FIELD_COMPONENTS, FIELD_BODY_FT)
+from turbospharticles_b200.state import ExportSnapshot, UniversalSimState
 
 ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(ORACLE_DIR, "_build", "libtsp_oracle.so")
@@ -45,6 +45,8 @@ def lib():
             "orc_get_stats": (C.c_int, [vp, C.POINTER(TspStepStats)]),
             "orc_get_contact_report": (C.c_int, [vp, C.POINTER(TspContactReport)]),
             "orc_fill_statistics": (C.c_int, [vp, C.POINTER(TspParams), C.POINTER(C.c_double)]),
+            "orc_pack_export_snapshot": (C.c_int, [vp, C.POINTER(TspParams), C.c_int, C.c_uint64,
+                                                   C.POINTER(TspExportSnapshot)]),
             "orc_read_cell_ids": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32]),
             "orc_read_permutation": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32]),
             "orc_read_cell_table": (C.c_int, [vp, C.c_uint32, vp, vp, C.c_uint32, C.POINTER(C.c_uint32)]),
@@ -132,6 +134,13 @@ class OracleBackend:
         cp = (params or self.params).to_c()
         self._chk(self.L.orc_fill_statistics(self.h, C.byref(cp), buf))
         return dict(zip(STAT_NAMES, list(buf)))
+
+    def pack_export_snapshot(self, params=None, include_b=True, mesh_id_begin_b=None) -> ExportSnapshot:
+        """PackExportSnapshot (cpu_backend.cpp:829-975)."""
+        cp = (params or self.params).to_c()
+        return ExportSnapshot.pack(lambda *a: self._chk(self.L.orc_pack_export_snapshot(self.h, *a)),
+                                   (self.counts[0], self.counts[1], self.counts[2]), cp, include_b,
+                                   mesh_id_begin_b)
 
     def contact_report(self) -> TspContactReport:
         r = TspContactReport()

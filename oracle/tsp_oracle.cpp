@@ -1465,6 +1465,55 @@ template <typename T> static void FillStats(const Oracle<T>& O, const tsp_params
     r[TSP_STAT_VEL_MAG_MIN] = O.NF ? vmin : 0.0f;
     r[TSP_STAT_VEL_MAG_MAX] = O.NF ? vmax : 0.0f;
 }
+// PackExportSnapshot (cpu_backend.cpp:829-975): FillFluidParticleNearSurfaceFlags +
+// ClassifyExportSurfaceParticles + the ordered copy of the marked fluid particles
+template <typename T> static void PackExport(const Oracle<T>& O, const tsp_params& p, bool includeB,
+                                             uint64_t meshBegin, tsp_export_snapshot& o) {
+    o.simStep = O.step;
+    o.simTime = O.time;
+    o.N_B = includeB ? O.NB : 0u;
+    for (uint32_t i = 0; i < o.N_B; i++) {
+        if (o.xPosB) o.xPosB[i] = (float)O.xB[i];
+        if (o.yPosB) o.yPosB[i] = (float)O.yB[i];
+        if (o.zPosB) o.zPosB[i] = (float)O.zB[i];
+        if (o.volB) o.volB[i] = (float)O.volB[i];
+        if (o.isMeshB) o.isMeshB[i] = (uint8_t)(O.idB[i] >= meshBegin);
+    }
+    o.N_R = O.NR;
+    for (uint32_t i = 0; i < O.NR; i++) {
+        if (o.bodyIdR) o.bodyIdR[i] = O.bodyR[i];
+        if (o.xPosR) o.xPosR[i] = (float)O.xR[i];
+        if (o.yPosR) o.yPosR[i] = (float)O.yR[i];
+        if (o.zPosR) o.zPosR[i] = (float)O.zR[i];
+        if (o.volR) o.volR[i] = (float)O.volR[i];
+    }
+    o.N_F = 0;
+    const CSR& ff = O.rows[0];
+    if (O.NF == 0 || ff.off.size() != (size_t)O.NF + 1) return;
+    const uint32_t threshold = p.surfaceNbrCountThreshold ? p.surfaceNbrCountThreshold : 27u;
+    auto count = [&](int k, uint32_t i) -> uint64_t {
+        const CSR& c = O.rows[k];
+        return c.off.size() == (size_t)O.NF + 1 ? c.off[i + 1] - c.off[i] : 0u;
+    };
+    std::vector<uint8_t> flag(O.NF, 0);
+    for (uint32_t i = 0; i < O.NF; i++) {
+        const uint64_t cFF = count(0, i), cFB = count(1, i), cFR = count(2, i);
+        if (!(cFB > 0 || cFR > 0 || cFF < threshold)) continue;  // IsNearSurfaceFluidParticle
+        flag[i] = 1;
+        for (uint64_t k = ff.off[i]; k < ff.off[i + 1]; k++) flag[ff.idx[k]] = 1;
+    }
+    uint32_t dst = 0;
+    for (uint32_t i = 0; i < O.NF; i++) {
+        if (!flag[i]) continue;
+        const float vx = (float)O.vxF[i], vy = (float)O.vyF[i], vz = (float)O.vzF[i];
+        if (o.xPosF) o.xPosF[dst] = (float)O.xF[i];
+        if (o.yPosF) o.yPosF[dst] = (float)O.yF[i];
+        if (o.zPosF) o.zPosF[dst] = (float)O.zF[i];
+        if (o.velMagF) o.velMagF[dst] = std::sqrt(vx * vx + vy * vy + vz * vz);
+        dst++;
+    }
+    o.N_F = dst;
+}
 }  // namespace orc
 
 extern "C" {
@@ -1505,6 +1554,10 @@ int orc_step(orc_handle* h, const tsp_params* p, uint32_t n) {
 }
 int orc_fill_statistics(orc_handle* h, const tsp_params* p, double* r) {
     ORC_TRY(h, ORC_DISPATCH(h, orc::FillStats(O, *p, r)))
+}
+int orc_pack_export_snapshot(orc_handle* h, const tsp_params* p, int includeB, uint64_t meshBegin,
+                             tsp_export_snapshot* o) {
+    ORC_TRY(h, ORC_DISPATCH(h, orc::PackExport(O, *p, includeB != 0, meshBegin, *o)))
 }
 int orc_get_contact_report(orc_handle* h, tsp_contact_report* r) {
     ORC_TRY(h, ORC_DISPATCH(h, {

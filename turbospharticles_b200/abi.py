@@ -54,7 +54,7 @@ class TspParams(C.Structure):
         ("fixedIters", _u32), ("minSolverIters", _u32), ("maxSolverIters", _u32),
         ("solverTerminationCond", _u32), ("gridCellSizeRatio", _f), ("boundaryLayers", _u32),
         ("cubicSplineAlphaOverride", _f), ("rigidContactDensityDevTarget", _f),
-        ("rigidContactMaxSolverIters", _u32), ("reserved", _u32 * 2),
+        ("rigidContactMaxSolverIters", _u32), ("surfaceNbrCountThreshold", _u32), ("reserved", _u32 * 1),
     ]
 
 
@@ -113,6 +113,17 @@ class TspContactReport(C.Structure):
                 ("nContacts", C.c_uint64), ("nContactBoundary", C.c_uint64)]
 
 
+class TspExportSnapshot(C.Structure):
+    """tsp_export_snapshot (Sync::ExportSnapshot, snapshots.h:37-66)."""
+    _fields_ = [("simStep", C.c_uint64), ("simTime", C.c_double), ("N_F", _u32), ("N_B", _u32), ("N_R", _u32),
+                ("reserved", _u32)] + [(n, _pf) for n in ("xPosF", "yPosF", "zPosF", "velMagF", "xPosB", "yPosB",
+                                                           "zPosB", "volB")] + \
+               [("isMeshB", C.POINTER(C.c_uint8)), ("bodyIdR", _pu32)] + \
+               [(n, _pf) for n in ("xPosR", "yPosR", "zPosR", "volR")]
+
+
+NO_MESH_ID = (1 << 64) - 1
+
 _VP = C.c_void_p
 EXPORTS = {
     "tsp_b200_create": (C.c_int, [C.POINTER(TspParams), C.c_int, C.POINTER(_VP)]),
@@ -143,6 +154,8 @@ EXPORTS = {
     "tsp_b200_get_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
     "tsp_b200_fill_statistics": (C.c_int, [_VP, C.POINTER(TspParams), C.POINTER(C.c_double), C.c_uint32]),
     "tsp_b200_get_contact_report": (C.c_int, [_VP, C.POINTER(TspContactReport)]),
+    "tsp_b200_pack_export_snapshot": (C.c_int, [_VP, C.POINTER(TspParams), C.c_int, C.c_uint64,
+                                                C.POINTER(TspExportSnapshot)]),
     "tsp_b200_get_phase_times": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32)]),
     "tsp_b200_try_build_cell_frame": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                                  C.POINTER(C.c_uint32)]),

@@ -16,7 +16,7 @@ import numpy as np
 from . import abi
 from .abi import TspError, TspStepStats, FIELD_COMPONENTS, FIELD_BODY_FT
 from .params import SimParams
-from .state import UniversalSimState
+from .state import ExportSnapshot, UniversalSimState
 
 
 def _p(a):
@@ -191,6 +191,17 @@ class SimBackendB200:
         return dict(zip(abi.STAT_NAMES, list(buf)))
 
     statistics = FillStatisticsRecord
+
+    def PackExportSnapshot(self, params: SimParams | None = None, include_b: bool = True,
+                           mesh_id_begin_b: int | None = None) -> ExportSnapshot:
+        """I_SimBackend::PackExportSnapshot (backend_sim.h:215): surface fluid particles,
+        boundary (when `include_b`) and rigid particles of the current state; boundary particles
+        with ID >= `mesh_id_begin_b` are flagged as mesh particles (None: no mesh)."""
+        cp = self.params.to_c() if params is None else params.to_c()
+        return ExportSnapshot.pack(lambda *a: self._chk(self.L.tsp_b200_pack_export_snapshot(self.h, *a)),
+                                   self.counts[:3], cp, include_b, mesh_id_begin_b)
+
+    pack_export_snapshot = PackExportSnapshot
 
     def contact_report(self):
         """Rigid contact solve of the last step (GetRigidContactReport, cpu_backend.h:132)."""

@@ -90,6 +90,7 @@ struct HostMirror {
     uint32_t err;
     ContactState contact;
     uint64_t contactTot[2];
+    uint32_t exportCount;
 };
 
 class Backend {
@@ -866,6 +867,57 @@ public:
         lastContactB = nc;
         launches += 16;
     }
+    // PackExportSnapshot (gpu_backend.cpp:346-540; classification as cpu_backend.cpp:829-975)
+    DBuf<uint8_t> expFlags, expMesh;
+    DBuf<uint32_t> expTiles, expCount;
+    void PackExport(const tsp_params& p, bool includeB, uint64_t meshBegin, tsp_export_snapshot& o) {
+        CK(cudaSetDevice(device));
+        o.simStep = stepCount;
+        o.simTime = simTime;
+        DBuf<float>& tmp = stage;
+        o.N_B = includeB ? nB : 0u;
+        if (o.N_B) {
+            Unpack4(posB.p, nB, o.xPosB, o.yPosB, o.zPosB, nullptr, tmp);
+            if (o.volB) CK(cudaMemcpyAsync(o.volB, volB.p, nB * 4ull, cudaMemcpyDeviceToHost, s));
+            if (o.isMeshB) {
+                expMesh.ensure(nB);
+                LaunchMeshFlags(idB.p, nB, meshBegin, expMesh.p, s);
+                CK(cudaMemcpyAsync(o.isMeshB, expMesh.p, nB, cudaMemcpyDeviceToHost, s));
+                launches += 1;
+            }
+            launches += 1;
+            Sync();
+        }
+        o.N_R = nR;
+        if (nR) {
+            if (o.bodyIdR) CK(cudaMemcpyAsync(o.bodyIdR, bodyR.p, nR * 4ull, cudaMemcpyDeviceToHost, s));
+            Unpack4(posR.p, nR, o.xPosR, o.yPosR, o.zPosR, nullptr, tmp);
+            Sync();
+            Unpack4(relR.p, nR, nullptr, nullptr, nullptr, o.volR, tmp);
+            launches += 2;
+            Sync();
+        }
+        o.N_F = 0;
+        if (nF == 0 || !listsValid) return;
+        const uint32_t threshold = p.surfaceNbrCountThreshold ? p.surfaceNbrCountThreshold : 27u;
+        expFlags.ensure(nF);
+        expTiles.ensure(ExportTiles(nF));
+        expCount.ensure(1);
+        tmp.ensure(4ull * nF);
+        const NeighborView nv = NView();
+        LaunchExportSurface(nv.ff, nv.fb.counts, nv.fr.counts, nF, threshold, posP.p, velRho.p, expFlags.p,
+                            expTiles.p, expCount.p, tmp.p, nF, s);
+        launches += 4;
+        CK(cudaMemcpyAsync(&hm->exportCount, expCount.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        Sync();
+        const uint32_t nS = hm->exportCount;
+        if (nS > nF) throw Error(TSP_ERR_INVALID, "export surface count exceeds the fluid count");
+        o.N_F = nS;
+        float* dst[4] = {o.xPosF, o.yPosF, o.zPosF, o.velMagF};
+        for (int k = 0; k < 4; k++)
+            if (dst[k] && nS) CK(cudaMemcpyAsync(dst[k], tmp.p + (uint64_t)k * nF, nS * 4ull, cudaMemcpyDeviceToHost, s));
+        Sync();
+    }
     // FillStatisticsRecord (gpu_backend.cpp:1067-1203) of the last step / neighbor search
     DBuf<uint32_t> statHist, statOut;
     DBuf<double> statPart, statF;
@@ -1564,6 +1616,12 @@ int tsp_b200_get_contact_report(const tsp_backend* h, tsp_contact_report* out) {
     if (!out) return TSP_ERR_INVALID;
     tsp_backend* hh = const_cast<tsp_backend*>(h);
     TSP_GUARD(hh, hh->b->ContactReport(*out));
+}
+int tsp_b200_pack_export_snapshot(tsp_backend* h, const tsp_params* params, int include_b,
+                                  uint64_t mesh_id_begin_b, tsp_export_snapshot* snap) {
+    TSP_NEED(h);
+    if (!params || !snap) return TSP_ERR_INVALID;
+    TSP_GUARD(h, h->b->PackExport(*params, include_b != 0, mesh_id_begin_b, *snap));
 }
 int tsp_b200_get_phase_times(const tsp_backend* h, float* ms, uint32_t cap, uint32_t* n) {
     TSP_NEED(h);

@@ -241,6 +241,16 @@ void LaunchStatNeighborCounts(const uint16_t* counts, uint32_t n, uint32_t* hist
 void LaunchStatFields(const float4* velRho, uint32_t n, float rho0, double* partials, float* mm, double* out,
                       cudaStream_t s);
 
+// ---- export_kernels.cu: export snapshot surface classification and compaction
+//      (PackExportSnapshot, gpu_backend.cpp:346-540)
+uint32_t ExportTiles(uint32_t n);
+// writes x, y, z, |v| of the exported particles to out[0 .. ), out[stride ..), out[2 stride ..),
+// out[3 stride ..) and their count to *nOut
+void LaunchExportSurface(const SellView& ff, const uint16_t* cntFB, const uint16_t* cntFR, uint32_t n,
+                         uint32_t threshold, const float4* posP, const float4* velRho, uint8_t* flags,
+                         uint32_t* tileCounts, uint32_t* nOut, float* out, uint64_t stride, cudaStream_t s);
+void LaunchMeshFlags(const uint64_t* idB, uint32_t n, uint64_t meshIdBegin, uint8_t* out, cudaStream_t s);
+
 // ---- contact_kernels.cu: rigid contact solver (rigid_solver.cpp:90-799)
 struct ContactState {
     double errSum;

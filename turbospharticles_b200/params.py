@@ -42,6 +42,7 @@ class SimParams:
     cubicSplineAlphaOverride: float = 0.0
     rigidContactDensityDevTarget: float = 0.001   # parameters_sim.h:100
     rigidContactMaxSolverIters: int = 100         # parameters_sim.h:101
+    surfaceNbrCountThreshold: int = 27            # parameters_sim.h:170 (export surface classification)
     # scene-building parameters (builder.cpp; not read by the step)
     jitterFracF: float = 0.0
     jitterSeedF: int = 42
@@ -71,7 +72,7 @@ class SimParams:
                   "jacobiOmega", "jacobiWarmStart", "densityDevTarget", "fixedIters",
                   "minSolverIters", "maxSolverIters", "solverTerminationCond",
                   "gridCellSizeRatio", "boundaryLayers", "cubicSplineAlphaOverride",
-                  "rigidContactDensityDevTarget", "rigidContactMaxSolverIters"):
+                  "rigidContactDensityDevTarget", "rigidContactMaxSolverIters", "surfaceNbrCountThreshold"):
             setattr(p, f, getattr(self, f))
         for a in range(3):
             p.gravity[a] = self.gravity[a]

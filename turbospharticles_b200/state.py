@@ -10,7 +10,7 @@ import ctypes as C
 
 import numpy as np
 
-from .abi import TspStateView
+from .abi import NO_MESH_ID, TspExportSnapshot, TspStateView
 
 FLUID_F32 = ["xPosF", "yPosF", "zPosF", "xVelF", "yVelF", "zVelF", "xVelPredF", "yVelPredF",
              "zVelPredF", "xAccPressF", "yAccPressF", "zAccPressF", "sourceTermF", "diagElemF",
@@ -72,3 +72,45 @@ class UniversalSimState:
 
     def sync_counts_from(self, v: TspStateView):
         self.step, self.time = int(v.step), float(v.time)
+
+
+EXPORT_F32 = {"F": ["xPosF", "yPosF", "zPosF", "velMagF"], "B": ["xPosB", "yPosB", "zPosB", "volB"],
+              "R": ["xPosR", "yPosR", "zPosR", "volR"]}
+
+
+class ExportSnapshot:
+    """Mirrors `Sync::ExportSnapshot` (source/simulation/sync/snapshots.h:37-66): the surface
+    fluid particles (positions, velocity magnitudes), the boundary particles (positions,
+    volumes, mesh flags) and the rigid particles (world positions, volumes, body indices) of
+    one export. `rankF` stays empty outside distributed runs, as in the reference."""
+
+    def __init__(self, N_F=0, N_B=0, N_R=0):
+        self.simStep, self.simTime = 0, 0.0
+        self.N_F, self.N_B, self.N_R = int(N_F), int(N_B), int(N_R)
+        for pop, n in (("F", self.N_F), ("B", self.N_B), ("R", self.N_R)):
+            for name in EXPORT_F32[pop]:
+                setattr(self, name, np.zeros(n, np.float32))
+        self.isMeshB = np.zeros(self.N_B, np.uint8)
+        self.bodyIdR = np.zeros(self.N_R, np.uint32)
+        self.rankF = np.zeros(0, np.uint16)
+
+    @classmethod
+    def pack(cls, packer, counts, params_c, include_b=True, mesh_id_begin_b=None):
+        """Allocate full-size arrays for the backend's counts, let `packer(cparams, include_b,
+        mesh_begin, view)` fill them, and trim each population to the exported count."""
+        nF, nB, nR = counts
+        snap = cls(nF, nB if include_b else 0, nR)
+        v = TspExportSnapshot()
+        for name, ctype in TspExportSnapshot._fields_[6:]:
+            arr = getattr(snap, name)
+            setattr(v, name, arr.ctypes.data_as(ctype) if arr.size else None)
+        packer(C.byref(params_c), 1 if include_b else 0,
+               NO_MESH_ID if mesh_id_begin_b is None else int(mesh_id_begin_b), C.byref(v))
+        snap.simStep, snap.simTime = int(v.simStep), float(v.simTime)
+        snap.N_F, snap.N_B, snap.N_R = int(v.N_F), int(v.N_B), int(v.N_R)
+        for pop, n in (("F", snap.N_F), ("B", snap.N_B), ("R", snap.N_R)):
+            for name in EXPORT_F32[pop]:
+                setattr(snap, name, getattr(snap, name)[:n].copy())
+        snap.isMeshB = snap.isMeshB[:snap.N_B].copy()
+        snap.bodyIdR = snap.bodyIdR[:snap.N_R].copy()
+        return snap
