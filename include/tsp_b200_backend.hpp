@@ -53,6 +53,10 @@ public:
         Check(tsp_b200_get_stats(h_, &s));
         return s;
     }
+    // I_SimBackend::FillStatisticsRecord (backend_sim.h:243): record[k] is Stats::StatMetric k
+    void FillStatisticsRecord(const tsp_params& params, double (&record)[TSP_STAT_COUNT]) const {
+        Check(tsp_b200_fill_statistics(h_, &params, record, TSP_STAT_COUNT));
+    }
     // SimBackend_CPU::GetRigidContactReport (source/simulation/CPU/backend/cpu_backend.h:132)
     tsp_contact_report GetRigidContactReport() const {
         tsp_contact_report r{};

@@ -1,6 +1,7 @@
 // Drives the B200 backend through the C++ adapter (include/tsp_b200_backend.hpp) the way the
 // reference's SimulationMgr drives I_SimBackend: pull, neighbor search, steps, push.
-// A 16^3 fluid lattice in free fall (no walls) must fall by g t^2 / 2 to FP32 accuracy.
+// A 16^3 fluid lattice in free fall (no walls) must fall by g t^2 / 2 to FP32 accuracy; the
+// statistics record and the export snapshot come through the same adapter.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -47,6 +48,17 @@ int main() {
                     got, expected, be.Stats().solverIters);
         if (std::fabs(got - expected) > 2e-2 * std::fabs(expected)) return 2;  // FP32 position rounding
         if (o.N_F != N || be.Stats().step != (uint64_t)steps) return 3;
+        double rec[TSP_STAT_COUNT];
+        be.FillStatisticsRecord(p, rec);
+        const double vExpected = 9.81 * dt * steps;  // every particle falls at the same speed
+        std::printf("NumF=%g VelMag_Avg=%.9g expected=%.9g\n", rec[TSP_STAT_NUM_F], rec[TSP_STAT_VEL_MAG_AVG], vExpected);
+        if (rec[TSP_STAT_NUM_F] != N || std::fabs(rec[TSP_STAT_VEL_MAG_AVG] - vExpected) > 2e-2 * vExpected) return 4;
+        std::vector<float> ex(N), ey(N), ez(N), ev(N);
+        tsp_export_snapshot snap{};
+        snap.xPosF = ex.data(); snap.yPosF = ey.data(); snap.zPosF = ez.data(); snap.velMagF = ev.data();
+        be.PackExportSnapshot(snap, p, false);
+        std::printf("exported %u of %u fluid particles\n", snap.N_F, N);
+        if (snap.N_F == 0 || snap.N_F > N || snap.N_B != 0 || snap.simStep != (uint64_t)steps) return 5;
     } catch (const std::exception& e) {
         std::printf("error: %s\n", e.what());
         return 1;
