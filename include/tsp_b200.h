@@ -341,6 +341,41 @@ typedef struct tsp_export_snapshot {
 int tsp_b200_pack_export_snapshot(tsp_backend* h, const tsp_params* params, int include_b,
                                   uint64_t mesh_id_begin_b, tsp_export_snapshot* snap);
 
+/* ---- mesh surface sampling ---------------------------------------------------------------
+ * Scene::SurfaceSampler (source/simulation/scene/geometry/surface_sampling.cpp): deterministic
+ * Poisson sampling of a triangle surface (seeded candidates, area-proportional triangle choice,
+ * acceptance in cell phase groups at a minimum spacing) followed by coverage repair (barycentric
+ * probe lattices; a probe farther than max(minDistance, maxDistance - probeSpacing) from every
+ * sample becomes a sample). Used for mesh boundaries and mesh rigid bodies
+ * (boundary_mesh_helpers.h, rigid_mesh_helpers.h). Parameters: parameters_sim.h:122-139. */
+typedef struct tsp_surface_sampling_params {
+    float minDistance;             /* minimum accepted sample spacing */
+    float maxDistance;             /* maximum surface-to-sample gap */
+    float coverageProbeSpacing;    /* spacing of the coverage probes */
+    float particleSizeF;           /* the sampling may not be coarser than the fluid spacing */
+    uint32_t candidateMultiplier;  /* candidates = multiplier x estimated sample count */
+    uint32_t reserved;
+    uint64_t seed;
+} tsp_surface_sampling_params;
+/* SurfaceSamplingStats (surface_sampling.h:18-26) */
+typedef struct tsp_surface_sampling_stats {
+    uint64_t N_candidates;
+    uint32_t N_initialSamples;
+    uint32_t N_coverageRepairs;
+    uint64_t N_coverageProbes;
+    float surfaceArea;
+    uint32_t reserved;
+} tsp_surface_sampling_stats;
+/* SurfaceSampler::Sample on the GPU `device` (-1: current): `vertices` 3*nV floats (x, y, z),
+ * `triangles` 3*nT vertex indices. The samples (x, y, z) go to `out` (capacity `cap` samples) and
+ * their count to *nOut; a too small `cap` returns TSP_ERR_OVERFLOW with *nOut = the count needed
+ * (the result is deterministic, so a second call with that capacity returns it). Invalid meshes
+ * or parameters return TSP_ERR_INVALID with the reference's message (tsp_b200_last_error(NULL)).
+ * `stats` may be NULL. */
+int tsp_b200_sample_surface(int device, const float* vertices, uint32_t nV, const uint32_t* triangles, uint32_t nT,
+                            const tsp_surface_sampling_params* params, float* out, uint64_t cap, uint64_t* nOut,
+                            tsp_surface_sampling_stats* stats);
+
 /* ---- served batch ------------------------------------------------------------------------
  * No counterpart in the reference (its SimulationMgr runs one scene per backend). A batch keeps
  * many independent scenes of one physics setup resident on one GPU and advances all of them

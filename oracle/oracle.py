@@ -58,6 +58,9 @@ def lib():
             "orc_read_field": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32]),
             "orc_write_field": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32]),
             "orc_kernel_eval": (None, [C.c_float] * 6 + [C.POINTER(C.c_float)]),
+            "orc_surface_last_error": (C.c_char_p, []),
+            "orc_sample_surface": (C.c_int, [C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32,
+                                             vp, C.POINTER(C.c_float), C.c_uint64, C.POINTER(C.c_uint64), vp]),
         }
         for n, (r, a) in sig.items():
             f = getattr(L, n)
@@ -69,6 +72,16 @@ def lib():
 
 def _p(a):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def sample_surface(mesh, sp):
+    """Sequential CPU restatement of SurfaceSampler::Sample (surface_oracle.cpp): the checker of
+    turbospharticles_b200.mesh.sample_surface."""
+    from turbospharticles_b200.mesh import _sample_with
+    L = lib()
+    return _sample_with(lambda v, nv, t, nt, p, o, cap, n, st: L.orc_sample_surface(
+        v, nv, t, nt, C.cast(p, C.c_void_p), o, cap, n, C.cast(st, C.c_void_p)), mesh, sp,
+        lambda: L.orc_surface_last_error().decode())
 
 
 class OracleBackend:

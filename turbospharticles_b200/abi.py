@@ -123,6 +123,19 @@ class TspExportSnapshot(C.Structure):
 
 
 NO_MESH_ID = (1 << 64) - 1
+TSP_ERR_INVALID, TSP_ERR_OVERFLOW = -1, -3
+
+
+class TspSurfaceSamplingParams(C.Structure):
+    """tsp_surface_sampling_params (parameters_sim.h:122-139)."""
+    _fields_ = [("minDistance", _f), ("maxDistance", _f), ("coverageProbeSpacing", _f), ("particleSizeF", _f),
+                ("candidateMultiplier", _u32), ("reserved", _u32), ("seed", C.c_uint64)]
+
+
+class TspSurfaceSamplingStats(C.Structure):
+    """tsp_surface_sampling_stats (SurfaceSamplingStats, surface_sampling.h:18-26)."""
+    _fields_ = [("N_candidates", C.c_uint64), ("N_initialSamples", _u32), ("N_coverageRepairs", _u32),
+                ("N_coverageProbes", C.c_uint64), ("surfaceArea", _f), ("reserved", _u32)]
 
 _VP = C.c_void_p
 EXPORTS = {
@@ -156,6 +169,8 @@ EXPORTS = {
     "tsp_b200_get_contact_report": (C.c_int, [_VP, C.POINTER(TspContactReport)]),
     "tsp_b200_pack_export_snapshot": (C.c_int, [_VP, C.POINTER(TspParams), C.c_int, C.c_uint64,
                                                 C.POINTER(TspExportSnapshot)]),
+    "tsp_b200_sample_surface": (C.c_int, [C.c_int, _pf, _u32, _pu32, _u32, C.POINTER(TspSurfaceSamplingParams), _pf,
+                                          C.c_uint64, _pu64, C.POINTER(TspSurfaceSamplingStats)]),
     "tsp_b200_get_phase_times": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_uint32, C.POINTER(C.c_uint32)]),
     "tsp_b200_try_build_cell_frame": (C.c_int, [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int32),
                                                  C.POINTER(C.c_uint32)]),

@@ -14,7 +14,7 @@ import sys
 from .abi import LIB_PATH, PKG_DIR
 
 CSRC = os.path.join(PKG_DIR, "csrc")
-SOURCES = ["backend.cu", "ns_kernels.cu", "sph_kernels.cu", "rigid_kernels.cu", "noalloc.cu", "batch.cu", "contact_kernels.cu", "stats_kernels.cu", "export_kernels.cu"]
+SOURCES = ["backend.cu", "ns_kernels.cu", "sph_kernels.cu", "rigid_kernels.cu", "noalloc.cu", "batch.cu", "contact_kernels.cu", "stats_kernels.cu", "export_kernels.cu", "surface_kernels.cu"]
 HEADERS = ["common.cuh", "kernels.h", "primitives.cuh", "host_common.h"]
 INCLUDE = os.path.join(os.path.dirname(PKG_DIR), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

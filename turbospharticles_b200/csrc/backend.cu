@@ -1623,6 +1623,29 @@ int tsp_b200_pack_export_snapshot(tsp_backend* h, const tsp_params* params, int 
     if (!params || !snap) return TSP_ERR_INVALID;
     TSP_GUARD(h, h->b->PackExport(*params, include_b != 0, mesh_id_begin_b, *snap));
 }
+int tsp_b200_sample_surface(int device, const float* vertices, uint32_t nV, const uint32_t* triangles, uint32_t nT,
+                            const tsp_surface_sampling_params* params, float* out, uint64_t cap, uint64_t* nOut,
+                            tsp_surface_sampling_stats* stats) {
+    if (!params || !nOut) { g_lastError = "NULL argument"; return TSP_ERR_INVALID; }
+    try {
+        tsp_surface_sampling_stats st{};
+        const std::vector<float> smp = tsp::SampleSurfaceGpu(device, vertices, nV, triangles, nT, *params, st);
+        if (stats) *stats = st;
+        *nOut = smp.size() / 3;
+        if (*nOut > cap || !out) {
+            g_lastError = "surface sample buffer too small";
+            return TSP_ERR_OVERFLOW;
+        }
+        std::memcpy(out, smp.data(), smp.size() * sizeof(float));
+        return TSP_OK;
+    } catch (const Error& e) {
+        g_lastError = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_lastError = e.what();
+        return TSP_ERR_INVALID;
+    }
+}
 int tsp_b200_get_phase_times(const tsp_backend* h, float* ms, uint32_t cap, uint32_t* n) {
     TSP_NEED(h);
     if (!n || (cap && !ms)) return TSP_ERR_INVALID;

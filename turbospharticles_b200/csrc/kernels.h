@@ -4,9 +4,11 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "../../include/tsp_b200.h"
 
 namespace tsp {
 
@@ -250,6 +252,11 @@ void LaunchExportSurface(const SellView& ff, const uint16_t* cntFB, const uint16
                          uint32_t threshold, const float4* posP, const float4* velRho, uint8_t* flags,
                          uint32_t* tileCounts, uint32_t* nOut, float* out, uint64_t stride, cudaStream_t s);
 void LaunchMeshFlags(const uint64_t* idB, uint32_t n, uint64_t meshIdBegin, uint8_t* out, cudaStream_t s);
+
+// ---- surface_kernels.cu: mesh surface sampling (SurfaceSampler, surface_sampling.cpp); throws
+//      Error(TSP_ERR_INVALID) with the reference's message for invalid meshes / parameters
+std::vector<float> SampleSurfaceGpu(int device, const float* vtx, uint32_t nV, const uint32_t* tri, uint32_t nT,
+                                    const tsp_surface_sampling_params& p, tsp_surface_sampling_stats& st);
 
 // ---- contact_kernels.cu: rigid contact solver (rigid_solver.cpp:90-799)
 struct ContactState {

@@ -43,6 +43,22 @@ class SimParams:
     rigidContactDensityDevTarget: float = 0.001   # parameters_sim.h:100
     rigidContactMaxSolverIters: int = 100         # parameters_sim.h:101
     surfaceNbrCountThreshold: int = 27            # parameters_sim.h:170 (export surface classification)
+    # mesh surface sampling (parameters_sim.h:122-139); the distances follow the ratios x
+    # particleSizeB (UpdateSurfaceSamplingDistances_, parameters_sim.cpp:2032-2046)
+    surfaceSamplingMinDistanceRatioB: float = 0.8
+    surfaceSamplingMaxDistanceRatioB: float = 1.0
+    surfaceSamplingCoverageProbeSpacingRatioB: float = 0.2
+    surfaceSamplingMinDistanceRatioR: float = 0.8
+    surfaceSamplingMaxDistanceRatioR: float = 1.0
+    surfaceSamplingCoverageProbeSpacingRatioR: float = 0.2
+    surfaceSamplingMinDistanceB: float = 0.008
+    surfaceSamplingMaxDistanceB: float = 0.01
+    surfaceSamplingCoverageProbeSpacingB: float = 0.002
+    surfaceSamplingMinDistanceR: float = 0.008
+    surfaceSamplingMaxDistanceR: float = 0.01
+    surfaceSamplingCoverageProbeSpacingR: float = 0.002
+    surfaceSamplingCandidateMultiplier: int = 8
+    surfaceSamplingSeed: int = 42
     # scene-building parameters (builder.cpp; not read by the step)
     jitterFracF: float = 0.0
     jitterSeedF: int = 42
@@ -59,6 +75,10 @@ class SimParams:
         self.massB = self.massF
         self.kernelRadius = float(f32(f32(self.kernelSuppRatio) * h32))
         self.kernelRadiusSqu = float(f32(f32(self.kernelRadius) * f32(self.kernelRadius)))
+        for kind in ("B", "R"):
+            for q in ("MinDistance", "MaxDistance", "CoverageProbeSpacing"):
+                ratio = f32(getattr(self, f"surfaceSampling{q}Ratio{kind}"))
+                setattr(self, f"surfaceSampling{q}{kind}", float(f32(ratio * f32(self.particleSizeB))))
         return self
 
     def set_rest_density(self, rho: float) -> "SimParams":

@@ -401,6 +401,24 @@ def floating_cubes(seed=5, dx=0.03, dt=1e-3):
     return st, dmin, dmax, p
 
 
+def floating_mesh_body(seed=5, dx=0.03, dt=1e-3, radius=0.1, density=500.0, sampler=None):
+    """Mesh rigid-body scene: the floating-cubes fluid slab and tank with one icosphere body
+    (radius `radius`, density `density`), sampled from its triangle surface by the mesh surface
+    sampler (GPU by default), resting on the fluid surface."""
+    from . import mesh as M
+    from .params import dam_params
+    p = dam_params(dx, dt)
+    p.jitterFracF = 0.01
+    p.jitterSeedF = seed
+    container = OBB((0.0, 0.0, 0.0), (0.9, 0.6, 0.6))
+    top = (10 + 0.5) * dx
+    fluid = OBB((0.0, 0.0, 0.0), ((30 + 0.5) * dx, top, (20 + 0.5) * dx))
+    st, dmin, dmax = breaking_dam(container, fluid, p)
+    st, _ = M.build_rigid_mesh(st, M.icosphere(1.0, 2), p, 2.0 * radius, density, (0.45, top + radius + 0.6 * dx, 0.3),
+                               M.euler_orientation(20.0, 10.0, 5.0), sampler=sampler)
+    return st, dmin, dmax, p
+
+
 @dataclasses.dataclass
 class ServedSceneSpec:
     """One scene of the served stream: a block of nx x ny x nz fluid particles (spacing dx)
