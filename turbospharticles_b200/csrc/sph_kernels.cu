@@ -9,6 +9,7 @@
 // the operation order of the reference CPU kernels (source/simulation/CPU/backend/
 // sph_solver.cpp:734-2089) with explicit fmaf where the reference uses fma, and the FF, FB
 // and FR partial sums are kept apart and combined exactly as the reference combines them.
+
 #include "kernels.h"
 
 namespace tsp {
@@ -28,7 +29,15 @@ constexpr uint32_t SPH_THREADS = 256;
 // 1: the list entries and gradient factors of the next slot group are loaded before the
 // gathers of the current group (one group of loads always in flight)
 #ifndef TSP_SPH_PIPELINE
-#define TSP_SPH_PIPELINE 0
+#define TSP_SPH_PIPELINE 1
+#endif
+// FF slots per group of the gradient-factor sweeps (pressure acceleration, Jacobi); measured on
+// the 1M dam: pipelined 3 / 2 slots beat 4 / 4 by 20 % / 9 %
+#ifndef TSP_PACC_FF_SLOTS
+#define TSP_PACC_FF_SLOTS 3
+#endif
+#ifndef TSP_JACOBI_FF_SLOTS
+#define TSP_JACOBI_FF_SLOTS 2
 #endif
 
 struct ChunkCursor {
@@ -49,84 +58,29 @@ struct ChunkCursor {
     }
 };
 
-// Visits the FF slots of a lane in order, U slots at a time: the U list entries are loaded
-// together, then the U neighbor gathers (one or two float4 each), then the U pair terms are
-// applied in slot order. The sum order is unchanged; the loads of a group are independent, so
-// up to 3U memory requests per lane are in flight instead of one dependent chain per slot.
-template <int U, bool TWO, typename Body>
-__device__ __forceinline__ void SweepSlots(const ChunkCursor& cur, const SellView& v, uint32_t lane,
-                                           const float4* A, const float4* B, Body&& body) {
-    for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
-        uint32_t j[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) j[u] = (k0 + u < cur.cnt) ? cur.nbr(v, k0 + u, lane) : EMPTY_32;
-        float4 a[U], b[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            a[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-            b[u] = a[u];
-            if (j[u] != EMPTY_32) {
-                a[u] = A[j[u]];
-                if (TWO) b[u] = B[j[u]];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++)
-            if (j[u] != EMPTY_32) body(k0 + u, j[u], a[u], b[u]);
-    }
-}
-
-// as SweepSlots, also loading each slot's recorded kernel-gradient factor (no sqrt / division)
-#if TSP_SPH_PIPELINE
-template <int U, bool TWO, typename Body>
-__device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellView& v, uint32_t lane,
-                                             const float4* A, const float4* B, Body&& body) {
-    uint32_t jn[U];
-    float kn[U];
-#pragma unroll
-    for (int u = 0; u < U; u++) {
-        const bool ok = (uint32_t)u < cur.cnt;
-        jn[u] = ok ? cur.nbr(v, u, lane) : EMPTY_32;
-        kn[u] = ok ? *cur.kgSlot(v, u, lane) : 0.0f;
-    }
-    for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
-        uint32_t j[U];
-        float kg[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) { j[u] = jn[u]; kg[u] = kn[u]; }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const bool ok = k0 + U + u < cur.cnt;
-            jn[u] = ok ? cur.nbr(v, k0 + U + u, lane) : EMPTY_32;
-            kn[u] = ok ? *cur.kgSlot(v, k0 + U + u, lane) : 0.0f;
-        }
-        float4 a[U], b[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            a[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-            b[u] = a[u];
-            if (j[u] != EMPTY_32) {
-                a[u] = A[j[u]];
-                if (TWO) b[u] = B[j[u]];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++)
-            if (j[u] != EMPTY_32) body(kg[u], a[u], b[u]);
-    }
-}
-#else
-template <int U, bool TWO, typename Body>
-__device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellView& v, uint32_t lane,
-                                             const float4* A, const float4* B, Body&& body) {
+// Visits the slots of a lane in order, U slots at a time: the U list entries (and, with KG,
+// the U recorded kernel-gradient factors) are loaded together, then the U neighbor gathers (one
+// or two float4 each), then the U pair terms are applied in slot order. The sum order is
+// unchanged; the loads of a group are independent, so up to 3U (4U) memory requests per lane
+// are in flight. The chunk's format is resolved once per chunk (D16: Delta16x2, else Abs32),
+// not per slot.
+template <int U, bool TWO, bool KG, bool D16, typename Body>
+__device__ __forceinline__ void SweepFmt(const ChunkCursor& cur, const SellView& v, uint32_t lane,
+                                         const float4* A, const float4* B, Body&& body) {
     for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
         uint32_t j[U];
         float kg[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const bool ok = k0 + u < cur.cnt;
-            j[u] = ok ? cur.nbr(v, k0 + u, lane) : EMPTY_32;
-            kg[u] = ok ? *cur.kgSlot(v, k0 + u, lane) : 0.0f;
+            const uint64_t lin = cur.off + (uint64_t)(k0 + u) * SELL_W + lane;
+            if constexpr (D16) {
+                const uint32_t e = ok ? v.list16[lin] : 0u;
+                j[u] = ok ? ((e & 0x8000u) ? cur.base2 + (e & 0x7fffu) : cur.base + e) : EMPTY_32;
+            } else {
+                j[u] = ok ? v.list32[lin] : EMPTY_32;
+            }
+            if constexpr (KG) kg[u] = ok ? (D16 ? v.kg16 : v.kg32)[lin] : 0.0f;
         }
         float4 a[U], b[U];
 #pragma unroll
@@ -135,15 +89,81 @@ __device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellV
             b[u] = a[u];
             if (j[u] != EMPTY_32) {
                 a[u] = A[j[u]];
-                if (TWO) b[u] = B[j[u]];
+                if constexpr (TWO) b[u] = B[j[u]];
             }
         }
 #pragma unroll
-        for (int u = 0; u < U; u++)
-            if (j[u] != EMPTY_32) body(kg[u], a[u], b[u]);
+        for (int u = 0; u < U; u++) {
+            if (j[u] == EMPTY_32) continue;
+            if constexpr (KG) body(kg[u], a[u], b[u]);
+            else body(k0 + u, j[u], a[u], b[u]);
+        }
     }
 }
+#if TSP_SPH_PIPELINE
+// pipelined: the list entries (and factors) of group g + 1 are loaded before the gathers of
+// group g, so one group of stream loads is always in flight; same slots, same order
+template <int U, bool TWO, bool KG, bool D16, typename Body>
+__device__ __forceinline__ void SweepFmtPipe(const ChunkCursor& cur, const SellView& v, uint32_t lane,
+                                             const float4* A, const float4* B, Body&& body) {
+    uint32_t jn[U];
+    float kn[U];
+    auto fetch = [&](uint32_t k0) {
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool ok = k0 + u < cur.cnt;
+            const uint64_t lin = cur.off + (uint64_t)(k0 + u) * SELL_W + lane;
+            if constexpr (D16) {
+                const uint32_t e = ok ? v.list16[lin] : 0u;
+                jn[u] = ok ? ((e & 0x8000u) ? cur.base2 + (e & 0x7fffu) : cur.base + e) : EMPTY_32;
+            } else {
+                jn[u] = ok ? v.list32[lin] : EMPTY_32;
+            }
+            if constexpr (KG) kn[u] = ok ? (D16 ? v.kg16 : v.kg32)[lin] : 0.0f;
+        }
+    };
+    fetch(0);
+    for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
+        uint32_t j[U];
+        float kg[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) { j[u] = jn[u]; kg[u] = KG ? kn[u] : 0.0f; }
+        fetch(k0 + U);
+        float4 a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            a[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+            b[u] = a[u];
+            if (j[u] != EMPTY_32) {
+                a[u] = A[j[u]];
+                if constexpr (TWO) b[u] = B[j[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (j[u] == EMPTY_32) continue;
+            if constexpr (KG) body(kg[u], a[u], b[u]);
+            else body(k0 + u, j[u], a[u], b[u]);
+        }
+    }
+}
+#define TSP_SWEEP_IMPL SweepFmtPipe
+#else
+#define TSP_SWEEP_IMPL SweepFmt
 #endif
+template <int U, bool TWO, typename Body>
+__device__ __forceinline__ void SweepSlots(const ChunkCursor& cur, const SellView& v, uint32_t lane,
+                                           const float4* A, const float4* B, Body&& body) {
+    if (cur.fmt == FMT_DELTA16X2) TSP_SWEEP_IMPL<U, TWO, false, true>(cur, v, lane, A, B, body);
+    else TSP_SWEEP_IMPL<U, TWO, false, false>(cur, v, lane, A, B, body);
+}
+// as SweepSlots, also loading each slot's recorded kernel-gradient factor (no sqrt / division)
+template <int U, bool TWO, typename Body>
+__device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellView& v, uint32_t lane,
+                                             const float4* A, const float4* B, Body&& body) {
+    if (cur.fmt == FMT_DELTA16X2) TSP_SWEEP_IMPL<U, TWO, true, true>(cur, v, lane, A, B, body);
+    else TSP_SWEEP_IMPL<U, TWO, true, false>(cur, v, lane, A, B, body);
+}
 
 // persistent warps: warp w of the grid handles chunks w, w + W, w + 2W, ...
 #define FOR_EACH_CHUNK(n)                                                                  \
@@ -349,7 +369,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KPressureAcc(
         float ax = 0.f, ay = 0.f, az = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsKg<TSP_SPH_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsKg<TSP_PACC_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float a = (fOuter + c.massF * pj.w * c.densInvSqu) * kg;
             ax = fmaf(a, dx, ax); ay = fmaf(a, dy, ay); az = fmaf(a, dz, az);
@@ -388,7 +408,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KJacobi(Const
         float sF = 0.f, sB = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsKg<TSP_SPH_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.acc, [&](float kg, const float4& pj, const float4& aj) {
+        SweepSlotsKg<TSP_JACOBI_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.acc, [&](float kg, const float4& pj, const float4& aj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
             const float sv = fmaf(dax, dx, fmaf(day, dy, daz * dz));
