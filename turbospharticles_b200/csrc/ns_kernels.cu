@@ -481,6 +481,47 @@ __device__ __forceinline__ void QueryWalk(const QueryArgs& a, const QueryScene& 
     }
 }
 
+// count walk of the fluid and boundary species, QUERY_WALK_U candidates of the current range per
+// iteration (their loads in flight together); same candidates, same order, same rows as QueryWalk
+#ifndef QUERY_WALK_U
+#define QUERY_WALK_U 4
+#endif
+template <int SP>
+__device__ __forceinline__ void QueryWalkCountU(const QueryArgs& a, const QueryScene& sc, const QueryWarp& w,
+                                                const QueryLaneInfo& q, uint32_t g0, uint32_t nb, LaneRefs& ref,
+                                                uint32_t* scr, uint32_t ks) {
+    static_assert(SP != 2, "rigid candidates go through the permutation (QueryWalk)");
+    constexpr uint32_t U = QUERY_WALK_U;
+    const float4* pos = SP == 0 ? a.posF : a.posB;
+    const uint32_t sv = StencilVolume(sc.fr.reach);
+    const bool mine = q.g != EMPTY_32 && q.g >= g0 && q.g < g0 + nb;
+    const uint32_t gl = mine ? q.g - g0 : 0u;
+    const uint32_t n = mine ? w.nne[gl] : 0u;
+    const uint2* rows = w.srt + gl * sv;
+    uint32_t k = 0, j = 0, e = 0;
+    if (n > 0) { const uint2 v = rows[0]; j = v.x; e = v.y; }
+    uint32_t* sp = scr + (uint64_t)ref.cnt * SELL_W;
+    while (k < n) {
+        const uint32_t m = min(U, e - j);  // candidates of this iteration, all in the current range
+        float4 p[U];
+#pragma unroll
+        for (uint32_t u = 0; u < U; u++) p[u] = (u < m) ? pos[j + u] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (uint32_t u = 0; u < U; u++) {
+            if (u < m && IsNeighbor(q.pi.x, q.pi.y, q.pi.z, p[u].x, p[u].y, p[u].z, a.r2)) {
+                if (ref.cnt < ks) *sp = j + u;
+                sp += SELL_W;
+                ref.cnt++;
+                ref.mx = j + u;
+            }
+        }
+        j += m;
+        if (j == e) {
+            if (++k < n) { const uint2 v = rows[k]; j = v.x; e = v.y; }
+        }
+    }
+}
+
 // whole-chunk walk of one species in group batches
 template <int SP, int MODE>
 __device__ __forceinline__ void QuerySpecies(const QueryArgs& a, const QueryScene& sc, const QueryWarp& w,
@@ -493,7 +534,10 @@ __device__ __forceinline__ void QuerySpecies(const QueryArgs& a, const QueryScen
     for (uint32_t g0 = 0; g0 < q.nGroups; g0 += gb) {
         const uint32_t nb = min(gb, q.nGroups - g0);
         QueryRanges<SP>(a, sc, w, g0, nb, lane);
-        QueryWalk<SP, MODE>(a, sc, w, q, g0, nb, lane, homeLo, homeHi, ref, scr, ks, wr, m);
+        if constexpr (MODE == WALK_COUNT && SP != 2)
+            QueryWalkCountU<SP>(a, sc, w, q, g0, nb, ref, scr, ks);
+        else
+            QueryWalk<SP, MODE>(a, sc, w, q, g0, nb, lane, homeLo, homeHi, ref, scr, ks, wr, m);
         __syncwarp();
     }
 }
