@@ -15,8 +15,9 @@ e2e: the same metric through the C ABI with pinned host buffers: per step pull_s
 the step's particle state) + step + push_state (D2H of positions, velocities, pressure,
 density).
 served: the seeded mixed-size served stream (continuous batching, turbospharticles_b200.serve;
-64 scenes x 100 steps by default, --served-scenes 256 --served-steps 500 for the full stream)
-against the same scenes one at a time on the plain one-scene path, both device-timed.
+256 scenes x 500 steps, the full stream, by default; --served-scenes 0 skips it) against the
+same scenes one at a time on the plain one-scene path, both device-timed; value_wall is the
+served loop's host wall clock (admission, relayout and read-back included).
 --impl reference: the CPU restatement of the reference step (oracle/, OpenMP over all host
 threads) on the same workload; the reference's own CPU backend cannot be built here.
 """
@@ -362,9 +363,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--served-scenes", type=int, default=64,
+    ap.add_argument("--served-scenes", type=int, default=256,
                     help="scenes of the served-stream sub-measure (0: skip; 256 = the full stream)")
-    ap.add_argument("--served-steps", type=int, default=100)
+    ap.add_argument("--served-steps", type=int, default=500)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "b200" else args.warmup
     if args.impl == "reference":

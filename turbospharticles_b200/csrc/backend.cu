@@ -145,9 +145,9 @@ public:
         DBuf<uint8_t> format;
         DBuf<uint32_t> base, base2;
         DBuf<uint64_t> offset;
-        DBuf<uint16_t> l16;
-        DBuf<uint32_t> l32;
-        DBuf<float> kg16, kg32;  // recorded kernel-gradient factors, parallel to l16 / l32
+        VBuf<uint16_t> l16;  // grow in place: list growth keeps the addresses
+        VBuf<uint32_t> l32;
+        VBuf<float> kg16, kg32;  // recorded kernel-gradient factors, parallel to l16 / l32
         uint64_t n16 = 0, n32 = 0;
     } sell[3];
     bool kgValid = false;  // the recorded factors belong to the current positions and lists
@@ -161,7 +161,7 @@ public:
     uint64_t nNbr[3] = {0, 0, 0};
     DBuf<uint16_t> cntR[3];
     DBuf<uint64_t> offR[3];
-    DBuf<uint32_t> listR[3];
+    VBuf<uint32_t> listR[3];
     DBuf<uint64_t> csrTot;
     uint64_t csrN[3] = {0, 0, 0};
     bool listsValid = false;

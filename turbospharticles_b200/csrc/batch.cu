@@ -286,6 +286,10 @@ uint64_t BatchSceneBytes(uint64_t nFpad, uint64_t nB, uint64_t gridCells) {
     return nFpad * perF + nB * perB + gridCells * 8;
 }
 
+// list buffers of a batch grow faster than the one-scene backend's: admissions add whole
+// scenes' lists at once while the batch fills up
+constexpr double BATCH_LIST_GROWTH = 1.5;
+
 class Batch {
 public:
     struct Scene {
@@ -319,11 +323,18 @@ public:
     uint64_t launches = 0;
     float lastSubstepMs = 0.f;
 
-    // fluid arena (SELL32-chunk aligned scenes)
+    // fluid arena (SELL32-chunk aligned scenes). Arrays are sized to a chunk capacity that only
+    // grows, and scene-rank tables to a rank capacity plus one never-active rank that owns the
+    // chunks past the live ones; the Jacobi-loop graph is captured over the capacities and reads
+    // the live particle count from the device (dLiveN), so a relayout (admission / retirement)
+    // neither allocates nor invalidates the captured graph.
     uint32_t nFtot = 0, nChunks = 0;
-    DBuf<float4> posP, velRho, velPred, acc, posP2, velRho2, tmp4;
-    DBuf<float2> srcDiag, tmp2;
-    DBuf<uint64_t> idF, idF2, tmp8;
+    uint32_t chunkCap = 0, sceneCap = 0;
+    uint32_t hLiveN = 0;
+    DBuf<uint32_t> dLiveN;
+    DBuf<float4> posP, velRho, velPred, acc, posP2, velRho2, velPred2, acc2;
+    DBuf<float2> srcDiag, srcDiag2;
+    DBuf<uint64_t> idF, idF2;
     DBuf<uint8_t> chunkLen;
     DBuf<uint32_t> chunkScene, srcChunk;
     // boundary arena
@@ -357,9 +368,9 @@ public:
         DBuf<uint8_t> format;
         DBuf<uint32_t> base, base2;
         DBuf<uint64_t> offset;
-        DBuf<uint16_t> l16;
-        DBuf<uint32_t> l32;
-        DBuf<float> kg16, kg32;
+        VBuf<uint16_t> l16;  // grow in place: list growth keeps the addresses
+        VBuf<uint32_t> l32;
+        VBuf<float> kg16, kg32;
         uint64_t n16 = 0, n32 = 0;
     } sell[3];
     DBuf<uint32_t> scrF, scrB, scrR;
@@ -392,6 +403,8 @@ public:
         nbrTot.ensure(3);
         dNActive.ensure(1);
         CK(cudaMemset(dNActive.p, 0, 4));
+        dLiveN.ensure(1);
+        CK(cudaMemset(dLiveN.p, 0, 4));
         SetCellSize();
     }
     ~Batch() {
@@ -579,10 +592,19 @@ public:
         for (uint32_t slot : newOrder) tot += slots[slot].nFpad;
         if (tot > 0x7fffffe0ull) throw Error(TSP_ERR_OVERFLOW, "batch fluid arena exceeds 2^31 particles");
         const uint32_t nNew = (uint32_t)tot, chunksNew = nNew / SELL_W;
+        if (chunksNew > chunkCap) {
+            // doubling, but not past the chunks the memory budget can hold (each growth
+            // reallocates the arena and the scratch and re-captures the loop graph)
+            const uint64_t budgetChunks = budget / (BatchSceneBytes(SELL_W, 0, 0) * 1ull);
+            const uint64_t want = std::max<uint64_t>(std::min<uint64_t>(2ull * chunkCap, budgetChunks), chunksNew);
+            chunkCap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 64ull), 0x7fffffe0ull / SELL_W);
+        }
+        if (newOrder.size() > sceneCap) sceneCap = std::max<uint32_t>((uint32_t)newOrder.size(), std::max(2u * sceneCap, 16u));
+        const uint32_t padRank = sceneCap;  // owner of the padding chunks, never active
         // chunk map: surviving scenes move whole chunks
-        std::vector<uint32_t> srcMap(std::max<uint32_t>(chunksNew, 1), EMPTY_32);
-        std::vector<uint8_t> len(std::max<uint32_t>(chunksNew, 1), 0);
-        std::vector<uint32_t> scn(std::max<uint32_t>(chunksNew, 1), 0);
+        std::vector<uint32_t> srcMap(chunkCap, EMPTY_32);
+        std::vector<uint8_t> len(chunkCap, 0);
+        std::vector<uint32_t> scn(chunkCap, padRank);
         uint64_t at = 0;
         for (uint32_t r = 0; r < newOrder.size(); r++) {
             Scene& sc = slots[newOrder[r]];
@@ -597,33 +619,33 @@ public:
             sc.rank = r;
             at += sc.nFpad;
         }
-        // move surviving chunks into fresh arrays, then place the new scenes
-        DBuf<float4> nPos, nVel, nVelPred, nAcc;
-        DBuf<float2> nSd;
-        DBuf<uint64_t> nId;
-        const size_t cap = std::max<size_t>(nNew, 32);
-        nPos.ensure(cap); nVel.ensure(cap); nVelPred.ensure(cap); nAcc.ensure(cap); nSd.ensure(cap); nId.ensure(cap);
-        CK(cudaMemsetAsync(nVelPred.p, 0, cap * sizeof(float4), s));
-        CK(cudaMemsetAsync(nAcc.p, 0, cap * sizeof(float4), s));
-        CK(cudaMemsetAsync(nSd.p, 0, cap * sizeof(float2), s));
+        // move surviving chunks into the alternate arrays, then place the new scenes
+        const size_t cap = (size_t)chunkCap * SELL_W;
+        posP2.ensure(cap); velRho2.ensure(cap); velPred2.ensure(cap); acc2.ensure(cap); srcDiag2.ensure(cap);
+        idF2.ensure(cap);
+        if (nNew) {
+            CK(cudaMemsetAsync(velPred2.p, 0, nNew * sizeof(float4), s));
+            CK(cudaMemsetAsync(acc2.p, 0, nNew * sizeof(float4), s));
+            CK(cudaMemsetAsync(srcDiag2.p, 0, nNew * sizeof(float2), s));
+        }
         srcChunk.ensure(srcMap.size());
         CK(cudaMemcpyAsync(srcChunk.p, srcMap.data(), srcMap.size() * 4, cudaMemcpyHostToDevice, s));
         if (nFtot && chunksNew) {
             const unsigned g = (unsigned)((chunksNew * 32ull + 255) / 256);
-            KBatchMoveChunks<float4><<<g, 256, 0, s>>>(posP.p, nPos.p, srcChunk.p, chunksNew);
-            KBatchMoveChunks<float4><<<g, 256, 0, s>>>(velRho.p, nVel.p, srcChunk.p, chunksNew);
-            KBatchMoveChunks<float4><<<g, 256, 0, s>>>(velPred.p, nVelPred.p, srcChunk.p, chunksNew);
-            KBatchMoveChunks<float4><<<g, 256, 0, s>>>(acc.p, nAcc.p, srcChunk.p, chunksNew);
-            KBatchMoveChunks<float2><<<g, 256, 0, s>>>(srcDiag.p, nSd.p, srcChunk.p, chunksNew);
-            KBatchMoveChunks<uint64_t><<<g, 256, 0, s>>>(idF.p, nId.p, srcChunk.p, chunksNew);
+            KBatchMoveChunks<float4><<<g, 256, 0, s>>>(posP.p, posP2.p, srcChunk.p, chunksNew);
+            KBatchMoveChunks<float4><<<g, 256, 0, s>>>(velRho.p, velRho2.p, srcChunk.p, chunksNew);
+            KBatchMoveChunks<float4><<<g, 256, 0, s>>>(velPred.p, velPred2.p, srcChunk.p, chunksNew);
+            KBatchMoveChunks<float4><<<g, 256, 0, s>>>(acc.p, acc2.p, srcChunk.p, chunksNew);
+            KBatchMoveChunks<float2><<<g, 256, 0, s>>>(srcDiag.p, srcDiag2.p, srcChunk.p, chunksNew);
+            KBatchMoveChunks<uint64_t><<<g, 256, 0, s>>>(idF.p, idF2.p, srcChunk.p, chunksNew);
             launches += 6;
         }
         for (uint32_t slot : newOrder) {
             Scene& sc = slots[slot];
             if (sc.admitted) continue;
-            CK(cudaMemcpyAsync(nPos.p + sc.fStart, sc.upPos.data(), sc.nFpad * sizeof(float4), cudaMemcpyHostToDevice, s));
-            CK(cudaMemcpyAsync(nVel.p + sc.fStart, sc.upVel.data(), sc.nFpad * sizeof(float4), cudaMemcpyHostToDevice, s));
-            CK(cudaMemcpyAsync(nId.p + sc.fStart, sc.upId.data(), sc.nFpad * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(posP2.p + sc.fStart, sc.upPos.data(), sc.nFpad * sizeof(float4), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(velRho2.p + sc.fStart, sc.upVel.data(), sc.nFpad * sizeof(float4), cudaMemcpyHostToDevice, s));
+            CK(cudaMemcpyAsync(idF2.p + sc.fStart, sc.upId.data(), sc.nFpad * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
         }
         Sync();
         for (uint32_t slot : newOrder) {
@@ -634,8 +656,8 @@ public:
             std::vector<float4>().swap(sc.upVel);
             std::vector<uint64_t>().swap(sc.upId);
         }
-        Swap(posP, nPos); Swap(velRho, nVel); Swap(velPred, nVelPred); Swap(acc, nAcc); Swap(srcDiag, nSd);
-        Swap(idF, nId);
+        Swap(posP, posP2); Swap(velRho, velRho2); Swap(velPred, velPred2); Swap(acc, acc2); Swap(srcDiag, srcDiag2);
+        Swap(idF, idF2);
         posP2.ensure(cap); velRho2.ensure(cap); idF2.ensure(cap);
         chunkLen.ensure(len.size());
         chunkScene.ensure(scn.size());
@@ -644,8 +666,9 @@ public:
         order = newOrder;
         nFtot = nNew;
         nChunks = chunksNew;
-        const size_t S = std::max<size_t>(order.size(), 1);
+        const size_t S = (size_t)sceneCap + 1;  // + the padding rank
         dSc.ensure(S); dGeom.ensure(S); dSolver.ensure(S); dActive.ensure(S); dProbe.ensure(S);
+        CK(cudaMemsetAsync(dSc.p, 0, S * sizeof(BatchSceneDev), s));  // ranks >= order.size(): no fluid
         if (hCap < S) {
             if (hSolver) cudaFreeHost(hSolver);
             if (hProbe) cudaFreeHost(hProbe);
@@ -654,15 +677,20 @@ public:
             CK(cudaMallocHost(&hProbe, hCap * sizeof(ProbeResult)));
         }
         EnsureScratch();
+        hLiveN = nNew;
+        CK(cudaMemcpyAsync(dLiveN.p, &hLiveN, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
         Sync();
         layoutDirty = false;
     }
 
+    // scratch sized to the arena capacity (and the largest boundary of a live scene, grown by
+    // 1.25x), so a relayout allocates only when a capacity grows
     void EnsureScratch() {
-        const uint32_t n = std::max<uint32_t>(nFtot, 32), nc = std::max<uint32_t>(nChunks, 1);
+        const uint32_t n = std::max<uint32_t>(chunkCap * SELL_W, 32), nc = std::max<uint32_t>(chunkCap, 1);
         uint32_t nSort = n;  // sort / scan scratch also serves the boundary sort of one scene
         for (const auto& sc : slots)
             if (sc.live) nSort = std::max(nSort, sc.nB);
+        if (nSort > keysA.cap) nSort = (uint32_t)std::min<uint64_t>(nSort + nSort / 4ull, 0xffffffffull);
         keysA.ensure(nSort); keysB.ensure(nSort); valsA.ensure(nSort); valsB.ensure(nSort); cidF.ensure(n);
         uniqF.ensure(n); startF.ensure(n + 1ull);
         tileHist.ensure(RadixTileHistItems(nSort));
@@ -681,6 +709,7 @@ public:
         scrOver.ensure(nc);
         partials.ensure(3ull * nc);
         velPred.ensure(n); acc.ensure(n); srcDiag.ensure(n);
+        velPred2.ensure(n); acc2.ensure(n); srcDiag2.ensure(n);
     }
 
     // ------------------------------------------------------------------------ frames
@@ -795,12 +824,15 @@ public:
         return SellView{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p,
                         m.kg16.p, m.kg32.p};
     }
+    // masked: the Jacobi-loop view (n = the arena capacity, the live count read on the device,
+    // converged scenes masked out)
     FluidDev Fluid(bool masked) {
-        FluidDev f{posP.p, velRho.p, velPred.p, acc.p, srcDiag.p, nFtot};
+        FluidDev f{posP.p, velRho.p, velPred.p, acc.p, srcDiag.p, masked ? chunkCap * SELL_W : nFtot};
         f.chunkLen = chunkLen.p;
         f.chunkScene = chunkScene.p;
         f.sceneActive = masked ? dActive.p : nullptr;
         f.chunkPartials = masked ? partials.p : nullptr;
+        f.liveN = masked ? dLiveN.p : nullptr;
         return f;
     }
     void CheckErrors() {
@@ -817,7 +849,7 @@ public:
         auto P = [&](const void* q) { k.push_back((uint64_t)(uintptr_t)q); };
         const FluidDev f = Fluid(true);
         P(f.posP); P(f.velRho); P(f.velPred); P(f.acc); P(f.srcDiag); k.push_back(f.n);
-        P(f.chunkLen); P(f.chunkScene); P(f.sceneActive); P(f.chunkPartials);
+        P(f.chunkLen); P(f.chunkScene); P(f.sceneActive); P(f.chunkPartials); P(f.liveN);
         P(posB.p); P(volB.p);
         for (int s2 = 0; s2 < 3; s2++) {
             const SellView v = View(s2);
@@ -830,7 +862,7 @@ public:
         uint32_t tb;
         std::memcpy(&tb, &ctl.target, 4);
         k.push_back(tb);
-        P(dSc.p); P(dSolver.p); P(dActive.p); P(dNActive.p); k.push_back(order.size());
+        P(dSc.p); P(dSolver.p); P(dActive.p); P(dNActive.p); k.push_back(sceneCap);
         return k;
     }
     cudaGraphExec_t LoopGraphFor(const Consts& c, const SolverControl& ctl) {
@@ -856,7 +888,7 @@ public:
         const NeighborView nv{View(0), View(1), View(2)};
         LaunchPressureAcc(c, f, b, r, nv, capStream);
         LaunchJacobi(c, f, b, r, nv, ctl, nullptr, nullptr, 0ull, false, capStream);
-        const uint32_t S = (uint32_t)order.size();
+        const uint32_t S = sceneCap + 1;
         KBatchSceneReduce<<<(S * 32 + 127) / 128, 128, 0, capStream>>>(partials.p, dSc.p, dSolver.p, dActive.p,
                                                                       dNActive.p, ctl, S);
         KBatchLoopCond<<<1, 1, 0, capStream>>>(dNActive.p, handle);
@@ -964,7 +996,7 @@ public:
         Sync();
         for (int k = 0; k < 3; k++) {
             sell[k].n16 = tot[k].a; sell[k].n32 = tot[k].b;
-            sell[k].l16.grow(tot[k].a, LIST_GROWTH); sell[k].l32.grow(tot[k].b, LIST_GROWTH);
+            sell[k].l16.grow(tot[k].a, BATCH_LIST_GROWTH); sell[k].l32.grow(tot[k].b, BATCH_LIST_GROWTH);
             sell[k].kg16.ensure(sell[k].l16.cap); sell[k].kg32.ensure(sell[k].l32.cap);
         }
         LaunchQueryFluid(true, qa, Meta(0), Meta(1), Meta(2), s);
@@ -978,7 +1010,7 @@ public:
         LaunchDensity(c, f, b, rd, nv, s);
         LaunchNonPressure(c, f, b, rd, nv, s);
         LaunchSourceDiagInit(c, f, b, rd, nv, nullptr, s);
-        KBatchSolverReset<<<(S + 127) / 128, 128, 0, s>>>(dSolver.p, dActive.p, dSc.p, S);
+        KBatchSolverReset<<<(sceneCap + 1 + 127) / 128, 128, 0, s>>>(dSolver.p, dActive.p, dSc.p, sceneCap + 1);
         const SolverControl ctl{prm.minSolverIters, prm.maxSolverIters, prm.fixedIters, prm.solverTerminationCond,
                                 prm.densityDevTarget, 0u};
         CK(cudaGraphLaunch(LoopGraphFor(c, ctl), s));

@@ -7,6 +7,9 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
+#include <vector>
+#include <cuda.h>  // types of the driver's virtual-memory calls (resolved at run time, no libcuda link)
 #include <cuda_runtime.h>
 
 #include "../../include/tsp_b200.h"
@@ -51,12 +54,127 @@ struct DBuf {
 };
 template <typename T> inline void Swap(DBuf<T>& a, DBuf<T>& b) { std::swap(a.p, b.p); std::swap(a.cap, b.cap); }
 
+// The driver's virtual-memory entry points, looked up once through the runtime.
+struct VmmApi {
+    decltype(&cuMemAddressReserve) reserve = nullptr;
+    decltype(&cuMemAddressFree) addressFree = nullptr;
+    decltype(&cuMemCreate) create = nullptr;
+    decltype(&cuMemRelease) release = nullptr;
+    decltype(&cuMemMap) map = nullptr;
+    decltype(&cuMemUnmap) unmap = nullptr;
+    decltype(&cuMemSetAccess) setAccess = nullptr;
+    decltype(&cuMemGetAllocationGranularity) granularity = nullptr;
+    static const VmmApi& Get() {
+        static const VmmApi api = [] {
+            VmmApi a;
+            auto get = [](const char* name, void** fn) {
+                cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+                CK(cudaGetDriverEntryPointByVersion(name, fn, 12000, cudaEnableDefault, &q));
+                if (q != cudaDriverEntryPointSuccess || !*fn)
+                    throw Error(TSP_ERR_CUDA, std::string("driver entry point not found: ") + name);
+            };
+            get("cuMemAddressReserve", reinterpret_cast<void**>(&a.reserve));
+            get("cuMemAddressFree", reinterpret_cast<void**>(&a.addressFree));
+            get("cuMemCreate", reinterpret_cast<void**>(&a.create));
+            get("cuMemRelease", reinterpret_cast<void**>(&a.release));
+            get("cuMemMap", reinterpret_cast<void**>(&a.map));
+            get("cuMemUnmap", reinterpret_cast<void**>(&a.unmap));
+            get("cuMemSetAccess", reinterpret_cast<void**>(&a.setAccess));
+            get("cuMemGetAllocationGranularity", reinterpret_cast<void**>(&a.granularity));
+            return a;
+        }();
+        return api;
+    }
+};
+#define CKD(x)                                                                                      \
+    do {                                                                                            \
+        CUresult e_ = (x);                                                                          \
+        if (e_ != CUDA_SUCCESS) throw Error(TSP_ERR_CUDA, std::string(#x) + ": driver error " + std::to_string((int)e_)); \
+    } while (0)
+
+// Device buffer that grows in place: a virtual address range (8x the first request) is
+// reserved once and physical memory is mapped onto the end of the used part as the buffer
+// grows. The address does not change (graphs captured with it stay valid) and a growth costs
+// neither a copy, a free nor a device-wide synchronisation; only a request beyond the
+// reservation re-reserves (new address, contents not kept, like DBuf::ensure).
+template <typename T>
+struct VBuf {
+    T* p = nullptr;
+    size_t cap = 0;  // elements backed by physical memory
+    size_t reservedBytes = 0, mappedBytes = 0;
+    std::vector<std::pair<CUmemGenericAllocationHandle, size_t>> maps;  // in address order
+    VBuf() = default;
+    VBuf(const VBuf&) = delete;
+    VBuf& operator=(const VBuf&) = delete;
+    static CUmemAllocationProp Prop() {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CUmemAllocationProp prop{};
+        prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+        prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+        prop.location.id = dev;
+        return prop;
+    }
+    void ensure(size_t n) {  // contents of the backed part are kept unless re-reserved
+        const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        if (p && bytes <= mappedBytes) return;
+        const VmmApi& api = VmmApi::Get();
+        const CUmemAllocationProp prop = Prop();
+        size_t gran = 0;
+        CKD(api.granularity(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED));
+        const size_t need = (bytes + gran - 1) / gran * gran;
+        if (!p || need > reservedBytes) {
+            release();
+            const size_t want = std::max<size_t>(need * 8, size_t(64) << 20);
+            reservedBytes = (want + gran - 1) / gran * gran;
+            CUdeviceptr va = 0;
+            CKD(api.reserve(&va, reservedBytes, gran, 0, 0));
+            p = reinterpret_cast<T*>(va);
+        }
+        const size_t add = need - mappedBytes;
+        CUmemGenericAllocationHandle h = 0;
+        CKD(api.create(&h, add, &prop, 0));
+        const CUdeviceptr at = reinterpret_cast<CUdeviceptr>(p) + mappedBytes;
+        if (api.map(at, add, 0, h, 0) != CUDA_SUCCESS) {
+            api.release(h);
+            throw Error(TSP_ERR_CUDA, "cuMemMap of a growing neighbor-list buffer failed");
+        }
+        maps.emplace_back(h, add);
+        CUmemAccessDesc acc{};
+        acc.location = prop.location;
+        acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+        CKD(api.setAccess(at, add, &acc, 1));
+        mappedBytes = need;
+        cap = mappedBytes / sizeof(T);
+    }
+    void grow(size_t n, double slack) {
+        if (n <= cap && p) return;
+        ensure((size_t)((double)n * slack) + 16);
+    }
+    void release() {
+        if (!p) return;
+        cudaDeviceSynchronize();  // no kernel may still use the range (destruction / re-reservation only)
+        const VmmApi& api = VmmApi::Get();
+        CUdeviceptr at = reinterpret_cast<CUdeviceptr>(p);
+        for (auto& m : maps) {
+            api.unmap(at, m.second);
+            api.release(m.first);
+            at += m.second;
+        }
+        maps.clear();
+        api.addressFree(reinterpret_cast<CUdeviceptr>(p), reservedBytes);
+        p = nullptr;
+        cap = 0;
+        reservedBytes = mappedBytes = 0;
+    }
+    ~VBuf() { release(); }
+};
+
 inline unsigned G(uint32_t n) { return (n + 255) / 256; }
 
-// Growth factor of the neighbor-list buffers. A list outgrowing its buffer costs a free and an
-// allocation (both synchronise the device) plus a new capture of the Jacobi graph, whose nodes
-// hold the buffer addresses; a flow that compresses or spreads grows its lists by a few percent
-// per hundred steps, so the buffers grow in large steps and never shrink.
+// Growth factor of the neighbor-list buffers (VBuf: grown in place, addresses kept). A flow that
+// compresses or spreads grows its lists by a few percent per hundred steps; each growth maps
+// physical memory (a few driver calls), so the buffers grow in 25 % steps and never shrink.
 constexpr double LIST_GROWTH = 1.25;
 
 // ------------------------------------------------------------------------------ helpers

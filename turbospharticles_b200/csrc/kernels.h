@@ -132,10 +132,14 @@ struct FluidDev {
     const uint32_t* chunkScene;
     const uint32_t* sceneActive;
     double* chunkPartials;
+    // batch Jacobi loop only: the live particle count read on the device (n is then the arena
+    // capacity, a graph-captured constant; the sweeps stop at the live chunks)
+    const uint32_t* liveN;
 };
 __device__ __forceinline__ bool LaneActive(const FluidDev& f, uint32_t chunk, uint32_t lane, uint32_t i) {
     return f.chunkLen ? lane < (uint32_t)f.chunkLen[chunk] : i < f.n;
 }
+__device__ __forceinline__ uint32_t SweepCount(const FluidDev& f) { return f.liveN ? *f.liveN : f.n; }
 __device__ __forceinline__ bool ChunkSkipped(const FluidDev& f, uint32_t chunk) {
     return f.sceneActive != nullptr && f.sceneActive[f.chunkScene[chunk]] == 0u;
 }

@@ -39,6 +39,12 @@ constexpr uint32_t SPH_THREADS = 256;
 #ifndef TSP_JACOBI_FF_SLOTS
 #define TSP_JACOBI_FF_SLOTS 2
 #endif
+// minimum resident blocks per SM of the pressure-acceleration sweep; measured on the 1M dam
+// (ms per launch, 3 / 4 / 5 / 6 blocks): 0.129 / 0.130 / 0.122 / 0.121, while the other sweeps
+// are fastest at 4 (KJacobi 0.159 / 0.150 / 0.160 / 0.181)
+#ifndef TSP_PACC_MIN_BLOCKS
+#define TSP_PACC_MIN_BLOCKS 5
+#endif
 
 struct ChunkCursor {
     uint32_t pitch, cnt, base, base2;
@@ -358,9 +364,9 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagIn
 }
 
 // ----------------------------------------------------------------------------- pressure acceleration
-__global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+__global__ void __launch_bounds__(SPH_THREADS, TSP_PACC_MIN_BLOCKS) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
-    FOR_EACH_CHUNK_PF(f.n, nv, true) {
+    FOR_EACH_CHUNK_PF(SweepCount(f), nv, true) {
         if (ChunkSkipped(f, chunk)) continue;  // converged scene of a batch
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = LaneActive(f, chunk, lane, i);
@@ -398,7 +404,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KJacobi(Const
                                                     SolverControl ctl, SolverState* st, double* partials,
                                                     cudaGraphConditionalHandle cond, int hasCond) {
     double eRaw = 0.0, ePos = 0.0, eAbs = 0.0;  // per-lane FP64 sums over the warp's chunks
-    FOR_EACH_CHUNK_PF(f.n, nv, true) {
+    FOR_EACH_CHUNK_PF(SweepCount(f), nv, true) {
         if (ChunkSkipped(f, chunk)) continue;  // converged scene of a batch
         double cRaw = 0.0, cPos = 0.0, cAbs = 0.0;  // this chunk's contribution of the lane
         const uint32_t i = chunk * SELL_W + lane;
