@@ -3,7 +3,9 @@ PredictRigidBodies, IntegrateRigidBodies: source/simulation/CPU/backend/cpu_back
 2009-2303; rigid force accumulations: sph_solver.cpp:1151, 1717).
 
 Body sums and body integration run in FP64 on both sides, per-particle forces in FP32;
-the only difference is the FP32 summation order of the per-particle terms. Tolerances:
+the differences are the FP32 summation order of the per-particle terms and the distances of
+the SPH sweeps (hardware reciprocal square root on the GPU, IEEE square root in the oracle).
+Tolerances:
 |gpu - oracle| <= rtol * (|oracle| + max|oracle|), rtol stated per quantity.
 """
 import numpy as np

@@ -95,10 +95,15 @@ __device__ __forceinline__ bool IsNeighbor(float xi, float yi, float zi, float x
     return fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz))) <= r2;
 }
 
+// Distance from its square as the reference's GPU kernels form it (sph_kernels.cu:88-97 of
+// its CUDA backend): d2 * rsqrt(max(d2, FLT_MIN)), exactly zero at the self pair; rsqrtf is the
+// hardware approximation (at most 2 ulp), not the IEEE square root of the CPU path
+__device__ __forceinline__ float DistInv(float d2) { return rsqrtf(fmaxf(d2, 1.17549435e-38f)); }
+
 // KernelWeight_CubicSpline_SIMD (simd.h:279-309): zero outside the strict support
 __device__ __forceinline__ float KernelWeight(float dx, float dy, float dz, const Consts& c) {
     const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const float dist = sqrtf(d2);
+    const float dist = d2 * DistInv(d2);
     const float q = dist * c.sizeInv;
     const float t1 = fmaxf(1.0f - q, 0.0f);
     const float t2 = fmaxf(2.0f - q, 0.0f);
@@ -108,12 +113,15 @@ __device__ __forceinline__ float KernelWeight(float dx, float dy, float dz, cons
     return (d2 < c.radSqu) ? kw : 0.0f;
 }
 
-// KernelGradientFactorNoMinDist_CubicSpline_SIMD (simd.h:374-388); gradient = factor * (dx,dy,dz)
+// KernelGradientFactorNoMinDist_CubicSpline_SIMD (simd.h:374-388); gradient = factor * (dx,dy,dz);
+// 1/dist and dist from one reciprocal square root, as the reference's GPU kernels do
+// (sph_kernels.cu:99-114 of its CUDA backend)
 __device__ __forceinline__ float GradFactor(float d2, const Consts& c) {
-    const float dist = sqrtf(d2);
+    const float distInv = DistInv(d2);
+    const float dist = d2 * distInv;
     const float inner = fmaf(c.kInnerSlope, dist, c.kInnerOffset);
     const float t2 = fmaxf(c.kTwoSize - dist, 0.0f);
-    const float outer = (t2 * t2) * (c.kOuterScale / dist);
+    const float outer = (t2 * t2) * (c.kOuterScale * distInv);
     return (dist < c.kSize) ? inner : outer;
 }
 
