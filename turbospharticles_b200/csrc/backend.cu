@@ -147,10 +147,8 @@ public:
         DBuf<uint64_t> offset;
         VBuf<uint16_t> l16;  // grow in place: list growth keeps the addresses
         VBuf<uint32_t> l32;
-        VBuf<float> kg16, kg32;  // recorded kernel-gradient factors, parallel to l16 / l32
         uint64_t n16 = 0, n32 = 0;
     } sell[3];
-    bool kgValid = false;  // the recorded factors belong to the current positions and lists
     DBuf<U64x2> sellTot;
     DBuf<unsigned long long> nbrTot;
     // count-pass rows of the fluid query ([chunk][slot][lane]); rows longer than KS_* slots make
@@ -469,13 +467,12 @@ public:
     SellMeta Meta(int k) {
         Sell& m = sell[k];
         return SellMeta{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p,
-                        (uint64_t)m.l16.cap, (uint64_t)m.l32.cap, m.kg16.p, m.kg32.p};
+                        (uint64_t)m.l16.cap, (uint64_t)m.l32.cap};
     }
     NeighborView NView() {
         auto sv = [&](int k) {
             Sell& m = sell[k];
-            return SellView{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p,
-                            m.kg16.p, m.kg32.p};
+            return SellView{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p};
         };
         return NeighborView{sv(0), sv(1), sv(2)};
     }
@@ -579,7 +576,6 @@ public:
             m.base.ensure(std::max<uint32_t>(nChunks, 1)); m.base2.ensure(std::max<uint32_t>(nChunks, 1));
             m.offset.ensure(std::max<uint32_t>(nChunks, 1));
             m.l16.ensure(std::max<size_t>(m.l16.cap, 16)); m.l32.ensure(std::max<size_t>(m.l32.cap, 16));
-            m.kg16.ensure(m.l16.cap); m.kg32.ensure(m.l32.cap);
             cntR[k].ensure(std::max<uint32_t>(nR, 1)); offR[k].ensure(nR + 1ull);
             listR[k].ensure(std::max<size_t>(listR[k].cap, 16));
         }
@@ -662,8 +658,6 @@ public:
             sell[k].n32 = hm->sellTot[k].b;
             sell[k].l16.grow(sell[k].n16, LIST_GROWTH);
             sell[k].l32.grow(sell[k].n32, LIST_GROWTH);
-            sell[k].kg16.ensure(sell[k].l16.cap);
-            sell[k].kg32.ensure(sell[k].l32.cap);
             csrN[k] = hm->csrTot[k];
             listR[k].grow(csrN[k], LIST_GROWTH);
         }
@@ -672,7 +666,6 @@ public:
         LaunchQueryFluid(true, qa, m0, m1, m2, s);
         LaunchQueryRigid(true, qa, rl, s);
         CK(cudaEventRecord(pev[5], s));
-        kgValid = false;
         launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + (nF ? 9u : 0u) + (nR ? 9u : 0u);
         listsValid = true;
     }
@@ -708,7 +701,7 @@ public:
         P(r.pos); P(r.vel); P(r.velPred); k.push_back(r.n);
         for (const SellView* v : {&nv.ff, &nv.fb, &nv.fr}) {
             P(v->counts); P(v->pitch); P(v->format); P(v->base); P(v->base2); P(v->offset);
-            P(v->list16); P(v->list32); P(v->kg16); P(v->kg32);
+            P(v->list16); P(v->list32);
         }
         static_assert(sizeof(Consts) % 4 == 0, "Consts holds 4-byte fields only");
         const uint32_t* cw = reinterpret_cast<const uint32_t*>(&c);
@@ -1003,7 +996,6 @@ public:
         }
         CK(cudaEventRecord(pev[7], s));
         LaunchSourceDiagInit(c, f, b, r, nv, st.p, s);
-        kgValid = true;
         CK(cudaEventRecord(ev[2], s));
         CK(cudaEventRecord(pev[8], s));
         if (nF) {
@@ -1022,7 +1014,6 @@ public:
         }
         CK(cudaEventRecord(pev[10], s));
         LaunchIntegration(c, f, s);
-        kgValid = false;
         if (nRB) {
             SolveRigidContacts(c, rp, bd);
             LaunchRigidPredict(bd, prm.timeStep, s);
@@ -1071,13 +1062,9 @@ public:
         switch (stage) {
             case TSP_STAGE_DENSITY: LaunchDensity(c, f, b, r, nv, s); break;
             case TSP_STAGE_NON_PRESSURE: LaunchNonPressure(c, f, b, r, nv, s); break;
-            case TSP_STAGE_SOURCE_DIAG_INIT: LaunchSourceDiagInit(c, f, b, r, nv, st.p, s); kgValid = true; break;
-            case TSP_STAGE_PRESSURE_ACC:
-                if (!kgValid) { LaunchGradFactors(c, f, b, r, nv, s); kgValid = true; }
-                LaunchPressureAcc(c, f, b, r, nv, s);
-                break;
+            case TSP_STAGE_SOURCE_DIAG_INIT: LaunchSourceDiagInit(c, f, b, r, nv, st.p, s); break;
+            case TSP_STAGE_PRESSURE_ACC: LaunchPressureAcc(c, f, b, r, nv, s); break;
             case TSP_STAGE_JACOBI_UPDATE: {
-                if (!kgValid) { LaunchGradFactors(c, f, b, r, nv, s); kgValid = true; }
                 partials.ensure(3ull * JacobiBlocks(nF) + 3);
                 LaunchJacobi(c, f, b, r, nv, Control(), st.p, partials.p, 0ull, false, s);
                 CK(cudaMemcpyAsync(&hm->st, st.p, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
@@ -1085,8 +1072,8 @@ public:
                 if (errSums) for (int k = 0; k < 3; k++) errSums[k] = hm->st.sums[k];
                 break;
             }
-            case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); kgValid = false; break;
-            case TSP_STAGE_BOUNDARY_VOLUMES: BoundaryVolumes(c); kgValid = false; break;
+            case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); break;
+            case TSP_STAGE_BOUNDARY_VOLUMES: BoundaryVolumes(c); break;
             default: throw Error(TSP_ERR_INVALID, "unknown stage");
         }
         CheckErrors();
@@ -1102,10 +1089,6 @@ public:
         FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
         partials.ensure(3ull * JacobiBlocks(nF) + 3);
         const SolverControl ctl = Control();
-        if (!kgValid && (stage == TSP_STAGE_PRESSURE_ACC || stage == TSP_STAGE_JACOBI_UPDATE)) {
-            LaunchGradFactors(c, f, b, r, nv, s);
-            kgValid = true;
-        }
         Sync();
         CK(cudaEventRecord(ev[0], s));
         for (uint32_t k = 0; k < reps; k++) {
@@ -1276,7 +1259,6 @@ public:
             for (uint32_t i = 0; i < cnt; i++) { h[i].x = x[3 * i]; h[i].y = x[3 * i + 1]; h[i].z = x[3 * i + 2]; }
             if (cnt) CK(cudaMemcpy(dst.p, h.data(), cnt * 16ull, cudaMemcpyHostToDevice));
         };
-        if (field == TSP_FIELD_POS || field == TSP_FIELD_PSI_B) kgValid = false;
         switch (field) {
             case TSP_FIELD_POS: set3(posP, nF); break;
             case TSP_FIELD_VEL: set3(velRho, nF); break;

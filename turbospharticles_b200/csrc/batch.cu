@@ -280,7 +280,7 @@ public:
 // particle, boundary arena + cell table per boundary particle, dense grids of its frame)
 uint64_t BatchSceneBytes(uint64_t nFpad, uint64_t nB, uint64_t gridCells) {
     const uint64_t perF = 120 /* arena + reorder buffers */ + 48 /* keys, cell IDs, tables */ +
-                          3 * 2 /* counts */ + 4 * 64 /* FF + FB + FR slices and gradient factors (est.) */ +
+                          3 * 2 /* counts */ + 4 * 64 /* FF + FB + FR slices, grown by 1.5x (est.) */ +
                           4 * (64 + 48) /* query row scratch */ + 24 /* Jacobi partials, meta */;
     const uint64_t perB = 16 + 4 + 8 + 8 + 4 + 16 /* arena, table, sort scratch */;
     return nFpad * perF + nB * perB + gridCells * 8;
@@ -370,7 +370,6 @@ public:
         DBuf<uint64_t> offset;
         VBuf<uint16_t> l16;  // grow in place: list growth keeps the addresses
         VBuf<uint32_t> l32;
-        VBuf<float> kg16, kg32;
         uint64_t n16 = 0, n32 = 0;
     } sell[3];
     DBuf<uint32_t> scrF, scrB, scrR;
@@ -701,7 +700,6 @@ public:
             m.counts.ensure(n); m.pitch.ensure(nc); m.format.ensure(nc); m.base.ensure(nc); m.base2.ensure(nc);
             m.offset.ensure(nc);
             m.l16.ensure(std::max<size_t>(m.l16.cap, 16)); m.l32.ensure(std::max<size_t>(m.l32.cap, 16));
-            m.kg16.ensure(m.l16.cap); m.kg32.ensure(m.l32.cap);
         }
         scrF.ensure(QueryScratchWords(nc, KS_F));
         scrB.ensure(QueryScratchWords(nc, KS_B));
@@ -817,12 +815,11 @@ public:
     SellMeta Meta(int k) {
         Sell& m = sell[k];
         return SellMeta{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p,
-                        (uint64_t)m.l16.cap, (uint64_t)m.l32.cap, m.kg16.p, m.kg32.p};
+                        (uint64_t)m.l16.cap, (uint64_t)m.l32.cap};
     }
     SellView View(int k) {
         Sell& m = sell[k];
-        return SellView{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p,
-                        m.kg16.p, m.kg32.p};
+        return SellView{m.counts.p, m.pitch.p, m.format.p, m.base.p, m.base2.p, m.offset.p, m.l16.p, m.l32.p};
     }
     // masked: the Jacobi-loop view (n = the arena capacity, the live count read on the device,
     // converged scenes masked out)
@@ -854,7 +851,6 @@ public:
         for (int s2 = 0; s2 < 3; s2++) {
             const SellView v = View(s2);
             P(v.counts); P(v.pitch); P(v.format); P(v.base); P(v.base2); P(v.offset); P(v.list16); P(v.list32);
-            P(v.kg16); P(v.kg32);
         }
         const uint32_t* cw = reinterpret_cast<const uint32_t*>(&c);
         for (size_t i = 0; i < sizeof(Consts) / 4; i++) k.push_back(cw[i]);
@@ -997,7 +993,6 @@ public:
         for (int k = 0; k < 3; k++) {
             sell[k].n16 = tot[k].a; sell[k].n32 = tot[k].b;
             sell[k].l16.grow(tot[k].a, BATCH_LIST_GROWTH); sell[k].l32.grow(tot[k].b, BATCH_LIST_GROWTH);
-            sell[k].kg16.ensure(sell[k].l16.cap); sell[k].kg32.ensure(sell[k].l32.cap);
         }
         LaunchQueryFluid(true, qa, Meta(0), Meta(1), Meta(2), s);
         launches += 2 + 9;

@@ -166,8 +166,6 @@ struct SellMeta {
     uint16_t* list16;
     uint32_t* list32;
     uint64_t cap16, cap32;
-    float* kg16;        // kernel-gradient factor per slot, parallel to list16 / list32
-    float* kg32;
 };
 
 // neighbor j of (chunk meta, slot k, lane); decode of StoreNeighbor_CompressedSell32

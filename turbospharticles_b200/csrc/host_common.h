@@ -92,9 +92,9 @@ struct VmmApi {
         if (e_ != CUDA_SUCCESS) throw Error(TSP_ERR_CUDA, std::string(#x) + ": driver error " + std::to_string((int)e_)); \
     } while (0)
 
-// Device buffer that grows in place: a virtual address range (8x the first request) is
-// reserved once and physical memory is mapped onto the end of the used part as the buffer
-// grows. The address does not change (graphs captured with it stay valid) and a growth costs
+// Device buffer that grows in place: a virtual address range (8x the first request, at least
+// 64 MB) is reserved once and physical memory (at least 32 MB) is mapped onto the end of the
+// used part as the buffer grows. The address does not change (graphs captured with it stay valid) and a growth costs
 // neither a copy, a free nor a device-wide synchronisation; only a request beyond the
 // reservation re-reserves (new address, contents not kept, like DBuf::ensure).
 template <typename T>
@@ -122,7 +122,8 @@ struct VBuf {
         const CUmemAllocationProp prop = Prop();
         size_t gran = 0;
         CKD(api.granularity(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED));
-        const size_t need = (bytes + gran - 1) / gran * gran;
+        // at least 32 MB backed: small lists (boundary, 32-bit entries) then never grow in a run
+        const size_t need = (std::max<size_t>(bytes, size_t(32) << 20) + gran - 1) / gran * gran;
         if (!p || need > reservedBytes) {
             release();
             const size_t want = std::max<size_t>(need * 8, size_t(64) << 20);
@@ -174,8 +175,9 @@ inline unsigned G(uint32_t n) { return (n + 255) / 256; }
 
 // Growth factor of the neighbor-list buffers (VBuf: grown in place, addresses kept). A flow that
 // compresses or spreads grows its lists by a few percent per hundred steps; each growth maps
-// physical memory (a few driver calls), so the buffers grow in 25 % steps and never shrink.
-constexpr double LIST_GROWTH = 1.25;
+// physical memory (a few driver calls, 0.3-0.6 ms measured, but steps with a growth have also
+// shown 5-10 ms outliers), so the buffers grow in 50 % steps and never shrink.
+constexpr double LIST_GROWTH = 1.5;
 
 // ------------------------------------------------------------------------------ helpers
 inline int HostFloorToInt(float v) {

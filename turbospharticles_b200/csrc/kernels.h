@@ -163,8 +163,6 @@ struct SellView {
     const uint64_t* offset;
     const uint16_t* list16;
     const uint32_t* list32;
-    float* kg16;   // per-slot kernel-gradient factors of the current positions, written by the
-    float* kg32;   // source/diagonal stage and read by the pressure-acceleration / Jacobi sweeps
 };
 struct NeighborView {
     SellView ff, fb, fr;
@@ -216,10 +214,6 @@ void LaunchBoundaryVolumes(const Consts& c, const float4* posB, uint32_t nB, con
                            const uint32_t* gridB, const Frame& fr, float defaultVol, float defaultPsi, float restDensity,
                            float* volOut, float* psiOut, cudaStream_t s);
 void LaunchSolverReset(SolverState* st, uint32_t nF, cudaStream_t s);
-// per-slot kernel-gradient factors for the current positions (same values the source /
-// diagonal stage records), for stage-level use after positions were rewritten
-void LaunchGradFactors(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
-                       const NeighborView& nv, cudaStream_t s);
 
 // ---- rigid_kernels.cu
 struct BodyDev {

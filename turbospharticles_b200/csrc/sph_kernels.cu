@@ -26,13 +26,14 @@ constexpr uint32_t SPH_THREADS = 256;
 #ifndef TSP_SPH_PERSISTENT
 #define TSP_SPH_PERSISTENT 1
 #endif
-// 1: the list entries and gradient factors of the next slot group are loaded before the
-// gathers of the current group (one group of loads always in flight)
+// 1: the list entries of the next slot group are loaded before the gathers of the current group
+// (one group of loads always in flight)
 #ifndef TSP_SPH_PIPELINE
 #define TSP_SPH_PIPELINE 1
 #endif
-// FF slots per group of the gradient-factor sweeps (pressure acceleration, Jacobi); measured on
-// the 1M dam: pipelined 3 / 2 slots beat 4 / 4 by 20 % / 9 %
+// FF slots per group of the pressure sweeps (pressure acceleration, Jacobi); measured on the 1M
+// dam with the kernel-gradient factor computed per pair: 3 / 2 slots (0.109 / 0.146 ms per
+// launch) against 2 / 2 (0.110 / 0.146) and 4 / 4 (0.116 / 0.158)
 #ifndef TSP_PACC_FF_SLOTS
 #define TSP_PACC_FF_SLOTS 3
 #endif
@@ -58,24 +59,18 @@ struct ChunkCursor {
     __device__ __forceinline__ uint32_t nbr(const SellView& v, uint32_t k, uint32_t lane) const {
         return SellNeighbor(fmt, base, base2, off, k, lane, v.list16, v.list32);
     }
-    // recorded kernel-gradient factor of slot k (same index as the list entry)
-    __device__ __forceinline__ float* kgSlot(const SellView& v, uint32_t k, uint32_t lane) const {
-        return (fmt == FMT_DELTA16X2 ? v.kg16 : v.kg32) + off + (uint64_t)k * SELL_W + lane;
-    }
 };
 
-// Visits the slots of a lane in order, U slots at a time: the U list entries (and, with KG,
-// the U recorded kernel-gradient factors) are loaded together, then the U neighbor gathers (one
-// or two float4 each), then the U pair terms are applied in slot order. The sum order is
-// unchanged; the loads of a group are independent, so up to 3U (4U) memory requests per lane
-// are in flight. The chunk's format is resolved once per chunk (D16: Delta16x2, else Abs32),
-// not per slot.
-template <int U, bool TWO, bool KG, bool D16, typename Body>
+// Visits the slots of a lane in order, U slots at a time: the U list entries are loaded
+// together, then the U neighbor gathers (one or two float4 each), then the U pair terms are
+// applied in slot order. The sum order is unchanged; the loads of a group are independent, so
+// up to 3U memory requests per lane are in flight. The chunk's format is resolved once per
+// chunk (D16: Delta16x2, else Abs32), not per slot.
+template <int U, bool TWO, bool D16, typename Body>
 __device__ __forceinline__ void SweepFmt(const ChunkCursor& cur, const SellView& v, uint32_t lane,
                                          const float4* A, const float4* B, Body&& body) {
     for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
         uint32_t j[U];
-        float kg[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const bool ok = k0 + u < cur.cnt;
@@ -86,7 +81,6 @@ __device__ __forceinline__ void SweepFmt(const ChunkCursor& cur, const SellView&
             } else {
                 j[u] = ok ? v.list32[lin] : EMPTY_32;
             }
-            if constexpr (KG) kg[u] = ok ? (D16 ? v.kg16 : v.kg32)[lin] : 0.0f;
         }
         float4 a[U], b[U];
 #pragma unroll
@@ -101,19 +95,17 @@ __device__ __forceinline__ void SweepFmt(const ChunkCursor& cur, const SellView&
 #pragma unroll
         for (int u = 0; u < U; u++) {
             if (j[u] == EMPTY_32) continue;
-            if constexpr (KG) body(kg[u], a[u], b[u]);
-            else body(k0 + u, j[u], a[u], b[u]);
+            body(k0 + u, j[u], a[u], b[u]);
         }
     }
 }
 #if TSP_SPH_PIPELINE
-// pipelined: the list entries (and factors) of group g + 1 are loaded before the gathers of
-// group g, so one group of stream loads is always in flight; same slots, same order
-template <int U, bool TWO, bool KG, bool D16, typename Body>
+// pipelined: the list entries of group g + 1 are loaded before the gathers of group g, so one
+// group of stream loads is always in flight; same slots, same order
+template <int U, bool TWO, bool D16, typename Body>
 __device__ __forceinline__ void SweepFmtPipe(const ChunkCursor& cur, const SellView& v, uint32_t lane,
                                              const float4* A, const float4* B, Body&& body) {
     uint32_t jn[U];
-    float kn[U];
     auto fetch = [&](uint32_t k0) {
 #pragma unroll
         for (int u = 0; u < U; u++) {
@@ -125,15 +117,13 @@ __device__ __forceinline__ void SweepFmtPipe(const ChunkCursor& cur, const SellV
             } else {
                 jn[u] = ok ? v.list32[lin] : EMPTY_32;
             }
-            if constexpr (KG) kn[u] = ok ? (D16 ? v.kg16 : v.kg32)[lin] : 0.0f;
         }
     };
     fetch(0);
     for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
         uint32_t j[U];
-        float kg[U];
 #pragma unroll
-        for (int u = 0; u < U; u++) { j[u] = jn[u]; kg[u] = KG ? kn[u] : 0.0f; }
+        for (int u = 0; u < U; u++) j[u] = jn[u];
         fetch(k0 + U);
         float4 a[U], b[U];
 #pragma unroll
@@ -148,8 +138,7 @@ __device__ __forceinline__ void SweepFmtPipe(const ChunkCursor& cur, const SellV
 #pragma unroll
         for (int u = 0; u < U; u++) {
             if (j[u] == EMPTY_32) continue;
-            if constexpr (KG) body(kg[u], a[u], b[u]);
-            else body(k0 + u, j[u], a[u], b[u]);
+            body(k0 + u, j[u], a[u], b[u]);
         }
     }
 }
@@ -160,15 +149,19 @@ __device__ __forceinline__ void SweepFmtPipe(const ChunkCursor& cur, const SellV
 template <int U, bool TWO, typename Body>
 __device__ __forceinline__ void SweepSlots(const ChunkCursor& cur, const SellView& v, uint32_t lane,
                                            const float4* A, const float4* B, Body&& body) {
-    if (cur.fmt == FMT_DELTA16X2) TSP_SWEEP_IMPL<U, TWO, false, true>(cur, v, lane, A, B, body);
-    else TSP_SWEEP_IMPL<U, TWO, false, false>(cur, v, lane, A, B, body);
+    if (cur.fmt == FMT_DELTA16X2) TSP_SWEEP_IMPL<U, TWO, true>(cur, v, lane, A, B, body);
+    else TSP_SWEEP_IMPL<U, TWO, false>(cur, v, lane, A, B, body);
 }
-// as SweepSlots, also loading each slot's recorded kernel-gradient factor (no sqrt / division)
+// as SweepSlots, handing the body the pair's kernel-gradient factor, computed from the gathered
+// position (A holds positions) with one reciprocal square root
 template <int U, bool TWO, typename Body>
-__device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellView& v, uint32_t lane,
-                                             const float4* A, const float4* B, Body&& body) {
-    if (cur.fmt == FMT_DELTA16X2) TSP_SWEEP_IMPL<U, TWO, true, true>(cur, v, lane, A, B, body);
-    else TSP_SWEEP_IMPL<U, TWO, true, false>(cur, v, lane, A, B, body);
+__device__ __forceinline__ void SweepSlotsGrad(const ChunkCursor& cur, const SellView& v, uint32_t lane,
+                                               const float4& pi, const Consts& c, const float4* A, const float4* B,
+                                               Body&& body) {
+    SweepSlots<U, TWO>(cur, v, lane, A, B, [&](uint32_t, uint32_t, const float4& a, const float4& b) {
+        const float dx = pi.x - a.x, dy = pi.y - a.y, dz = pi.z - a.z;
+        body(GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c), a, b);
+    });
 }
 
 // persistent warps: warp w of the grid handles chunks w, w + W, w + 2W, ...
@@ -181,9 +174,9 @@ __device__ __forceinline__ void SweepSlotsKg(const ChunkCursor& cur, const SellV
 // L2 prefetch of the SELL32 slices a warp sweeps next. A chunk's slice of each category is
 // contiguous (pitch * 32 entries from its offset, a multiple of 32 entries, so the start is
 // 64-byte aligned and the size a multiple of 64 bytes), so one bulk prefetch per slice pulls it
-// into L2 while the warp still works on its current chunk. Lanes 0-5 each own one slice
-// (FF/FB/FR list, FF/FB/FR recorded gradient factors); the slice meta of chunk c + 2W is loaded
-// while chunk c is processed and the prefetch of c + W is issued at the start of chunk c.
+// into L2 while the warp still works on its current chunk. Lanes 0-2 each own one slice (FF,
+// FB, FR list); the slice meta of chunk c + 2W is loaded while chunk c is processed and the
+// prefetch of c + W is issued at the start of chunk c.
 __device__ __forceinline__ void L2PrefetchBulk(const void* p, uint32_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
@@ -191,29 +184,24 @@ struct SlicePrefetch {
     uint32_t pitch, fmt;
     uint64_t off;
     __device__ __forceinline__ const SellView& view(const NeighborView& nv, uint32_t lane) const {
-        return lane < 2 ? nv.ff : (lane < 4 ? nv.fb : nv.fr);
+        return lane == 0 ? nv.ff : (lane == 1 ? nv.fb : nv.fr);
     }
     __device__ __forceinline__ void load(const NeighborView& nv, uint32_t chunk, uint32_t nChunks, uint32_t lane) {
         pitch = 0; fmt = 0; off = 0;
-        if (lane < 6 && chunk < nChunks) {
+        if (lane < 3 && chunk < nChunks) {
             const SellView& v = view(nv, lane);
             pitch = v.pitch[chunk]; fmt = v.format[chunk]; off = v.offset[chunk];
         }
     }
-    __device__ __forceinline__ void issue(const NeighborView& nv, uint32_t lane, bool kg) const {
+    __device__ __forceinline__ void issue(const NeighborView& nv, uint32_t lane) const {
         if (pitch == 0) return;
         const SellView& v = view(nv, lane);
         const uint32_t n = pitch * SELL_W;
-        const bool d16 = fmt == FMT_DELTA16X2;
-        if ((lane & 1u) == 0u) {
-            if (d16) L2PrefetchBulk(v.list16 + off, n * 2u);
-            else L2PrefetchBulk(v.list32 + off, n * 4u);
-        } else if (kg) {
-            L2PrefetchBulk((d16 ? v.kg16 : v.kg32) + off, n * 4u);
-        }
+        if (fmt == FMT_DELTA16X2) L2PrefetchBulk(v.list16 + off, n * 2u);
+        else L2PrefetchBulk(v.list32 + off, n * 4u);
     }
 };
-#define FOR_EACH_CHUNK_PF(n, nv, KG)                                                            \
+#define FOR_EACH_CHUNK_PF(n, nv)                                                                \
     const uint32_t lane = threadIdx.x & 31;                                                     \
     const uint32_t nChunks_ = ((n) + SELL_W - 1) / SELL_W;                                      \
     const uint32_t warps_ = (gridDim.x * blockDim.x) >> 5;                                      \
@@ -221,11 +209,11 @@ struct SlicePrefetch {
     pf_.load(nv, ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) + warps_, nChunks_, lane);       \
     for (uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; chunk < nChunks_;       \
          chunk += warps_)                                                                       \
-        if (pf_.issue(nv, lane, KG), pf_.load(nv, chunk + 2u * warps_, nChunks_, lane), true)
+        if (pf_.issue(nv, lane), pf_.load(nv, chunk + 2u * warps_, nChunks_, lane), true)
 
 // ----------------------------------------------------------------------------- density
 __global__ void __launch_bounds__(SPH_THREADS) KDensity(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv) {
-    FOR_EACH_CHUNK_PF(f.n, nv, false) {
+    FOR_EACH_CHUNK_PF(f.n, nv) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = LaneActive(f, chunk, lane, i);
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -250,7 +238,7 @@ __global__ void __launch_bounds__(SPH_THREADS) KDensity(Consts c, FluidDev f, Bo
 // ----------------------------------------------------------------------------- non-pressure
 __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
-    FOR_EACH_CHUNK_PF(f.n, nv, false) {
+    FOR_EACH_CHUNK_PF(f.n, nv) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = LaneActive(f, chunk, lane, i);
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -301,7 +289,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KNonPressure(
 // ----------------------------------------------------------------------------- source / diagonal / init
 __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagInit(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                             NeighborView nv) {
-    FOR_EACH_CHUNK_PF(f.n, nv, false) {
+    FOR_EACH_CHUNK_PF(f.n, nv) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = LaneActive(f, chunk, lane, i);
         const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -315,7 +303,6 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagIn
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float kg = GradFactor(d2, c);
-            *cur.kgSlot(nv.ff, k, lane) = kg;
             const float st = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
             sF = fmaf(kg, st, sF);
             cxF = fmaf(kg, dx, cxF); cyF = fmaf(kg, dy, cyF); czF = fmaf(kg, dz, czF);
@@ -325,7 +312,6 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagIn
         SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
-            *cur.kgSlot(nv.fb, k, lane) = kg;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float dvx = vi.x - 0.0f, dvy = vi.y - 0.0f, dvz = vi.z - 0.0f;
             const float st = fmaf(dvx, gx, fmaf(dvy, gy, dvz * gz));
@@ -336,7 +322,6 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagIn
         SweepSlots<2, true>(cur, nv.fr, lane, r.pos, r.velPred, [&](uint32_t k, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
-            *cur.kgSlot(nv.fr, k, lane) = kg;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float st = fmaf(dvx, gx, fmaf(dvy, gy, dvz * gz));
@@ -366,7 +351,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagIn
 // ----------------------------------------------------------------------------- pressure acceleration
 __global__ void __launch_bounds__(SPH_THREADS, TSP_PACC_MIN_BLOCKS) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
-    FOR_EACH_CHUNK_PF(SweepCount(f), nv, true) {
+    FOR_EACH_CHUNK_PF(SweepCount(f), nv) {
         if (ChunkSkipped(f, chunk)) continue;  // converged scene of a batch
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = LaneActive(f, chunk, lane, i);
@@ -375,20 +360,20 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_PACC_MIN_BLOCKS) KPressureAcc
         float ax = 0.f, ay = 0.f, az = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsKg<TSP_PACC_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<TSP_PACC_FF_SLOTS, false>(cur, nv.ff, lane, pi, c, f.posP, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float a = (fOuter + c.massF * pj.w * c.densInvSqu) * kg;
             ax = fmaf(a, dx, ax); ay = fmaf(a, dy, ay); az = fmaf(a, dz, az);
         });
         cur.load(nv.fb, chunk, i, act);
-        SweepSlotsKg<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<2, false>(cur, nv.fb, lane, pi, c, b.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float a = c.accCoeffB * pj.w * pi.w;
             ax = fmaf(a, gx, ax); ay = fmaf(a, gy, ay); az = fmaf(a, gz, az);
         });
         cur.load(nv.fr, chunk, i, act);
-        SweepSlotsKg<2, false>(cur, nv.fr, lane, r.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<2, false>(cur, nv.fr, lane, pi, c, r.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float a = c.accCoeffB * pj.w * pi.w;
@@ -404,7 +389,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KJacobi(Const
                                                     SolverControl ctl, SolverState* st, double* partials,
                                                     cudaGraphConditionalHandle cond, int hasCond) {
     double eRaw = 0.0, ePos = 0.0, eAbs = 0.0;  // per-lane FP64 sums over the warp's chunks
-    FOR_EACH_CHUNK_PF(SweepCount(f), nv, true) {
+    FOR_EACH_CHUNK_PF(SweepCount(f), nv) {
         if (ChunkSkipped(f, chunk)) continue;  // converged scene of a batch
         double cRaw = 0.0, cPos = 0.0, cAbs = 0.0;  // this chunk's contribution of the lane
         const uint32_t i = chunk * SELL_W + lane;
@@ -414,7 +399,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KJacobi(Const
         float sF = 0.f, sB = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsKg<TSP_JACOBI_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.acc, [&](float kg, const float4& pj, const float4& aj) {
+        SweepSlotsGrad<TSP_JACOBI_FF_SLOTS, true>(cur, nv.ff, lane, pi, c, f.posP, f.acc, [&](float kg, const float4& pj, const float4& aj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
             const float sv = fmaf(dax, dx, fmaf(day, dy, daz * dz));
@@ -422,14 +407,14 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KJacobi(Const
         });
         sF *= c.massF;
         cur.load(nv.fb, chunk, i, act);
-        SweepSlotsKg<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<2, false>(cur, nv.fb, lane, pi, c, b.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
             sB = sB + pj.w * sv;
         });
         cur.load(nv.fr, chunk, i, act);
-        SweepSlotsKg<2, false>(cur, nv.fr, lane, r.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<2, false>(cur, nv.fr, lane, pi, c, r.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
@@ -533,33 +518,6 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KJacobi(Const
     if (hasCond) cudaGraphSetConditional(cond, done ? 0u : 1u);
 }
 
-// records the per-slot kernel-gradient factors of the current positions (the values the
-// source / diagonal stage records), for stage-level runs after positions were rewritten
-__global__ void __launch_bounds__(SPH_THREADS) KGradFactors(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
-                                                         NeighborView nv) {
-    FOR_EACH_CHUNK(f.n) {
-        const uint32_t i = chunk * SELL_W + lane;
-        const bool act = LaneActive(f, chunk, lane, i);
-        const float4 pi = act ? f.posP[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        ChunkCursor cur;
-        cur.load(nv.ff, chunk, i, act);
-        SweepSlots<TSP_SPH_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
-            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            *cur.kgSlot(nv.ff, k, lane) = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
-        });
-        cur.load(nv.fb, chunk, i, act);
-        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
-            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            *cur.kgSlot(nv.fb, k, lane) = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
-        });
-        cur.load(nv.fr, chunk, i, act);
-        SweepSlots<2, false>(cur, nv.fr, lane, r.pos, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
-            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-            *cur.kgSlot(nv.fr, k, lane) = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
-        });
-    }
-}
-
 __global__ void KSolverReset(SolverState* st, uint32_t nF) {
     st->iters = nF > 0 ? 1u : 0u;
     st->avg[0] = st->avg[1] = st->avg[2] = 0.0f;
@@ -659,10 +617,6 @@ void LaunchSourceDiagInit(const Consts& c, const FluidDev& f, const BoundaryDev&
     if (st) KSolverReset<<<1, 1, 0, s>>>(st, f.n);
 }
 void LaunchSolverReset(SolverState* st, uint32_t nF, cudaStream_t s) { KSolverReset<<<1, 1, 0, s>>>(st, nF); }
-void LaunchGradFactors(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
-                       const NeighborView& nv, cudaStream_t s) {
-    if (f.n) KGradFactors<<<PersistentBlocks(KGradFactors, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
-}
 void LaunchPressureAcc(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
                        const NeighborView& nv, cudaStream_t s) {
     if (f.n) KPressureAcc<<<PersistentBlocks(KPressureAcc, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
