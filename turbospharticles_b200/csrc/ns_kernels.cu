@@ -395,13 +395,15 @@ __device__ __forceinline__ QueryLaneInfo QuerySetup(const QueryArgs& a, uint32_t
     return q;
 }
 
-// stencil ranges of groups [g0, g0 + nb) of species SP, ranked by first index
-template <int SP>
+// stencil ranges of groups [g0, g0 + nb) of species SP, ranked by first index; RC is the
+// frame's reach when known at compile time (1: cell size = kernel radius, the usual frame,
+// where the stencil index arithmetic becomes constant multiplies), 0 to read it from the frame
+template <int SP, int RC>
 __device__ __forceinline__ void QueryRanges(const QueryArgs& a, const QueryScene& sc, const QueryWarp& w, uint32_t g0,
                                             uint32_t nb, uint32_t lane) {
     const uint32_t* grid = SP == 0 ? sc.gridF : SP == 1 ? sc.gridB : sc.gridR;
     const uint32_t* start = SP == 0 ? a.startF : SP == 1 ? a.startB : a.startR;
-    const int r = (int)sc.fr.reach, D = 2 * r + 1;
+    const int r = RC ? RC : (int)sc.fr.reach, D = 2 * r + 1;
     const uint32_t sv = (uint32_t)(D * D * D), total = nb * sv;
     if (lane < nb) w.nne[lane] = 0;
     __syncwarp();
@@ -533,7 +535,8 @@ __device__ __forceinline__ void QuerySpecies(const QueryArgs& a, const QueryScen
     const uint32_t gb = QueryGroupsPerBatch(sc.fr.reach);
     for (uint32_t g0 = 0; g0 < q.nGroups; g0 += gb) {
         const uint32_t nb = min(gb, q.nGroups - g0);
-        QueryRanges<SP>(a, sc, w, g0, nb, lane);
+        if (sc.fr.reach == 1) QueryRanges<SP, 1>(a, sc, w, g0, nb, lane);
+        else QueryRanges<SP, 0>(a, sc, w, g0, nb, lane);
         if constexpr (MODE == WALK_COUNT && SP != 2)
             QueryWalkCountU<SP>(a, sc, w, q, g0, nb, ref, scr, ks);
         else

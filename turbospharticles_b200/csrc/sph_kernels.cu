@@ -40,11 +40,14 @@ constexpr uint32_t SPH_THREADS = 256;
 #ifndef TSP_JACOBI_FF_SLOTS
 #define TSP_JACOBI_FF_SLOTS 2
 #endif
-// minimum resident blocks per SM of the pressure-acceleration sweep; measured on the 1M dam
-// (ms per launch, 3 / 4 / 5 / 6 blocks): 0.129 / 0.130 / 0.122 / 0.121, while the other sweeps
-// are fastest at 4 (KJacobi 0.159 / 0.150 / 0.160 / 0.181)
+// minimum resident blocks per SM of the pressure sweeps; measured on the 1M dam with the
+// gradient factor computed per pair (ms per launch): KPressureAcc 4 / 5 / 6 blocks 0.120 /
+// 0.110 / 0.105 (40 registers at 6), KJacobi 3 / 4 / 5 / 6 blocks 0.148 / 0.147 / 0.153 / 0.16
 #ifndef TSP_PACC_MIN_BLOCKS
-#define TSP_PACC_MIN_BLOCKS 5
+#define TSP_PACC_MIN_BLOCKS 6
+#endif
+#ifndef TSP_JACOBI_MIN_BLOCKS
+#define TSP_JACOBI_MIN_BLOCKS 4
 #endif
 
 struct ChunkCursor {
@@ -385,7 +388,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_PACC_MIN_BLOCKS) KPressureAcc
 
 // ----------------------------------------------------------------------------- relaxed Jacobi sweep
 
-__global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KJacobi(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv,
+__global__ void __launch_bounds__(SPH_THREADS, TSP_JACOBI_MIN_BLOCKS) KJacobi(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv,
                                                     SolverControl ctl, SolverState* st, double* partials,
                                                     cudaGraphConditionalHandle cond, int hasCond) {
     double eRaw = 0.0, ePos = 0.0, eAbs = 0.0;  // per-lane FP64 sums over the warp's chunks
