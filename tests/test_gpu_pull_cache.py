@@ -1,0 +1,76 @@
+"""Repeated pulls of the same boundary on the GPU against the oracle given the same states.
+
+The end-to-end loop pulls a state, steps, pushes and pulls the pushed state again. The backend
+keeps its sort of a boundary upload that equals the previous upload bit for bit, and then skips
+the boundary sort when the fresh frame of the next build is the same (the reference sorts the
+pulled raw order under the fresh frame every time: the same arrays). Every case pulls the same
+state into both backends and compares after the neighbor build: cell IDs, permutations, cell
+tables, rows and SELL32 words exactly, and the pushed boundary (order, IDs, positions, psi,
+volumes) bit for bit.
+- a plain pull / search / step / push loop (the kept sort is reused from the third pull on);
+- a pull of the same boundary whose fluid widens the fresh frame (the kept sort must be
+  replaced by a sort of the raw order under the new frame);
+- a pull of the same boundary after the boundary volumes were recomputed in place (the kept
+  arrays no longer hold the raw values and must be restored from the raw copy).
+"""
+import numpy as np
+import pytest
+
+from oracle import OracleBackend
+from test_gpu_parity import assert_neighbor_structures_equal
+from turbospharticles_b200 import abi, scene as S
+from turbospharticles_b200.backend import SimBackendB200
+
+pytestmark = pytest.mark.gpu
+
+BOUNDARY = ("idB", "xPosB", "yPosB", "zPosB", "psiB", "volB")
+
+
+def backends():
+    st, dmin, dmax, p = S.dam_32k()
+    g, o = SimBackendB200(p), OracleBackend(p)
+    for be in (g, o):
+        be.set_sim_domain_bounds(dmin, dmax)
+    g.pull(st, p)
+    g.run_stage(abi.STAGE_BOUNDARY_VOLUMES, p)
+    return g, o, p, g.push()
+
+
+def pull_search_compare(g, o, p, st, what):
+    for be in (g, o):
+        be.pull(st, p)
+        be.neighbor_search(p)
+    assert_neighbor_structures_equal(g, o, st.N_F, st.N_B, 0)
+    gs, os_ = g.push(), o.push()
+    for n in BOUNDARY:
+        assert np.array_equal(getattr(gs, n), getattr(os_, n)), (what, n)
+    assert np.array_equal(gs.idF, os_.idF), what
+
+
+def test_gpu_pull_step_push_loop_matches_oracle():
+    g, o, p, st = backends()
+    for k in range(5):
+        pull_search_compare(g, o, p, st, f"iteration {k}")
+        g.step(p)
+        st = g.push()
+
+
+def test_gpu_kept_boundary_sort_with_a_wider_frame():
+    g, o, p, st = backends()
+    for k in range(3):
+        pull_search_compare(g, o, p, st, f"iteration {k}")
+        g.step(p)
+        st = g.push()
+    # one fluid particle well above the tank: same boundary, wider fresh frame
+    st.yPosF[0] += 0.5
+    pull_search_compare(g, o, p, st, "wider frame")
+    g.step(p)
+    pull_search_compare(g, o, p, g.push(), "after the wider frame")
+
+
+def test_gpu_kept_boundary_sort_after_volumes_recomputed():
+    g, o, p, st = backends()
+    for k in range(3):
+        pull_search_compare(g, o, p, st, f"iteration {k}")
+    g.run_stage(abi.STAGE_BOUNDARY_VOLUMES, p)  # rewrites psi / volumes in the kept arrays
+    pull_search_compare(g, o, p, st, "after boundary volumes")

@@ -62,6 +62,17 @@ __global__ void KSetW(float4* v, const float* w, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i].w = w[i];
 }
+// bitwise equality of two boundary uploads (positions + psi, volumes, IDs); any difference sets *diff
+__global__ void KBoundaryDiff(const float4* __restrict__ a, const float* __restrict__ va, const uint64_t* __restrict__ ia,
+                              const float4* __restrict__ b, const float* __restrict__ vb, const uint64_t* __restrict__ ib,
+                              uint32_t n, uint32_t* diff) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint4 x = *reinterpret_cast<const uint4*>(a + i), y = *reinterpret_cast<const uint4*>(b + i);
+    const bool d = x.x != y.x || x.y != y.y || x.z != y.z || x.w != y.w || __float_as_uint(va[i]) != __float_as_uint(vb[i]) ||
+                   ia[i] != ib[i];
+    if (d) *diff = 1u;
+}
 __global__ void KIota(uint32_t* v, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = i;
@@ -91,6 +102,7 @@ struct HostMirror {
     ContactState contact;
     uint64_t contactTot[2];
     uint32_t exportCount;
+    uint32_t bDiff;
 };
 
 class Backend {
@@ -126,7 +138,24 @@ public:
     float cellSize = 0.0f;
     uint32_t reach = 1;
     uint32_t frameRebuilds = 0;
-    bool bSortedForFrame = false;
+    // Boundary arrays: posB/volB/idB hold the last pull's boundary in its raw (uploaded) order
+    // (B_RAW), the stable cell sort of that order under bSortFr (B_SORTED_FROM_RAW), or another
+    // order / other values (B_OTHER: sorted again after a frame change, volumes rewritten).
+    // rawPosB/rawVolB/rawIdB keep the raw upload, so a pull of the same boundary keeps a sort of
+    // it, and the first step after that pull sorts nothing when its fresh frame equals bSortFr
+    // (the reference re-sorts the raw order under the fresh frame: the same arrays).
+    enum { B_RAW = 0, B_SORTED_FROM_RAW = 1, B_OTHER = 2 };
+    int bState = B_OTHER;
+    bool bSortedValid = false;  // posB sorted, cell table and grid built, under bSortFr
+    Frame bSortFr{};
+    bool rawBValid = false;
+    uint32_t rawNB = 0;
+    bool bKeptAtPull = false;   // the last pull kept a sort of the same raw boundary (B_SORTED_FROM_RAW)
+    DBuf<uint32_t> rawPermB;    // permutation of the sort of the raw order under bSortFr
+    DBuf<float4> rawPosB;
+    DBuf<float> rawVolB;
+    DBuf<uint64_t> rawIdB;
+    DBuf<uint32_t> bDiff;
     bool bAabbValid = false;
     float bMin[3] = {0, 0, 0}, bMax[3] = {0, 0, 0};
     DBuf<uint64_t> keysA, keysB;
@@ -288,9 +317,15 @@ public:
     void Unpack4(const float4* in, uint32_t n, float* a, float* b, float* c, float* d, DBuf<float>& tmp) {
         if (n == 0) return;
         tmp.ensure(4ull * n);
+        UnpackTo(in, n, a, b, c, d, tmp.p);
+    }
+    // unpack into the 4 * n floats at dev (only the columns a host array asks for) and queue
+    // their device-to-host copies; dev must stay untouched until the stream passes the copies
+    void UnpackTo(const float4* in, uint32_t n, float* a, float* b, float* c, float* d, float* dev0) {
+        if (n == 0) return;
         float* host[4] = {a, b, c, d};
         float* dev[4];
-        for (int k = 0; k < 4; k++) dev[k] = host[k] ? tmp.p + (uint64_t)k * n : nullptr;
+        for (int k = 0; k < 4; k++) dev[k] = host[k] ? dev0 + (uint64_t)k * n : nullptr;
         KUnpack4<<<G(n), 256, 0, s>>>(in, dev[0], dev[1], dev[2], dev[3], n);
         for (int k = 0; k < 4; k++)
             if (host[k]) CK(cudaMemcpyAsync(host[k], dev[k], n * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -328,20 +363,29 @@ public:
         idF2.ensure(std::max<uint32_t>(nF, 1));
         // boundary: defaults psi = massB, vol = massB / rho0 (state_sim.h:347-362)
         const float defPsi = p.massB, defVol = p.restDensity > 0.0f ? p.massB / p.restDensity : 0.0f;
+        // the upload lands in posB2/volB2/idB2 and is compared with the raw copy of the last
+        // boundary upload (decided after the pull's synchronisation, PullBoundaryCommit)
         ids.clear();
         if (!v.idB) { ids.resize(nB); for (uint32_t i = 0; i < nB; i++) ids[i] = i; }
-        Upload(idB, v.idB ? v.idB : ids.data(), nB);
-        Pack4(posB, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, defPsi, tmp);
-        volB.ensure(std::max<uint32_t>(nB, 1));
+        Upload(idB2, v.idB ? v.idB : ids.data(), nB);
+        Pack4(posB2, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, defPsi, tmp);
+        volB2.ensure(std::max<uint32_t>(nB, 1));
         if (nB) {
-            if (v.volB) CK(cudaMemcpyAsync(volB.p, v.volB, nB * sizeof(float), cudaMemcpyHostToDevice, s));
+            if (v.volB) CK(cudaMemcpyAsync(volB2.p, v.volB, nB * sizeof(float), cudaMemcpyHostToDevice, s));
             else {
                 std::vector<float> d(nB, defVol);
-                CK(cudaMemcpy(volB.p, d.data(), nB * sizeof(float), cudaMemcpyHostToDevice));
+                CK(cudaMemcpyAsync(volB2.p, d.data(), nB * sizeof(float), cudaMemcpyHostToDevice, s));
+                Sync();
             }
         }
-        posB2.ensure(std::max<uint32_t>(nB, 1)); volB2.ensure(std::max<uint32_t>(nB, 1));
-        idB2.ensure(std::max<uint32_t>(nB, 1));
+        hm->bDiff = 1u;
+        const bool compare = nB && rawBValid && rawNB == nB;
+        if (compare) {
+            bDiff.ensure(1);
+            CK(cudaMemsetAsync(bDiff.p, 0, sizeof(uint32_t), s));
+            KBoundaryDiff<<<G(nB), 256, 0, s>>>(posB2.p, volB2.p, idB2.p, rawPosB.p, rawVolB.p, rawIdB.p, nB, bDiff.p);
+            CK(cudaMemcpyAsync(&hm->bDiff, bDiff.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        }
         // rigid particles (storage order preserved)
         ids.clear();
         if (!v.idR) { ids.resize(nR); for (uint32_t i = 0; i < nR; i++) ids[i] = i; }
@@ -395,43 +439,107 @@ public:
         bodyFT.ensure(std::max<size_t>((size_t)nRB * 6, 1));
         CK(cudaMemsetAsync(bodyFT.p, 0, bodyFT.cap * sizeof(double), s));
         // neighbor-search state is rebuilt from scratch
-        frameValid = false; frameRebuilds = 0; cellSize = 0.0f; reach = 1; bSortedForFrame = false;
-        bAabbValid = false; listsValid = false;
+        frameValid = false; frameRebuilds = 0; cellSize = 0.0f; reach = 1; listsValid = false;
         CK(cudaMemsetAsync(st.p, 0, sizeof(SolverState), s));
         // UpdateRigidParticles() at import (cpu_backend.cpp:326)
         if (nR) LaunchRigidUpdateParticles(RigidView(), BodyView(), false, err.p, s);
         CheckErrors();
+        PullBoundaryCommit(compare && hm->bDiff == 0u);
+    }
+    // same: the pulled boundary equals the raw copy bit for bit
+    void PullBoundaryCommit(bool same) {
+        if (same && bState != B_OTHER) {  // raw order or a sort of it: kept as is
+            bKeptAtPull = bState == B_SORTED_FROM_RAW;
+            return;
+        }
+        bKeptAtPull = false;
+        if (same) {  // other order / values: back to the raw order
+            CK(cudaMemcpyAsync(posB.p, rawPosB.p, nB * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(volB.p, rawVolB.p, nB * sizeof(float), cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(idB.p, rawIdB.p, nB * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+        } else {
+            Swap(posB, posB2); Swap(volB, volB2); Swap(idB, idB2);
+            rawPosB.ensure(std::max<uint32_t>(nB, 1)); rawVolB.ensure(std::max<uint32_t>(nB, 1));
+            rawIdB.ensure(std::max<uint32_t>(nB, 1));
+            if (nB) {
+                CK(cudaMemcpyAsync(rawPosB.p, posB.p, nB * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+                CK(cudaMemcpyAsync(rawVolB.p, volB.p, nB * sizeof(float), cudaMemcpyDeviceToDevice, s));
+                CK(cudaMemcpyAsync(rawIdB.p, idB.p, nB * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+            }
+            rawBValid = true;
+            rawNB = nB;
+            bAabbValid = false;
+        }
+        posB2.ensure(std::max<uint32_t>(nB, 1)); volB2.ensure(std::max<uint32_t>(nB, 1));
+        idB2.ensure(std::max<uint32_t>(nB, 1));
+        bState = B_RAW;
+        bSortedValid = false;
+    }
+    static bool SameFrame(const Frame& a, const Frame& b) {
+        return a.ox == b.ox && a.oy == b.oy && a.oz == b.oz && a.nx == b.nx && a.ny == b.ny && a.nz == b.nz &&
+               a.cellSizeInv == b.cellSizeInv && a.reach == b.reach && a.keyBits == b.keyBits;
+    }
+    // Boundary sorted by cell, with its cell table and grid, under the current frame. A stable
+    // sort of sorted cell IDs is the identity, so the reference's "sort only when not
+    // non-decreasing" (neighbor_search.cpp:1779-1810) is the same result. After a pull that kept
+    // a sort of the raw boundary, the reference sorts the raw order under the fresh frame: the
+    // kept arrays when the frame is the same, else the raw order is restored and sorted.
+    enum { B_SORTED_NOW = 0, B_KEPT_FROM_PULL = 1, B_ALREADY_SORTED = 2 };
+    int EnsureBoundarySorted(SortScratch& sc) {
+        const bool kept = bKeptAtPull;
+        bKeptAtPull = false;
+        if (bSortedValid && SameFrame(bSortFr, fr)) return kept ? B_KEPT_FROM_PULL : B_ALREADY_SORTED;
+        if (kept && nB) {
+            CK(cudaMemcpyAsync(posB.p, rawPosB.p, nB * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(volB.p, rawVolB.p, nB * sizeof(float), cudaMemcpyDeviceToDevice, s));
+            CK(cudaMemcpyAsync(idB.p, rawIdB.p, nB * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+            bState = B_RAW;
+        }
+        if (nB) {
+            SortByCell(posB.p, nB, fr, sc, permB.p, cidB.p, s);
+            GatherF4(permB.p, posB.p, posB2.p, nB, s); Swap(posB, posB2);
+            GatherF1(permB.p, volB.p, volB2.p, nB, s); Swap(volB, volB2);
+            GatherU64(permB.p, idB.p, idB2.p, nB, s); Swap(idB, idB2);
+            BuildCellTable(cidB.p, nB, uniqB.p, startB.p, nCellsDev.p + 1, scanScratch.p, s);
+            BuildGrid(uniqB.p, nCellsDev.p + 1, nB, fr, gridB.p, gridCells, s);
+            launches += SortLaunches(nB, fr.keyBits) + 3 + 3 + 1;
+        }
+        if (bState == B_RAW && nB) {
+            rawPermB.ensure(nB);
+            CK(cudaMemcpyAsync(rawPermB.p, permB.p, nB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        }
+        bState = bState == B_RAW ? B_SORTED_FROM_RAW : B_OTHER;
+        bSortFr = fr;
+        bSortedValid = true;
+        return B_SORTED_NOW;
     }
 
     void Push(tsp_state_view& v) {
         CK(cudaSetDevice(device));
         v.N_F = nF; v.N_B = nB; v.N_R = nR; v.N_RB = nRB; v.step = stepCount; v.time = simTime;
-        DBuf<float>& tmp = stage;
+        // every field gets its own staging columns, so all unpack kernels and copies queue
+        // back to back on the stream with one synchronisation at the end
+        const uint64_t F = nF, B = nB, R = nR;
+        stage.ensure(std::max<uint64_t>(18 * F + 4 * B + 8 * R, 1));
+        float* st0 = stage.p;
         if (v.idF && nF) CK(cudaMemcpyAsync(v.idF, idF.p, nF * 8ull, cudaMemcpyDeviceToHost, s));
-        Unpack4(posP.p, nF, v.xPosF, v.yPosF, v.zPosF, v.pressureF, tmp);
-        Sync();
-        Unpack4(velRho.p, nF, v.xVelF, v.yVelF, v.zVelF, v.densityF, tmp);
-        Sync();
-        Unpack4(velPred.p, nF, v.xVelPredF, v.yVelPredF, v.zVelPredF, nullptr, tmp);
-        Sync();
-        Unpack4(acc.p, nF, v.xAccPressF, v.yAccPressF, v.zAccPressF, nullptr, tmp);
-        Sync();
+        UnpackTo(posP.p, nF, v.xPosF, v.yPosF, v.zPosF, v.pressureF, st0);
+        UnpackTo(velRho.p, nF, v.xVelF, v.yVelF, v.zVelF, v.densityF, st0 + 4 * F);
+        UnpackTo(velPred.p, nF, v.xVelPredF, v.yVelPredF, v.zVelPredF, nullptr, st0 + 8 * F);
+        UnpackTo(acc.p, nF, v.xAccPressF, v.yAccPressF, v.zAccPressF, nullptr, st0 + 12 * F);
         if (nF && (v.sourceTermF || v.diagElemF)) {
-            tmp.ensure(2ull * nF);
-            KUnpack2<<<G(nF), 256, 0, s>>>(srcDiag.p, tmp.p, tmp.p + nF, nF);
-            if (v.sourceTermF) CK(cudaMemcpyAsync(v.sourceTermF, tmp.p, nF * 4ull, cudaMemcpyDeviceToHost, s));
-            if (v.diagElemF) CK(cudaMemcpyAsync(v.diagElemF, tmp.p + nF, nF * 4ull, cudaMemcpyDeviceToHost, s));
-            Sync();
+            float* sd = st0 + 16 * F;
+            KUnpack2<<<G(nF), 256, 0, s>>>(srcDiag.p, sd, sd + F, nF);
+            if (v.sourceTermF) CK(cudaMemcpyAsync(v.sourceTermF, sd, nF * 4ull, cudaMemcpyDeviceToHost, s));
+            if (v.diagElemF) CK(cudaMemcpyAsync(v.diagElemF, sd + F, nF * 4ull, cudaMemcpyDeviceToHost, s));
         }
         if (v.idB && nB) CK(cudaMemcpyAsync(v.idB, idB.p, nB * 8ull, cudaMemcpyDeviceToHost, s));
-        Unpack4(posB.p, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, tmp);
+        UnpackTo(posB.p, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, st0 + 18 * F);
         if (v.volB && nB) CK(cudaMemcpyAsync(v.volB, volB.p, nB * 4ull, cudaMemcpyDeviceToHost, s));
-        Sync();
         if (v.idR && nR) CK(cudaMemcpyAsync(v.idR, idR.p, nR * 8ull, cudaMemcpyDeviceToHost, s));
         if (v.bodyIdR && nR) CK(cudaMemcpyAsync(v.bodyIdR, bodyR.p, nR * 4ull, cudaMemcpyDeviceToHost, s));
-        Unpack4(relR.p, nR, v.xPosRelR, v.yPosRelR, v.zPosRelR, v.volR, tmp);
-        Sync();
-        Unpack4(posR.p, nR, v.xPosR, v.yPosR, v.zPosR, v.psiR, tmp);
+        UnpackTo(relR.p, nR, v.xPosRelR, v.yPosRelR, v.zPosRelR, v.volR, st0 + 18 * F + 4 * B);
+        UnpackTo(posR.p, nR, v.xPosR, v.yPosR, v.zPosR, v.psiR, st0 + 18 * F + 4 * B + 4 * R);
         Sync();
         if (nRB) {
             std::vector<double> bs((size_t)nRB * 48);
@@ -487,7 +595,8 @@ public:
         const bool zero = std::fabs(cs) <= 1e-7f;
         const float span = zero ? 0.0f : (prm.kernelRadius / cs);
         const uint32_t r = zero ? 1u : std::max<uint32_t>(1u, (uint32_t)std::ceil(std::max(0.0f, span - 1e-6f)));
-        if (std::fabs(cellSize - cs) > 1e-7f || reach != r) { frameValid = false; bSortedForFrame = false; }
+        // (a sort under another cell size is caught by the frame comparison of the boundary sort)
+        if (std::fabs(cellSize - cs) > 1e-7f || reach != r) frameValid = false;
         if (QuerySmemBytes(r) > 227u * 1024u)
             throw Error(TSP_ERR_UNSUPPORTED, "cell size ratio too small: query stencil exceeds shared memory");
         cellSize = cs;
@@ -590,26 +699,20 @@ public:
     void NeighborBuild(bool permuteAll) {
         SetCellSize();
         CK(cudaEventRecord(pev[0], s));
-        const bool frameChanged = UpdateFrame();
+        UpdateFrame();  // a changed frame invalidates the boundary sort through bSortFr
         CK(cudaEventRecord(pev[1], s));
         if (!frameValid) { listsValid = false; return; }
         EnsureNsScratch();
         SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p};
-        if (frameChanged || !bSortedForFrame) {
-            gridF.ensure(gridCells); gridB.ensure(gridCells); gridR.ensure(gridCells);
-            // boundary: a stable sort of already sorted cell IDs is the identity, so the
-            // reference's "sort only when not non-decreasing" (1779-1810) is the same result
-            if (nB) {
-                SortByCell(posB.p, nB, fr, sc, permB.p, cidB.p, s);
-                GatherF4(permB.p, posB.p, posB2.p, nB, s); Swap(posB, posB2);
-                GatherF1(permB.p, volB.p, volB2.p, nB, s); Swap(volB, volB2);
-                GatherU64(permB.p, idB.p, idB2.p, nB, s); Swap(idB, idB2);
-                BuildCellTable(cidB.p, nB, uniqB.p, startB.p, nCellsDev.p + 1, scanScratch.p, s);
-                BuildGrid(uniqB.p, nCellsDev.p + 1, nB, fr, gridB.p, gridCells, s);
-                launches += SortLaunches(nB, fr.keyBits) + 3 + 3 + 1;
-            }
-            bSortedForFrame = true;
-        } else if (nB) {
+        // boundary: sorted under this frame unless it already is (then its permutation this
+        // step is the identity, or, on the first build after a pull that kept a sort of the same
+        // raw boundary, that sort's permutation)
+        if (gridCells > gridB.cap) bSortedValid = false;
+        gridF.ensure(gridCells); gridB.ensure(gridCells); gridR.ensure(gridCells);
+        const int bs = EnsureBoundarySorted(sc);
+        if (nB && bs == B_KEPT_FROM_PULL) {
+            CK(cudaMemcpyAsync(permB.p, rawPermB.p, nB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        } else if (nB && bs == B_ALREADY_SORTED) {
             KIota<<<G(nB), 256, 0, s>>>(permB.p, nB);
             launches += 1;
         }
@@ -1122,6 +1225,7 @@ public:
                 psiTmpB.ensure(nB);
                 CK(cudaMemcpy(psiTmpB.p, dp.data(), nB * 4ull, cudaMemcpyHostToDevice));
                 KSetW<<<G(nB), 256, 0, s>>>(posB.p, psiTmpB.p, nB);
+                bState = B_OTHER;
             }
             if (nR) {
                 CK(cudaMemcpy(volR.p, dv.data(), nR * 4ull, cudaMemcpyHostToDevice));
@@ -1136,21 +1240,15 @@ public:
             SetCellSize();
             UpdateFrame();
             EnsureNsScratch();
-            if (!bSortedForFrame) {
-                gridF.ensure(gridCells); gridB.ensure(gridCells); gridR.ensure(gridCells);
-                SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p};
-                SortByCell(posB.p, nB, fr, sc, permB.p, cidB.p, s);
-                GatherF4(permB.p, posB.p, posB2.p, nB, s); Swap(posB, posB2);
-                GatherF1(permB.p, volB.p, volB2.p, nB, s); Swap(volB, volB2);
-                GatherU64(permB.p, idB.p, idB2.p, nB, s); Swap(idB, idB2);
-                BuildCellTable(cidB.p, nB, uniqB.p, startB.p, nCellsDev.p + 1, scanScratch.p, s);
-                BuildGrid(uniqB.p, nCellsDev.p + 1, nB, fr, gridB.p, gridCells, s);
-                bSortedForFrame = true;
-            }
+            if (gridCells > gridB.cap) bSortedValid = false;
+            gridF.ensure(gridCells); gridB.ensure(gridCells); gridR.ensure(gridCells);
+            SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p};
+            EnsureBoundarySorted(sc);
             psiTmpB.ensure(nB);
             LaunchBoundaryVolumes(c, posB.p, nB, startB.p, gridB.p, fr, defVol, defPsi, prm.restDensity, volB.p,
                                   psiTmpB.p, s);
             KSetW<<<G(nB), 256, 0, s>>>(posB.p, psiTmpB.p, nB);
+            bState = B_OTHER;  // volumes and psi no longer those of the raw upload
         }
         if (nR) {
             // per body, in the body frame, over the body's own particles, sorted by (z, y, x) cell
@@ -1278,8 +1376,9 @@ public:
             case TSP_FIELD_VOL_B:
                 if (n != nB) throw Error(TSP_ERR_INVALID, "field size mismatch");
                 if (nB) CK(cudaMemcpy(volB.p, x, nB * 4ull, cudaMemcpyHostToDevice));
+                bState = B_OTHER;
                 break;
-            case TSP_FIELD_PSI_B: setW(posB, nB); break;
+            case TSP_FIELD_PSI_B: setW(posB, nB); bState = B_OTHER; break;
             default: throw Error(TSP_ERR_INVALID, "field is not writable");
         }
     }
