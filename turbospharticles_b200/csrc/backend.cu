@@ -227,6 +227,22 @@ public:
     // (+ rigid integration), 12 end
     static constexpr int N_PHASE_EVENTS = 13;
     cudaEvent_t pev[N_PHASE_EVENTS] = {};
+    // copy stream of the state boundary: the host <-> device copies of pull / push run on xs
+    // while the pack / unpack kernels run on s, ordered by events in both directions
+    cudaStream_t xs = nullptr;
+    cudaEvent_t xev[8] = {};
+    uint32_t xevNext = 0;
+    cudaEvent_t NextXev() { return xev[xevNext++ % 8]; }
+    void CopiesAfterCompute() {  // xs waits for everything queued on s so far
+        cudaEvent_t e = NextXev();
+        CK(cudaEventRecord(e, s));
+        CK(cudaStreamWaitEvent(xs, e, 0));
+    }
+    void ComputeAfterCopies() {  // s waits for everything queued on xs so far
+        cudaEvent_t e = NextXev();
+        CK(cudaEventRecord(e, xs));
+        CK(cudaStreamWaitEvent(s, e, 0));
+    }
     bool phaseValid = false;
     float lastStepMs = 0.f, lastNbrMs = 0.f, lastJacMs = 0.f;
     std::string lastErr;
@@ -241,6 +257,8 @@ public:
         CK(cudaSetDevice(device));
         CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&capStream, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&xs, cudaStreamNonBlocking));
+        for (auto& e : xev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         CK(cudaMallocHost(&hm, sizeof(HostMirror)));
         std::memset(hm, 0, sizeof(HostMirror));
         st.ensure(1);
@@ -265,6 +283,9 @@ public:
             }
         for (auto& e : ev) if (e) cudaEventDestroy(e);
         for (auto& e : pev) if (e) cudaEventDestroy(e);
+        if (xs) cudaStreamSynchronize(xs);
+        for (auto& e : xev) if (e) cudaEventDestroy(e);
+        if (xs) cudaStreamDestroy(xs);
         if (hm) cudaFreeHost(hm);
         if (capStream) cudaStreamDestroy(capStream);
         if (s) cudaStreamDestroy(s);
@@ -300,6 +321,27 @@ public:
         d.ensure(std::max<size_t>(n, 1));
         if (n && h) CK(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
     }
+    // Pack4 with the host columns copied on the copy stream into stg[0, 4n) (the caller's own
+    // staging region) and the pack kernel on s once they have arrived
+    void Pack4X(DBuf<float4>& out, uint32_t n, const float* a, const float* b, const float* c, const float* d,
+                float dDefault, float* stg) {
+        out.ensure(std::max<uint32_t>(n, 1));
+        if (n == 0) return;
+        const float* src[4] = {a, b, c, d};
+        float* dst[4] = {nullptr, nullptr, nullptr, nullptr};
+        for (int k = 0; k < 4; k++)
+            if (src[k]) {
+                dst[k] = stg + (uint64_t)k * n;
+                CK(cudaMemcpyAsync(dst[k], src[k], n * sizeof(float), cudaMemcpyHostToDevice, xs));
+            }
+        ComputeAfterCopies();
+        KPack4<<<G(n), 256, 0, s>>>(dst[0], dst[1], dst[2], dst[3], dDefault, out.p, n);
+    }
+    template <typename T>
+    void UploadX(DBuf<T>& d, const T* h, size_t n) {
+        d.ensure(std::max<size_t>(n, 1));
+        if (n && h) CK(cudaMemcpyAsync(d.p, h, n * sizeof(T), cudaMemcpyHostToDevice, xs));
+    }
     void Pack4(DBuf<float4>& out, uint32_t n, const float* a, const float* b, const float* c, const float* d,
                float dDefault, DBuf<float>& tmp) {
         out.ensure(std::max<uint32_t>(n, 1));
@@ -321,14 +363,20 @@ public:
     }
     // unpack into the 4 * n floats at dev (only the columns a host array asks for) and queue
     // their device-to-host copies; dev must stay untouched until the stream passes the copies
-    void UnpackTo(const float4* in, uint32_t n, float* a, float* b, float* c, float* d, float* dev0) {
+    // cs: the stream of the device-to-host copies (s, or the copy stream xs ordered after the
+    // unpack kernel)
+    void UnpackTo(const float4* in, uint32_t n, float* a, float* b, float* c, float* d, float* dev0,
+                  cudaStream_t cs = nullptr) {
         if (n == 0) return;
         float* host[4] = {a, b, c, d};
         float* dev[4];
         for (int k = 0; k < 4; k++) dev[k] = host[k] ? dev0 + (uint64_t)k * n : nullptr;
+        if (!host[0] && !host[1] && !host[2] && !host[3]) return;
         KUnpack4<<<G(n), 256, 0, s>>>(in, dev[0], dev[1], dev[2], dev[3], n);
+        if (!cs) cs = s;
+        else CopiesAfterCompute();
         for (int k = 0; k < 4; k++)
-            if (host[k]) CK(cudaMemcpyAsync(host[k], dev[k], n * sizeof(float), cudaMemcpyDeviceToHost, s));
+            if (host[k]) CK(cudaMemcpyAsync(host[k], dev[k], n * sizeof(float), cudaMemcpyDeviceToHost, cs));
     }
 
     void Pull(const tsp_state_view& v, const tsp_params& p) {
@@ -339,24 +387,30 @@ public:
         if (nF > 0x7fffffffu || nB > 0x7fffffffu || nR > 0x7fffffffu)
             throw Error(TSP_ERR_OVERFLOW, "particle count exceeds the local particle limit");
         stepCount = v.step; simTime = v.time;
+        // every column group has its own staging region, so the copies (on xs) run back to back
+        // while the pack kernels (on s) follow each group as it arrives
+        const uint64_t F = nF, B = nB, R = nR;
+        tmp.ensure(std::max<uint64_t>(18 * F + 4 * B + 8 * R, 1));
+        float* stg = tmp.p;
+        CopiesAfterCompute();  // no copy may overwrite staging that queued work still reads
         // fluid
         std::vector<uint64_t> ids;
         if (!v.idF) { ids.resize(nF); for (uint32_t i = 0; i < nF; i++) ids[i] = i; }
-        Upload(idF, v.idF ? v.idF : ids.data(), nF);
-        Pack4(posP, nF, v.xPosF, v.yPosF, v.zPosF, v.pressureF, 0.0f, tmp);
-        Pack4(velRho, nF, v.xVelF, v.yVelF, v.zVelF, v.densityF, p.restDensity, tmp);
-        Pack4(velPred, nF, v.xVelPredF, v.yVelPredF, v.zVelPredF, nullptr, 0.0f, tmp);
-        Pack4(acc, nF, v.xAccPressF, v.yAccPressF, v.zAccPressF, nullptr, 0.0f, tmp);
+        UploadX(idF, v.idF ? v.idF : ids.data(), nF);
+        Pack4X(posP, nF, v.xPosF, v.yPosF, v.zPosF, v.pressureF, 0.0f, stg);
+        Pack4X(velRho, nF, v.xVelF, v.yVelF, v.zVelF, v.densityF, p.restDensity, stg + 4 * F);
+        Pack4X(velPred, nF, v.xVelPredF, v.yVelPredF, v.zVelPredF, nullptr, 0.0f, stg + 8 * F);
+        Pack4X(acc, nF, v.xAccPressF, v.yAccPressF, v.zAccPressF, nullptr, 0.0f, stg + 12 * F);
         srcDiag.ensure(std::max<uint32_t>(nF, 1));
         if (nF) {
-            tmp.ensure(2ull * nF);
             const float* sh[2] = {v.sourceTermF, v.diagElemF};
             float* sd[2] = {nullptr, nullptr};
             for (int k = 0; k < 2; k++)
                 if (sh[k]) {
-                    sd[k] = tmp.p + (uint64_t)k * nF;
-                    CK(cudaMemcpyAsync(sd[k], sh[k], nF * sizeof(float), cudaMemcpyHostToDevice, s));
+                    sd[k] = stg + 16 * F + (uint64_t)k * nF;
+                    CK(cudaMemcpyAsync(sd[k], sh[k], nF * sizeof(float), cudaMemcpyHostToDevice, xs));
                 }
+            ComputeAfterCopies();
             KPack2<<<G(nF), 256, 0, s>>>(sd[0], sd[1], srcDiag.p, nF);
         }
         posP2.ensure(std::max<uint32_t>(nF, 1)); velRho2.ensure(std::max<uint32_t>(nF, 1));
@@ -365,19 +419,17 @@ public:
         const float defPsi = p.massB, defVol = p.restDensity > 0.0f ? p.massB / p.restDensity : 0.0f;
         // the upload lands in posB2/volB2/idB2 and is compared with the raw copy of the last
         // boundary upload (decided after the pull's synchronisation, PullBoundaryCommit)
-        ids.clear();
-        if (!v.idB) { ids.resize(nB); for (uint32_t i = 0; i < nB; i++) ids[i] = i; }
-        Upload(idB2, v.idB ? v.idB : ids.data(), nB);
-        Pack4(posB2, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, defPsi, tmp);
+        std::vector<uint64_t> idsB;
+        if (!v.idB) { idsB.resize(nB); for (uint32_t i = 0; i < nB; i++) idsB[i] = i; }
+        UploadX(idB2, v.idB ? v.idB : idsB.data(), nB);
         volB2.ensure(std::max<uint32_t>(nB, 1));
+        std::vector<float> defVolB;
         if (nB) {
-            if (v.volB) CK(cudaMemcpyAsync(volB2.p, v.volB, nB * sizeof(float), cudaMemcpyHostToDevice, s));
-            else {
-                std::vector<float> d(nB, defVol);
-                CK(cudaMemcpyAsync(volB2.p, d.data(), nB * sizeof(float), cudaMemcpyHostToDevice, s));
-                Sync();
-            }
+            if (!v.volB) defVolB.assign(nB, defVol);
+            CK(cudaMemcpyAsync(volB2.p, v.volB ? v.volB : defVolB.data(), nB * sizeof(float), cudaMemcpyHostToDevice,
+                               xs));
         }
+        Pack4X(posB2, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, defPsi, stg + 18 * F);
         hm->bDiff = 1u;
         const bool compare = nB && rawBValid && rawNB == nB;
         if (compare) {
@@ -401,8 +453,8 @@ public:
             hRelY[i] = v.yPosRelR ? v.yPosRelR[i] : 0.f;
             hRelZ[i] = v.zPosRelR ? v.zPosRelR[i] : 0.f;
         }
-        Pack4(relR, nR, v.xPosRelR, v.yPosRelR, v.zPosRelR, v.volR, defVol, tmp);
-        Pack4(posR, nR, nullptr, nullptr, nullptr, v.psiR, defPsi, tmp);
+        Pack4X(relR, nR, v.xPosRelR, v.yPosRelR, v.zPosRelR, v.volR, defVol, stg + 18 * F + 4 * B);
+        Pack4X(posR, nR, nullptr, nullptr, nullptr, v.psiR, defPsi, stg + 18 * F + 4 * B + 4 * R);
         velR.ensure(std::max<uint32_t>(nR, 1)); velPredR.ensure(std::max<uint32_t>(nR, 1));
         forceR.ensure(std::max<uint32_t>(nR, 1));
         if (nR) CK(cudaMemsetAsync(forceR.p, 0, nR * sizeof(float4), s));
@@ -443,6 +495,7 @@ public:
         CK(cudaMemsetAsync(st.p, 0, sizeof(SolverState), s));
         // UpdateRigidParticles() at import (cpu_backend.cpp:326)
         if (nR) LaunchRigidUpdateParticles(RigidView(), BodyView(), false, err.p, s);
+        ComputeAfterCopies();
         CheckErrors();
         PullBoundaryCommit(compare && hm->bDiff == 0u);
     }
@@ -517,30 +570,33 @@ public:
     void Push(tsp_state_view& v) {
         CK(cudaSetDevice(device));
         v.N_F = nF; v.N_B = nB; v.N_R = nR; v.N_RB = nRB; v.step = stepCount; v.time = simTime;
-        // every field gets its own staging columns, so all unpack kernels and copies queue
-        // back to back on the stream with one synchronisation at the end
+        // every field gets its own staging columns: the unpack kernels run on s and the copies
+        // on the copy stream xs, each group's copies after its kernel, one synchronisation at the end
         const uint64_t F = nF, B = nB, R = nR;
         stage.ensure(std::max<uint64_t>(18 * F + 4 * B + 8 * R, 1));
         float* st0 = stage.p;
-        if (v.idF && nF) CK(cudaMemcpyAsync(v.idF, idF.p, nF * 8ull, cudaMemcpyDeviceToHost, s));
-        UnpackTo(posP.p, nF, v.xPosF, v.yPosF, v.zPosF, v.pressureF, st0);
-        UnpackTo(velRho.p, nF, v.xVelF, v.yVelF, v.zVelF, v.densityF, st0 + 4 * F);
-        UnpackTo(velPred.p, nF, v.xVelPredF, v.yVelPredF, v.zVelPredF, nullptr, st0 + 8 * F);
-        UnpackTo(acc.p, nF, v.xAccPressF, v.yAccPressF, v.zAccPressF, nullptr, st0 + 12 * F);
+        CopiesAfterCompute();  // the state the copies read is final
+        if (v.idF && nF) CK(cudaMemcpyAsync(v.idF, idF.p, nF * 8ull, cudaMemcpyDeviceToHost, xs));
+        UnpackTo(posP.p, nF, v.xPosF, v.yPosF, v.zPosF, v.pressureF, st0, xs);
+        UnpackTo(velRho.p, nF, v.xVelF, v.yVelF, v.zVelF, v.densityF, st0 + 4 * F, xs);
+        UnpackTo(velPred.p, nF, v.xVelPredF, v.yVelPredF, v.zVelPredF, nullptr, st0 + 8 * F, xs);
+        UnpackTo(acc.p, nF, v.xAccPressF, v.yAccPressF, v.zAccPressF, nullptr, st0 + 12 * F, xs);
         if (nF && (v.sourceTermF || v.diagElemF)) {
             float* sd = st0 + 16 * F;
             KUnpack2<<<G(nF), 256, 0, s>>>(srcDiag.p, sd, sd + F, nF);
-            if (v.sourceTermF) CK(cudaMemcpyAsync(v.sourceTermF, sd, nF * 4ull, cudaMemcpyDeviceToHost, s));
-            if (v.diagElemF) CK(cudaMemcpyAsync(v.diagElemF, sd + F, nF * 4ull, cudaMemcpyDeviceToHost, s));
+            CopiesAfterCompute();
+            if (v.sourceTermF) CK(cudaMemcpyAsync(v.sourceTermF, sd, nF * 4ull, cudaMemcpyDeviceToHost, xs));
+            if (v.diagElemF) CK(cudaMemcpyAsync(v.diagElemF, sd + F, nF * 4ull, cudaMemcpyDeviceToHost, xs));
         }
-        if (v.idB && nB) CK(cudaMemcpyAsync(v.idB, idB.p, nB * 8ull, cudaMemcpyDeviceToHost, s));
-        UnpackTo(posB.p, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, st0 + 18 * F);
-        if (v.volB && nB) CK(cudaMemcpyAsync(v.volB, volB.p, nB * 4ull, cudaMemcpyDeviceToHost, s));
-        if (v.idR && nR) CK(cudaMemcpyAsync(v.idR, idR.p, nR * 8ull, cudaMemcpyDeviceToHost, s));
-        if (v.bodyIdR && nR) CK(cudaMemcpyAsync(v.bodyIdR, bodyR.p, nR * 4ull, cudaMemcpyDeviceToHost, s));
-        UnpackTo(relR.p, nR, v.xPosRelR, v.yPosRelR, v.zPosRelR, v.volR, st0 + 18 * F + 4 * B);
-        UnpackTo(posR.p, nR, v.xPosR, v.yPosR, v.zPosR, v.psiR, st0 + 18 * F + 4 * B + 4 * R);
-        Sync();
+        if (v.idB && nB) CK(cudaMemcpyAsync(v.idB, idB.p, nB * 8ull, cudaMemcpyDeviceToHost, xs));
+        UnpackTo(posB.p, nB, v.xPosB, v.yPosB, v.zPosB, v.psiB, st0 + 18 * F, xs);
+        if (v.volB && nB) CK(cudaMemcpyAsync(v.volB, volB.p, nB * 4ull, cudaMemcpyDeviceToHost, xs));
+        if (v.idR && nR) CK(cudaMemcpyAsync(v.idR, idR.p, nR * 8ull, cudaMemcpyDeviceToHost, xs));
+        if (v.bodyIdR && nR) CK(cudaMemcpyAsync(v.bodyIdR, bodyR.p, nR * 4ull, cudaMemcpyDeviceToHost, xs));
+        UnpackTo(relR.p, nR, v.xPosRelR, v.yPosRelR, v.zPosRelR, v.volR, st0 + 18 * F + 4 * B, xs);
+        UnpackTo(posR.p, nR, v.xPosR, v.yPosR, v.zPosR, v.psiR, st0 + 18 * F + 4 * B + 4 * R, xs);
+        CK(cudaStreamSynchronize(xs));
+        ComputeAfterCopies();  // later work on s may reuse the staging the copies read
         if (nRB) {
             std::vector<double> bs((size_t)nRB * 48);
             CK(cudaMemcpyAsync(bs.data(), bodyState.p, bs.size() * 8, cudaMemcpyDeviceToHost, s));
