@@ -103,6 +103,7 @@ struct HostMirror {
     uint64_t contactTot[2];
     uint32_t exportCount;
     uint32_t bDiff;
+    ProbeResult probeInit;  // identity bounds of an empty class, the probe accumulator's reset
 };
 
 class Backend {
@@ -135,6 +136,10 @@ public:
     // neighbor search
     Frame fr{};
     bool frameValid = false;
+    // the probe (bounds + frame-exit flag) of the current positions under the current frame and
+    // domain was taken at the end of the last step, with its read-back: the next frame rule uses
+    // it without a launch and a round trip of its own
+    bool probeFresh = false;
     float cellSize = 0.0f;
     uint32_t reach = 1;
     uint32_t frameRebuilds = 0;
@@ -261,6 +266,10 @@ public:
         for (auto& e : xev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         CK(cudaMallocHost(&hm, sizeof(HostMirror)));
         std::memset(hm, 0, sizeof(HostMirror));
+        for (int a = 0; a < 3; a++) {  // (neighbor_search.cpp:205-213)
+            hm->probeInit.mnKey[a] = OrderedIntHost(3.402823466e38f);
+            hm->probeInit.mxKey[a] = OrderedIntHost(-3.402823466e38f);
+        }
         st.ensure(1);
         err.ensure(1);
         probe.ensure(1);
@@ -312,6 +321,7 @@ public:
 
     // -------------------------------------------------------------------------- state boundary
     void SetDomain(const float* mn, const float* mx) {
+        probeFresh = false;
         for (int a = 0; a < 3; a++) { dom.mn[a] = mn[a]; dom.mx[a] = mx[a]; }
         dom.bounded = !(mx[0] <= mn[0] || mx[1] <= mn[1] || mx[2] <= mn[2]);
     }
@@ -491,7 +501,7 @@ public:
         bodyFT.ensure(std::max<size_t>((size_t)nRB * 6, 1));
         CK(cudaMemsetAsync(bodyFT.p, 0, bodyFT.cap * sizeof(double), s));
         // neighbor-search state is rebuilt from scratch
-        frameValid = false; frameRebuilds = 0; cellSize = 0.0f; reach = 1; listsValid = false;
+        frameValid = false; frameRebuilds = 0; cellSize = 0.0f; reach = 1; listsValid = false; probeFresh = false;
         CK(cudaMemsetAsync(st.p, 0, sizeof(SolverState), s));
         // UpdateRigidParticles() at import (cpu_backend.cpp:326)
         if (nR) LaunchRigidUpdateParticles(RigidView(), BodyView(), false, err.p, s);
@@ -663,16 +673,12 @@ public:
     // UpdateCellFrame (neighbor_search.cpp:1902-2006); returns true when the frame changed
     bool UpdateFrame() {
         if (nF == 0 && nB == 0 && nR == 0) { frameValid = false; return false; }
-        ProbeResult init;  // identity bounds of an empty class (neighbor_search.cpp:205-213)
-        for (int a = 0; a < 3; a++) { init.mnKey[a] = OrderedIntHost(3.402823466e38f); init.mxKey[a] = OrderedIntHost(-3.402823466e38f); }
-        init.exceeded = 0; init.pad = 0;
-        hm->probe = init;
-        CK(cudaMemcpyAsync(probe.p, &hm->probe, sizeof(ProbeResult), cudaMemcpyHostToDevice, s));
-        LaunchProbe(posP.p, nF, fr, frameValid, dom, probe.p, s);
-        LaunchProbe(posR.p, nR, fr, frameValid, dom, probe.p, s);
-        launches += (nF ? 1 : 0) + (nR ? 1 : 0);
-        CK(cudaMemcpyAsync(&hm->probe, probe.p, sizeof(ProbeResult), cudaMemcpyDeviceToHost, s));
-        Sync();
+        const ProbeResult init = hm->probeInit;
+        if (!probeFresh) {
+            QueueProbe();
+            Sync();
+        }
+        probeFresh = false;
         ProbeResult pr = hm->probe;
         float mn[3], mx[3];
         for (int a = 0; a < 3; a++) { mn[a] = OrderedIntToFloat(pr.mnKey[a]); mx[a] = OrderedIntToFloat(pr.mxKey[a]); }
@@ -717,6 +723,14 @@ public:
             throw Error(TSP_ERR_UNSUPPORTED, "cell frame volume exceeds the dense grid limit (2^28 cells)");
         gridCells = cells;
         return true;
+    }
+    // probe of the fluid and rigid positions into hm->probe (valid after the stream passes it)
+    void QueueProbe() {
+        CK(cudaMemcpyAsync(probe.p, &hm->probeInit, sizeof(ProbeResult), cudaMemcpyHostToDevice, s));
+        LaunchProbe(posP.p, nF, fr, frameValid, dom, probe.p, s);
+        LaunchProbe(posR.p, nR, fr, frameValid, dom, probe.p, s);
+        launches += (nF ? 1 : 0) + (nR ? 1 : 0);
+        CK(cudaMemcpyAsync(&hm->probe, probe.p, sizeof(ProbeResult), cudaMemcpyDeviceToHost, s));
     }
     void EnsureNsScratch() {
         const uint32_t nMax = std::max(nF, std::max(nB, nR));
@@ -803,7 +817,7 @@ public:
         LaunchQueryRigid(false, qa, rl, s);
         CK(cudaEventRecord(pev[3], s));
         const uint32_t nChunks = (nF + SELL_W - 1) / SELL_W;
-        for (int k = 0; k < 3; k++) FinalizeSell(Meta(k), nChunks, scanScratch2.p, sellTot.p + k, s);
+        FinalizeSell3(Meta(0), Meta(1), Meta(2), nChunks, scanScratch2.p, sellTot.p, s);
         for (int k = 0; k < 3; k++) FinalizeCsr(cntR[k].p, offR[k].p, nR, scanScratch.p, csrTot.p + k, s);
         CK(cudaMemcpyAsync(hm->sellTot, sellTot.p, 3 * sizeof(U64x2), cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(hm->csrTot, csrTot.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
@@ -825,7 +839,7 @@ public:
         LaunchQueryFluid(true, qa, m0, m1, m2, s);
         LaunchQueryRigid(true, qa, rl, s);
         CK(cudaEventRecord(pev[5], s));
-        launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + (nF ? 9u : 0u) + (nR ? 9u : 0u);
+        launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + FinalizeSell3Launches(nChunks) + (nR ? 9u : 0u);
         listsValid = true;
     }
     QueryArgs MakeQueryArgs() {
@@ -1180,10 +1194,13 @@ public:
             LaunchRigidUpdateParticles(rp, bd, false, err.p, s);
         }
         CK(cudaEventRecord(pev[11], s));
+        probeFresh = false;
+        if (frameValid) QueueProbe();  // the next step's frame rule reads it with this read-back
         CK(cudaMemcpyAsync(&hm->st, st.p, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
         launches += (nF ? 6u : 0u) + (nRB ? 13u : 0u);
         CK(cudaEventRecord(pev[12], s));
         CheckErrors();
+        probeFresh = frameValid;
         float t = 0.f;
         cudaEventElapsedTime(&t, ev[0], pev[12]); lastStepMs = t;
         cudaEventElapsedTime(&t, ev[0], ev[1]); lastNbrMs = t;
@@ -1231,7 +1248,7 @@ public:
                 if (errSums) for (int k = 0; k < 3; k++) errSums[k] = hm->st.sums[k];
                 break;
             }
-            case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); break;
+            case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); probeFresh = false; break;
             case TSP_STAGE_BOUNDARY_VOLUMES: BoundaryVolumes(c); break;
             default: throw Error(TSP_ERR_INVALID, "unknown stage");
         }
@@ -1257,7 +1274,7 @@ public:
                 case TSP_STAGE_SOURCE_DIAG_INIT: LaunchSourceDiagInit(c, f, b, r, nv, st.p, s); break;
                 case TSP_STAGE_PRESSURE_ACC: LaunchPressureAcc(c, f, b, r, nv, s); break;
                 case TSP_STAGE_JACOBI_UPDATE: LaunchJacobi(c, f, b, r, nv, ctl, st.p, partials.p, 0ull, false, s); break;
-                case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); break;
+                case TSP_STAGE_INTEGRATION: LaunchIntegration(c, f, s); probeFresh = false; break;
                 default: throw Error(TSP_ERR_INVALID, "stage cannot be timed");
             }
             launches += 1;
@@ -1414,7 +1431,7 @@ public:
             if (cnt) CK(cudaMemcpy(dst.p, h.data(), cnt * 16ull, cudaMemcpyHostToDevice));
         };
         switch (field) {
-            case TSP_FIELD_POS: set3(posP, nF); break;
+            case TSP_FIELD_POS: set3(posP, nF); probeFresh = false; break;
             case TSP_FIELD_VEL: set3(velRho, nF); break;
             case TSP_FIELD_VEL_PRED: set3(velPred, nF); break;
             case TSP_FIELD_ACC_PRESS: set3(acc, nF); break;

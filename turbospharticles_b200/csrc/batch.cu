@@ -986,7 +986,7 @@ public:
         qa.chunkLen = chunkLen.p; qa.chunkScene = chunkScene.p; qa.scenes = dGeom.p;
         CK(cudaMemsetAsync(nbrTot.p, 0, 3 * sizeof(unsigned long long), s));
         LaunchQueryFluid(false, qa, Meta(0), Meta(1), Meta(2), s);
-        for (int k = 0; k < 3; k++) FinalizeSell(Meta(k), nChunks, scanScratch2.p, sellTot.p + k, s);
+        FinalizeSell3(Meta(0), Meta(1), Meta(2), nChunks, scanScratch2.p, sellTot.p, s);
         U64x2 tot[3];
         CK(cudaMemcpyAsync(tot, sellTot.p, sizeof(tot), cudaMemcpyDeviceToHost, s));
         Sync();
@@ -995,7 +995,7 @@ public:
             sell[k].l16.grow(tot[k].a, BATCH_LIST_GROWTH); sell[k].l32.grow(tot[k].b, BATCH_LIST_GROWTH);
         }
         LaunchQueryFluid(true, qa, Meta(0), Meta(1), Meta(2), s);
-        launches += 2 + 9;
+        launches += 2 + FinalizeSell3Launches(nChunks);
         // ---- solver stages; the Jacobi loop skips converged scenes
         const Consts c = MakeConsts(prm);
         const FluidDev f = Fluid(false);

@@ -191,6 +191,10 @@ void LaunchQueryFluid(bool fill, const QueryArgs& a, const SellMeta& ff, const S
                       cudaStream_t s);
 void LaunchQueryRigid(bool fill, const QueryArgs& a, const RigidLists& L, cudaStream_t s);
 void FinalizeSell(const SellMeta& m, uint32_t nChunks, U64x2* scratch, U64x2* totals, cudaStream_t s);
+// the FF, FB and FR finalize scans in one launch (up to 65,536 chunks; three scans beyond)
+void FinalizeSell3(const SellMeta& m0, const SellMeta& m1, const SellMeta& m2, uint32_t nChunks, U64x2* scratch,
+                   U64x2* totals, cudaStream_t s);
+inline uint32_t FinalizeSell3Launches(uint32_t nChunks) { return nChunks == 0 ? 0u : (nChunks <= 65536u ? 1u : 9u); }
 void FinalizeCsr(const uint16_t* counts, uint64_t* off, uint32_t n, uint64_t* scratch, uint64_t* total, cudaStream_t s);
 void LaunchDecodeSellRows(const SellMeta& m, uint32_t nF, const uint64_t* rowOff, uint32_t* out, cudaStream_t s);
 

@@ -780,6 +780,58 @@ void FinalizeSell(const SellMeta& m, uint32_t nChunks, U64x2* scratch, U64x2* to
     DeviceScan<U64x2>(SellSizeIn{m.pitch, m.format}, SellOffsetOut{m.format, m.offset}, nChunks, scratch, totals, s);
 }
 
+// The same three scans (FF, FB, FR lists) in one launch: block b scans list b, each thread a
+// contiguous run of chunks (local sums, block-wide exclusive scan of the thread sums, then the
+// offsets of its run). Integer sums: the offsets and totals equal the three-kernel scan's.
+constexpr uint32_t SELL3_THREADS = 1024;
+constexpr uint32_t SELL3_MAX_CHUNKS = 64u * SELL3_THREADS;
+__global__ void __launch_bounds__(SELL3_THREADS) KFinalizeSell3(SellMeta m0, SellMeta m1, SellMeta m2, uint32_t nChunks,
+                                                               U64x2* __restrict__ totals) {
+    __shared__ U64x2 warpSum[SELL3_THREADS / 32];
+    const SellMeta& m = blockIdx.x == 0 ? m0 : (blockIdx.x == 1 ? m1 : m2);
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t seg = (nChunks + SELL3_THREADS - 1) / SELL3_THREADS;
+    const uint32_t beg = min(t * seg, nChunks), end = min(beg + seg, nChunks);
+    U64x2 own{0, 0};
+    for (uint32_t c = beg; c < end; c++) {
+        const uint64_t sz = (uint64_t)m.pitch[c] * SELL_W;
+        if (m.format[c] == FMT_DELTA16X2) own.a += sz;
+        else own.b += sz;
+    }
+    U64x2 incl = own;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const U64x2 o = ShflUp(incl, d);
+        if ((int)lane >= d) incl = incl + o;
+    }
+    if (lane == 31) warpSum[warp] = incl;
+    __syncthreads();
+    U64x2 pre{0, 0}, tot{0, 0};
+    for (uint32_t w = 0; w < SELL3_THREADS / 32; w++) {
+        if (w < warp) pre = pre + warpSum[w];
+        tot = tot + warpSum[w];
+    }
+    U64x2 run = pre + incl;
+    run.a -= own.a;
+    run.b -= own.b;
+    for (uint32_t c = beg; c < end; c++) {
+        const uint64_t sz = (uint64_t)m.pitch[c] * SELL_W;
+        if (m.format[c] == FMT_DELTA16X2) { m.offset[c] = run.a; run.a += sz; }
+        else { m.offset[c] = run.b; run.b += sz; }
+    }
+    if (t == 0) totals[blockIdx.x] = tot;
+}
+void FinalizeSell3(const SellMeta& m0, const SellMeta& m1, const SellMeta& m2, uint32_t nChunks, U64x2* scratch,
+                   U64x2* totals, cudaStream_t s) {
+    if (nChunks > 0 && nChunks <= SELL3_MAX_CHUNKS) {
+        KFinalizeSell3<<<3, SELL3_THREADS, 0, s>>>(m0, m1, m2, nChunks, totals);
+        return;
+    }
+    FinalizeSell(m0, nChunks, scratch, totals + 0, s);
+    FinalizeSell(m1, nChunks, scratch, totals + 1, s);
+    FinalizeSell(m2, nChunks, scratch, totals + 2, s);
+}
+
 struct CountIn {
     const uint16_t* c;
     __device__ uint64_t operator()(uint64_t i) const { return c[i]; }
