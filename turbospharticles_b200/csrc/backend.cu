@@ -91,12 +91,25 @@ void LaunchUnpack2(const float2* in, float* a, float* b, uint32_t n, cudaStream_
     if (n) KUnpack2<<<G(n), 256, 0, s>>>(in, a, b, n);
 }
 
-struct HostMirror {
+// neighbor-build totals the host reads back in one copy before the fill
+struct NsTotals {
     unsigned long long nbrTot[3];
-    ProbeResult probe;
     U64x2 sellTot[3];
     uint64_t csrTot[3];
     uint64_t nCells[3];
+};
+__global__ void KGatherNsTotals(const U64x2* sell, const uint64_t* csr, const uint64_t* nCells,
+                                const unsigned long long* nbr, int hasRigid, NsTotals* out) {
+    const uint32_t k = threadIdx.x;
+    if (k >= 3) return;
+    out->nbrTot[k] = nbr[k];
+    out->sellTot[k] = sell[k];
+    out->csrTot[k] = hasRigid ? csr[k] : 0ull;
+    out->nCells[k] = nCells[k];
+}
+struct HostMirror {
+    NsTotals ns;
+    ProbeResult probe;
     SolverState st;
     uint32_t err;
     ContactState contact;
@@ -185,6 +198,7 @@ public:
     } sell[3];
     DBuf<U64x2> sellTot;
     DBuf<unsigned long long> nbrTot;
+    DBuf<NsTotals> nsTot;
     // count-pass rows of the fluid query ([chunk][slot][lane]); rows longer than KS_* slots make
     // the fill walk that chunk's stencil again
     static constexpr uint32_t KS_F = 64, KS_B = 48, KS_R = 16;
@@ -818,20 +832,20 @@ public:
         CK(cudaEventRecord(pev[3], s));
         const uint32_t nChunks = (nF + SELL_W - 1) / SELL_W;
         FinalizeSell3(Meta(0), Meta(1), Meta(2), nChunks, scanScratch2.p, sellTot.p, s);
-        for (int k = 0; k < 3; k++) FinalizeCsr(cntR[k].p, offR[k].p, nR, scanScratch.p, csrTot.p + k, s);
-        CK(cudaMemcpyAsync(hm->sellTot, sellTot.p, 3 * sizeof(U64x2), cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(hm->csrTot, csrTot.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(hm->nCells, nCellsDev.p, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(hm->nbrTot, nbrTot.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        if (nR)
+            for (int k = 0; k < 3; k++) FinalizeCsr(cntR[k].p, offR[k].p, nR, scanScratch.p, csrTot.p + k, s);
+        nsTot.ensure(1);
+        KGatherNsTotals<<<1, 32, 0, s>>>(sellTot.p, csrTot.p, nCellsDev.p, nbrTot.p, nR ? 1 : 0, nsTot.p);
+        CK(cudaMemcpyAsync(&hm->ns, nsTot.p, sizeof(NsTotals), cudaMemcpyDeviceToHost, s));
         CK(cudaEventRecord(pev[4], s));
         Sync();
         for (int k = 0; k < 3; k++) {
-            nNbr[k] = nF ? hm->nbrTot[k] : 0;
-            sell[k].n16 = hm->sellTot[k].a;
-            sell[k].n32 = hm->sellTot[k].b;
+            nNbr[k] = nF ? hm->ns.nbrTot[k] : 0;
+            sell[k].n16 = hm->ns.sellTot[k].a;
+            sell[k].n32 = hm->ns.sellTot[k].b;
             sell[k].l16.grow(sell[k].n16, LIST_GROWTH);
             sell[k].l32.grow(sell[k].n32, LIST_GROWTH);
-            csrN[k] = hm->csrTot[k];
+            csrN[k] = hm->ns.csrTot[k];
             listR[k].grow(csrN[k], LIST_GROWTH);
         }
         m0 = Meta(0); m1 = Meta(1); m2 = Meta(2);
@@ -839,7 +853,7 @@ public:
         LaunchQueryFluid(true, qa, m0, m1, m2, s);
         LaunchQueryRigid(true, qa, rl, s);
         CK(cudaEventRecord(pev[5], s));
-        launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + FinalizeSell3Launches(nChunks) + (nR ? 9u : 0u);
+        launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + FinalizeSell3Launches(nChunks) + (nR ? 9u : 0u) + 1u;
         listsValid = true;
     }
     QueryArgs MakeQueryArgs() {
@@ -1466,8 +1480,8 @@ public:
         o.cellOrig[0] = fr.ox; o.cellOrig[1] = fr.oy; o.cellOrig[2] = fr.oz;
         o.cellDims[0] = fr.nx; o.cellDims[1] = fr.ny; o.cellDims[2] = fr.nz;
         o.keyBits = fr.keyBits;
-        o.nCellsF = nF ? (uint32_t)hm->nCells[0] : 0; o.nCellsB = nB ? (uint32_t)hm->nCells[1] : 0;
-        o.nCellsR = nR ? (uint32_t)hm->nCells[2] : 0;
+        o.nCellsF = nF ? (uint32_t)hm->ns.nCells[0] : 0; o.nCellsB = nB ? (uint32_t)hm->ns.nCells[1] : 0;
+        o.nCellsR = nR ? (uint32_t)hm->ns.nCells[2] : 0;
         const bool lv = listsValid && nF;
         o.nNbrFF = lv ? nNbr[0] : 0; o.nNbrFB = lv ? nNbr[1] : 0; o.nNbrFR = lv ? nNbr[2] : 0;
         o.nNbrRF = csrN[0]; o.nNbrRB = csrN[1]; o.nNbrRR = csrN[2];

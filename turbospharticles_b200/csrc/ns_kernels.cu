@@ -793,6 +793,7 @@ __global__ void __launch_bounds__(SELL3_THREADS) KFinalizeSell3(SellMeta m0, Sel
     const uint32_t seg = (nChunks + SELL3_THREADS - 1) / SELL3_THREADS;
     const uint32_t beg = min(t * seg, nChunks), end = min(beg + seg, nChunks);
     U64x2 own{0, 0};
+#pragma unroll 8
     for (uint32_t c = beg; c < end; c++) {
         const uint64_t sz = (uint64_t)m.pitch[c] * SELL_W;
         if (m.format[c] == FMT_DELTA16X2) own.a += sz;
@@ -814,6 +815,7 @@ __global__ void __launch_bounds__(SELL3_THREADS) KFinalizeSell3(SellMeta m0, Sel
     U64x2 run = pre + incl;
     run.a -= own.a;
     run.b -= own.b;
+#pragma unroll 8
     for (uint32_t c = beg; c < end; c++) {
         const uint64_t sz = (uint64_t)m.pitch[c] * SELL_W;
         if (m.format[c] == FMT_DELTA16X2) { m.offset[c] = run.a; run.a += sz; }
