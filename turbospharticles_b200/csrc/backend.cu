@@ -107,7 +107,26 @@ __global__ void KGatherNsTotals(const U64x2* sell, const uint64_t* csr, const ui
     out->csrTot[k] = hasRigid ? csr[k] : 0ull;
     out->nCells[k] = nCells[k];
 }
+// end-of-step read-back in one copy: solver state, the frame probe of the new positions (the
+// accumulator is reset for the next probe by the same kernel) and the error flags
+struct StepEnd {
+    SolverState st;
+    ProbeResult probe;
+    uint32_t err;
+    uint32_t pad;
+};
+__global__ void KStepEnd(const SolverState* st, ProbeResult* probe, int takeProbe, const uint32_t* err,
+                         StepEnd* out, ProbeResult init) {
+    if (threadIdx.x != 0) return;
+    if (st) out->st = *st;
+    if (takeProbe) {
+        out->probe = *probe;
+        *probe = init;
+    }
+    out->err = *err;
+}
 struct HostMirror {
+    StepEnd se;
     NsTotals ns;
     ProbeResult probe;
     SolverState st;
@@ -199,6 +218,7 @@ public:
     DBuf<U64x2> sellTot;
     DBuf<unsigned long long> nbrTot;
     DBuf<NsTotals> nsTot;
+    DBuf<StepEnd> stepEnd;
     // count-pass rows of the fluid query ([chunk][slot][lane]); rows longer than KS_* slots make
     // the fill walk that chunk's stencil again
     static constexpr uint32_t KS_F = 64, KS_B = 48, KS_R = 16;
@@ -284,6 +304,7 @@ public:
             hm->probeInit.mnKey[a] = OrderedIntHost(3.402823466e38f);
             hm->probeInit.mxKey[a] = OrderedIntHost(-3.402823466e38f);
         }
+        stepEnd.ensure(1);
         st.ensure(1);
         err.ensure(1);
         probe.ensure(1);
@@ -293,6 +314,8 @@ public:
         csrTot.ensure(3);
         CK(cudaMemset(st.p, 0, sizeof(SolverState)));
         CK(cudaMemset(err.p, 0, sizeof(uint32_t)));
+        // the probe accumulator holds the empty bounds whenever no probe is in flight
+        CK(cudaMemcpy(probe.p, &hm->probeInit, sizeof(ProbeResult), cudaMemcpyHostToDevice));
         for (auto& e : ev) CK(cudaEventCreate(&e));
         for (auto& e : pev) CK(cudaEventCreate(&e));
     }
@@ -317,8 +340,10 @@ public:
     void CheckErrors() {
         CK(cudaMemcpyAsync(&hm->err, err.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         Sync();
+        RaiseErrors(hm->err);
+    }
+    void RaiseErrors(uint32_t e) {
         CK(cudaGetLastError());
-        const uint32_t e = hm->err;
         if (!e) return;
         CK(cudaMemsetAsync(err.p, 0, sizeof(uint32_t), s));
         if (e & (ERR_RIGID_ORIENT | ERR_RIGID_ATTACH))
@@ -687,10 +712,11 @@ public:
     // UpdateCellFrame (neighbor_search.cpp:1902-2006); returns true when the frame changed
     bool UpdateFrame() {
         if (nF == 0 && nB == 0 && nR == 0) { frameValid = false; return false; }
-        const ProbeResult init = hm->probeInit;
         if (!probeFresh) {
             QueueProbe();
+            QueueStepEnd(false, true);
             Sync();
+            hm->probe = hm->se.probe;
         }
         probeFresh = false;
         ProbeResult pr = hm->probe;
@@ -698,12 +724,11 @@ public:
         for (int a = 0; a < 3; a++) { mn[a] = OrderedIntToFloat(pr.mnKey[a]); mx[a] = OrderedIntToFloat(pr.mxKey[a]); }
         if (nB && !bAabbValid) {
             // boundary particles never move: their bounds are probed once per import
-            hm->probe = init;
-            CK(cudaMemcpyAsync(probe.p, &hm->probe, sizeof(ProbeResult), cudaMemcpyHostToDevice, s));
             LaunchProbe(posB.p, nB, fr, false, dom, probe.p, s);
-            CK(cudaMemcpyAsync(&hm->probe, probe.p, sizeof(ProbeResult), cudaMemcpyDeviceToHost, s));
+            QueueStepEnd(false, true);
             Sync();
-            for (int a = 0; a < 3; a++) { bMin[a] = OrderedIntToFloat(hm->probe.mnKey[a]); bMax[a] = OrderedIntToFloat(hm->probe.mxKey[a]); }
+            const ProbeResult& bp = hm->se.probe;
+            for (int a = 0; a < 3; a++) { bMin[a] = OrderedIntToFloat(bp.mnKey[a]); bMax[a] = OrderedIntToFloat(bp.mxKey[a]); }
             bAabbValid = true;
         }
         bool rebuild = !frameValid;
@@ -738,13 +763,18 @@ public:
         gridCells = cells;
         return true;
     }
-    // probe of the fluid and rigid positions into hm->probe (valid after the stream passes it)
+    // queue the read-back of the solver state (when st), the accumulated probe (reset for the
+    // next probe) and the error flags into hm->se, one copy
+    void QueueStepEnd(bool withState, bool withProbe) {
+        KStepEnd<<<1, 32, 0, s>>>(withState ? st.p : nullptr, probe.p, withProbe ? 1 : 0, err.p, stepEnd.p, hm->probeInit);
+        CK(cudaMemcpyAsync(&hm->se, stepEnd.p, sizeof(StepEnd), cudaMemcpyDeviceToHost, s));
+        launches += 1;
+    }
+    // probe of the fluid and rigid positions, read back into hm->se.probe
     void QueueProbe() {
-        CK(cudaMemcpyAsync(probe.p, &hm->probeInit, sizeof(ProbeResult), cudaMemcpyHostToDevice, s));
         LaunchProbe(posP.p, nF, fr, frameValid, dom, probe.p, s);
         LaunchProbe(posR.p, nR, fr, frameValid, dom, probe.p, s);
         launches += (nF ? 1 : 0) + (nR ? 1 : 0);
-        CK(cudaMemcpyAsync(&hm->probe, probe.p, sizeof(ProbeResult), cudaMemcpyDeviceToHost, s));
     }
     void EnsureNsScratch() {
         const uint32_t nMax = std::max(nF, std::max(nB, nR));
@@ -1209,12 +1239,16 @@ public:
         }
         CK(cudaEventRecord(pev[11], s));
         probeFresh = false;
-        if (frameValid) QueueProbe();  // the next step's frame rule reads it with this read-back
-        CK(cudaMemcpyAsync(&hm->st, st.p, sizeof(SolverState), cudaMemcpyDeviceToHost, s));
+        const bool probeNext = frameValid;  // the next step's frame rule reads it with this read-back
+        if (probeNext) QueueProbe();
+        QueueStepEnd(true, probeNext);
         launches += (nF ? 6u : 0u) + (nRB ? 13u : 0u);
         CK(cudaEventRecord(pev[12], s));
-        CheckErrors();
-        probeFresh = frameValid;
+        Sync();
+        hm->st = hm->se.st;
+        if (probeNext) hm->probe = hm->se.probe;
+        RaiseErrors(hm->se.err);
+        probeFresh = probeNext;
         float t = 0.f;
         cudaEventElapsedTime(&t, ev[0], pev[12]); lastStepMs = t;
         cudaEventElapsedTime(&t, ev[0], ev[1]); lastNbrMs = t;

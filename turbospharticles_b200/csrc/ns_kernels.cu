@@ -70,7 +70,21 @@ __global__ void __launch_bounds__(256) KProbe(const float4* __restrict__ pos, ui
             mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], d));
         }
     exceeded = __any_sync(0xffffffffu, exceeded);
+    // block reduction first: one set of global atomics per block, not per warp (the atomics on
+    // the seven shared words were the probe's cost)
+    __shared__ float smn[3][8], smx[3][8];
+    __shared__ uint32_t sex[8];
+    const uint32_t warp = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
+        for (int a = 0; a < 3; a++) { smn[a][warp] = mn[a]; smx[a][warp] = mx[a]; }
+        sex[warp] = exceeded;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t w = 1; w < (blockDim.x >> 5); w++) {
+            for (int a = 0; a < 3; a++) { mn[a] = fminf(mn[a], smn[a][w]); mx[a] = fmaxf(mx[a], smx[a][w]); }
+            exceeded |= sex[w];
+        }
         for (int a = 0; a < 3; a++) {
             atomicMin(&out->mnKey[a], OrderedInt(mn[a]));
             atomicMax(&out->mxKey[a], OrderedInt(mx[a]));
@@ -82,7 +96,7 @@ __global__ void __launch_bounds__(256) KProbe(const float4* __restrict__ pos, ui
 void LaunchProbe(const float4* pos, uint32_t n, const Frame& fr, bool frameValid, const DomainBox& dom,
                  ProbeResult* out, cudaStream_t s) {
     if (n == 0) return;
-    const uint32_t blocks = std::min<uint32_t>((n + 255) / 256, 148u * 8u);
+    const uint32_t blocks = std::min<uint32_t>((n + 255) / 256, 148u * 4u);
     KProbe<<<blocks, 256, 0, s>>>(pos, n, fr, frameValid ? 1 : 0, dom, out);
 }
 
