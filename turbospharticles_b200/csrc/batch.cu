@@ -69,11 +69,11 @@ __global__ void __launch_bounds__(256) KBatchProbe(const float4* __restrict__ po
                                                   const uint32_t* __restrict__ chunkScene,
                                                   const BatchSceneDev* __restrict__ sc, ProbeResult* __restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t chunk = i >> 5, lane = i & 31;
-    if (chunk >= nChunks) return;  // whole warps
-    const uint32_t s = chunkScene[chunk];
-    const BatchSceneDev& d = sc[s];
-    const bool act = lane < (uint32_t)chunkLen[chunk];
+    const uint32_t chunk = i >> 5, lane = i & 31, warp = threadIdx.x >> 5;
+    const bool live = chunk < nChunks;  // whole warps
+    const uint32_t s = live ? chunkScene[chunk] : EMPTY_32;
+    const BatchSceneDev& d = sc[live ? s : 0u];
+    const bool act = live && lane < (uint32_t)chunkLen[chunk];
     float mn[3] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
     float mx[3] = {-3.402823466e38f, -3.402823466e38f, -3.402823466e38f};
     uint32_t exceeded = 0;
@@ -103,12 +103,33 @@ __global__ void __launch_bounds__(256) KBatchProbe(const float4* __restrict__ po
             mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], dd));
         }
     exceeded = __any_sync(0xffffffffu, exceeded);
+    // the block's warps merged per scene (a scene's chunks are contiguous, so a block mostly
+    // holds one or two scenes), then one set of global atomics per scene run
+    __shared__ float smn[3][8], smx[3][8];
+    __shared__ uint32_t sex[8], ssc[8];
     if (lane == 0) {
-        for (int a = 0; a < 3; a++) {
-            atomicMin(&out[s].mnKey[a], OrderedIntDev(mn[a]));
-            atomicMax(&out[s].mxKey[a], OrderedIntDev(mx[a]));
+        for (int a = 0; a < 3; a++) { smn[a][warp] = mn[a]; smx[a][warp] = mx[a]; }
+        sex[warp] = exceeded;
+        ssc[warp] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const uint32_t nw = blockDim.x >> 5;
+    for (uint32_t w = 0; w < nw;) {
+        const uint32_t cs = ssc[w];
+        if (cs == EMPTY_32) break;
+        float a0[3], a1[3];
+        uint32_t ex = 0;
+        for (int a = 0; a < 3; a++) { a0[a] = smn[a][w]; a1[a] = smx[a][w]; }
+        for (; w < nw && ssc[w] == cs; w++) {
+            for (int a = 0; a < 3; a++) { a0[a] = fminf(a0[a], smn[a][w]); a1[a] = fmaxf(a1[a], smx[a][w]); }
+            ex |= sex[w];
         }
-        if (exceeded) atomicOr(&out[s].exceeded, 1u);
+        for (int a = 0; a < 3; a++) {
+            atomicMin(&out[cs].mnKey[a], OrderedIntDev(a0[a]));
+            atomicMax(&out[cs].mxKey[a], OrderedIntDev(a1[a]));
+        }
+        if (ex) atomicOr(&out[cs].exceeded, 1u);
     }
 }
 
