@@ -49,6 +49,16 @@ constexpr uint32_t SPH_THREADS = 256;
 #ifndef TSP_JACOBI_MIN_BLOCKS
 #define TSP_JACOBI_MIN_BLOCKS 4
 #endif
+// density sweep: minimum resident blocks per SM, and FF slots per group of the non-pressure and
+// source/diagonal sweeps; measured on the 1M dam (ms per launch): KDensity at 5 (no bound) / 6 /
+// 8 blocks 0.120 / 0.100 / 0.097; KNonPressure / KSourceDiagInit with 4 / 3 / 2 slots 0.186 /
+// 0.175 / 0.176 and 0.149 / 0.147 / 0.138
+#ifndef TSP_DENSITY_MIN_BLOCKS
+#define TSP_DENSITY_MIN_BLOCKS 8
+#endif
+#ifndef TSP_NPSD_FF_SLOTS
+#define TSP_NPSD_FF_SLOTS 2
+#endif
 
 struct ChunkCursor {
     uint32_t pitch, cnt, base, base2;
@@ -215,7 +225,7 @@ struct SlicePrefetch {
         if (pf_.issue(nv, lane), pf_.load(nv, chunk + 2u * warps_, nChunks_, lane), true)
 
 // ----------------------------------------------------------------------------- density
-__global__ void __launch_bounds__(SPH_THREADS) KDensity(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv) {
+__global__ void __launch_bounds__(SPH_THREADS, TSP_DENSITY_MIN_BLOCKS) KDensity(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv) {
     FOR_EACH_CHUNK_PF(f.n, nv) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = LaneActive(f, chunk, lane, i);
@@ -249,7 +259,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KNonPressure(
         float fx = 0.f, fy = 0.f, fz = 0.f, bx = 0.f, by = 0.f, bz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<TSP_SPH_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velRho, [&](uint32_t, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<TSP_NPSD_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velRho, [&](uint32_t, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -301,7 +311,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagIn
         float cxB = 0.f, cyB = 0.f, czB = 0.f, cxR = 0.f, cyR = 0.f, czR = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<TSP_SPH_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velPred, [&](uint32_t k, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<TSP_NPSD_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velPred, [&](uint32_t k, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
