@@ -571,8 +571,13 @@ __device__ __forceinline__ void HomeStatsFromScratch(const uint32_t* scr, LaneRe
     }
 }
 
-// count pass: neighbor counts, chunk compression meta, rows into the per-chunk scratch
-__global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidCount(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
+// count pass: neighbor counts, chunk compression meta, rows into the per-chunk scratch.
+// Minimum resident blocks per SM, measured on the 1M dam (ms per count pass): 1 (78 registers)
+// 0.393, none given (64 registers) 0.350, 9 (56) 0.332, 10 (48) 0.348, 12 (40, spills) 0.338
+#ifndef TSP_QUERY_MIN_BLOCKS
+#define TSP_QUERY_MIN_BLOCKS 9
+#endif
+__global__ void __launch_bounds__(QUERY_THREADS, TSP_QUERY_MIN_BLOCKS) KQueryFluidCount(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
     extern __shared__ uint2 qsm[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t chunk = blockIdx.x * (QUERY_THREADS / 32) + warp;
@@ -658,7 +663,12 @@ __device__ __forceinline__ void EncodeFromScratch(const SellMeta& m, LaneWriter&
 }
 
 // fill pass: scratch rows -> SELL32 (a chunk whose scratch overflowed walks its stencil again)
-__global__ void __launch_bounds__(QUERY_THREADS) KQueryFluidFill(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
+// fill pass: minimum resident blocks per SM, measured on the 1M dam (ms per fill pass):
+// none given 0.088, 8 0.086, 10 0.084, 12 0.095, 16 0.103
+#ifndef TSP_FILL_MIN_BLOCKS
+#define TSP_FILL_MIN_BLOCKS 10
+#endif
+__global__ void __launch_bounds__(QUERY_THREADS, TSP_FILL_MIN_BLOCKS) KQueryFluidFill(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
     extern __shared__ uint2 qsm[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t chunk = blockIdx.x * (QUERY_THREADS / 32) + warp;
