@@ -59,6 +59,10 @@ constexpr uint32_t SPH_THREADS = 256;
 #ifndef TSP_NPSD_FF_SLOTS
 #define TSP_NPSD_FF_SLOTS 2
 #endif
+// non-pressure sweep with 2-slot groups: 4 / 5 / 6 blocks per SM 0.177 / 0.173 / 0.180 ms
+#ifndef TSP_NP_MIN_BLOCKS
+#define TSP_NP_MIN_BLOCKS 5
+#endif
 
 struct ChunkCursor {
     uint32_t pitch, cnt, base, base2;
@@ -249,7 +253,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_DENSITY_MIN_BLOCKS) KDensity(
 }
 
 // ----------------------------------------------------------------------------- non-pressure
-__global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+__global__ void __launch_bounds__(SPH_THREADS, TSP_NP_MIN_BLOCKS) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
     FOR_EACH_CHUNK_PF(f.n, nv) {
         const uint32_t i = chunk * SELL_W + lane;
