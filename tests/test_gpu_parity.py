@@ -171,6 +171,24 @@ def test_gpu_neighbor_search_bit_exact(dist, n):
     assert_neighbor_structures_equal(g, o, st.N_F, 0, 0)
 
 
+def test_gpu_neighbor_lists_grow_between_builds():
+    """A build whose lists outgrow the buffers sized by the previous build (a sparse first
+    scene keeps them small): the buffers grow in place and the structures are still bit-exact
+    with the oracle."""
+    st, dmin, dmax, p = S.neighbor_search_scene(1 << 20, "uniform", seed=7)
+    sparse = st.copy()
+    for c in ("xPosF", "yPosF", "zPosF"):
+        setattr(sparse, c, (getattr(st, c) * np.float32(3.0)).astype(np.float32))
+    g, o = pair(p)
+    g.set_sim_domain_bounds(np.asarray(dmin, np.float32) * 3, np.asarray(dmax, np.float32) * 3)
+    g.pull(sparse, p)
+    g.neighbor_search(p)
+    load((g, o), st, p, dmin, dmax)
+    g.neighbor_search(p)
+    o.neighbor_search(p)
+    assert_neighbor_structures_equal(g, o, st.N_F, 0, 0)
+
+
 def test_gpu_neighbor_search_4m_properties():
     """4,194,304 uniform points (the oracle is not run at this size): size-independent
     properties -- FF rows ascending, self included exactly for in-frame particles, the FF
