@@ -91,7 +91,7 @@ void LaunchUnpack2(const float2* in, float* a, float* b, uint32_t n, cudaStream_
     if (n) KUnpack2<<<G(n), 256, 0, s>>>(in, a, b, n);
 }
 
-// neighbor-build totals the host reads back in one copy before the fill
+// neighbor-build totals the host reads before the fill (written into mapped pinned memory)
 struct NsTotals {
     unsigned long long nbrTot[3];
     U64x2 sellTot[3];
@@ -107,8 +107,9 @@ __global__ void KGatherNsTotals(const U64x2* sell, const uint64_t* csr, const ui
     out->csrTot[k] = hasRigid ? csr[k] : 0ull;
     out->nCells[k] = nCells[k];
 }
-// end-of-step read-back in one copy: solver state, the frame probe of the new positions (the
-// accumulator is reset for the next probe by the same kernel) and the error flags
+// end-of-step read-back, written by one thread straight into mapped pinned host memory: solver
+// state, the frame probe of the new positions (the accumulator is reset for the next probe by
+// the same kernel) and the error flags
 struct StepEnd {
     SolverState st;
     ProbeResult probe;
@@ -217,8 +218,8 @@ public:
     } sell[3];
     DBuf<U64x2> sellTot;
     DBuf<unsigned long long> nbrTot;
-    DBuf<NsTotals> nsTot;
-    DBuf<StepEnd> stepEnd;
+    StepEnd* seDev = nullptr;   // device view of hm->se (mapped pinned memory)
+    NsTotals* nsDev = nullptr;  // device view of hm->ns
     // count-pass rows of the fluid query ([chunk][slot][lane]); rows longer than KS_* slots make
     // the fill walk that chunk's stencil again
     static constexpr uint32_t KS_F = 64, KS_B = 48, KS_R = 16;
@@ -298,13 +299,15 @@ public:
         CK(cudaStreamCreateWithFlags(&capStream, cudaStreamNonBlocking));
         CK(cudaStreamCreateWithFlags(&xs, cudaStreamNonBlocking));
         for (auto& e : xev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        CK(cudaMallocHost(&hm, sizeof(HostMirror)));
+        CK(cudaHostAlloc((void**)&hm, sizeof(HostMirror), cudaHostAllocMapped | cudaHostAllocPortable));
         std::memset(hm, 0, sizeof(HostMirror));
         for (int a = 0; a < 3; a++) {  // (neighbor_search.cpp:205-213)
             hm->probeInit.mnKey[a] = OrderedIntHost(3.402823466e38f);
             hm->probeInit.mxKey[a] = OrderedIntHost(-3.402823466e38f);
         }
-        stepEnd.ensure(1);
+        // the step-end and neighbor-total gathers write straight into this pinned host memory
+        CK(cudaHostGetDevicePointer((void**)&seDev, &hm->se, 0));
+        CK(cudaHostGetDevicePointer((void**)&nsDev, &hm->ns, 0));
         st.ensure(1);
         err.ensure(1);
         probe.ensure(1);
@@ -766,8 +769,7 @@ public:
     // queue the read-back of the solver state (when st), the accumulated probe (reset for the
     // next probe) and the error flags into hm->se, one copy
     void QueueStepEnd(bool withState, bool withProbe) {
-        KStepEnd<<<1, 32, 0, s>>>(withState ? st.p : nullptr, probe.p, withProbe ? 1 : 0, err.p, stepEnd.p, hm->probeInit);
-        CK(cudaMemcpyAsync(&hm->se, stepEnd.p, sizeof(StepEnd), cudaMemcpyDeviceToHost, s));
+        KStepEnd<<<1, 32, 0, s>>>(withState ? st.p : nullptr, probe.p, withProbe ? 1 : 0, err.p, seDev, hm->probeInit);
         launches += 1;
     }
     // probe of the fluid and rigid positions, read back into hm->se.probe
@@ -864,9 +866,7 @@ public:
         FinalizeSell3(Meta(0), Meta(1), Meta(2), nChunks, scanScratch2.p, sellTot.p, s);
         if (nR)
             for (int k = 0; k < 3; k++) FinalizeCsr(cntR[k].p, offR[k].p, nR, scanScratch.p, csrTot.p + k, s);
-        nsTot.ensure(1);
-        KGatherNsTotals<<<1, 32, 0, s>>>(sellTot.p, csrTot.p, nCellsDev.p, nbrTot.p, nR ? 1 : 0, nsTot.p);
-        CK(cudaMemcpyAsync(&hm->ns, nsTot.p, sizeof(NsTotals), cudaMemcpyDeviceToHost, s));
+        KGatherNsTotals<<<1, 32, 0, s>>>(sellTot.p, csrTot.p, nCellsDev.p, nbrTot.p, nR ? 1 : 0, nsDev);
         CK(cudaEventRecord(pev[4], s));
         Sync();
         for (int k = 0; k < 3; k++) {
