@@ -424,14 +424,21 @@ int tsp_b200_try_build_cell_frame(const int64_t cell_min[3], const int64_t cell_
  * 0xFFFFFFFFFFFFFFFF and sort last, as tsp_b200_read_cell_ids returns them). Output, all
  * device memory: d_unique_out[c] = cell ID of run c (room for n), d_start_out[c] = index of
  * the first particle of run c plus d_start_out[num_cells] = n (room for n + 1), and
- * *d_num_cells_out = num_cells. Outputs need not be zeroed, and nothing has to start at zero.
+ * *d_num_cells_out = num_cells. For n = 0 only *d_num_cells_out = 0 and, when d_start_out is
+ * not NULL, d_start_out[0] = 0 are written. Outputs need not be zeroed, and nothing has to
+ * start at zero.
  * Work is queued on `stream` (a cudaStream_t; NULL = legacy default stream); results are
  * ready when that stream reaches them.
  *
- * Setup: the first call on a device looks up the scratch's device address for that device
- * (cudaGetSymbolAddress, which may load this library's device code there). Call
- * tsp_b200_noalloc_setup() with each device current once during setup -- before any stream
- * capture or time-critical section -- so later calls only launch kernels.
+ * Setup: tsp_b200_noalloc_setup(), called once per device with that device current, looks up
+ * the scratch's device address there (cudaGetSymbolAddress) and runs one tiny build on the
+ * legacy default stream, waiting for it, so that this library's device code, scan kernels
+ * included, is loaded on that device (under lazy module loading, the CUDA 12 default, code is
+ * otherwise loaded at first use, which takes device memory). Call it during setup, before any
+ * time-critical section; later calls then only queue kernels. A call on a device without
+ * setup does the same set-up first.
+ * Errors: an error that the caller's earlier work left pending is not reported (nor cleared)
+ * by a call; a launch error of the call itself is reported as TSP_ERR_CUDA.
  * Limit: n <= TSP_NOALLOC_MAX_PARTICLES; larger n returns TSP_ERR_INVALID and queues nothing.
  * Races: all calls on one device share the scratch, so calls must not overlap in time on that
  * device (issue them on one stream, or order them with events).

@@ -5,8 +5,8 @@
 // meaning (a parameter struct by const reference per call, the universal SoA state for
 // pull/push) and the same error behaviour (failures throw std::runtime_error, like
 // GPU::Check in source/simulation/GPU/gpu_utils.h:24-45). It depends only on tsp_b200.h;
-// INTEGRATION.md shows the few lines that make it a `Sim::I_SimBackend` inside the
-// reference tree.
+// deriving a class from both `Sim::I_SimBackend` and this one, with each interface method
+// forwarding to the method of the same name, makes it a backend of the reference tree.
 #pragma once
 
 #include <cstdint>

@@ -29,7 +29,7 @@ namespace {
 // uint64 partial per 1024-item tile plus one (16,385 words = 128 KiB for 2^24 particles).
 constexpr uint32_t kNoAllocMaxParticles = TSP_NOALLOC_MAX_PARTICLES;
 constexpr uint64_t kNoAllocScratchItems = (kNoAllocMaxParticles + SCAN_TILE - 1) / SCAN_TILE + 1;
-static_assert(kNoAllocScratchItems >= 2, "scratch holds at least one tile partial and the total slot");
+static_assert(kNoAllocScratchItems >= 12, "scratch holds the setup build's partial, input and outputs");
 
 // One scratch per device (each device that loads this library has its own copy of a
 // __device__ variable). Nothing in it has to start at zero: each call writes every word it
@@ -47,9 +47,10 @@ int Fail(int code, const std::string& msg) {
     return code;
 }
 
-// Device address of the scratch on the current device, looked up once per device. The lookup
-// may load the library's device code on that device, which is why it belongs in setup, before
-// any stream capture or time-critical section.
+// Device address of the scratch on the current device, looked up once per device, followed by
+// one small build that loads the scan kernels on that device. Both may load device code (and
+// so take device memory for it), which is why they belong in setup, before any time-critical
+// section. The setup build runs on the legacy default stream and waits for it.
 int ScratchForCurrentDevice(uint64_t** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
@@ -65,6 +66,19 @@ int ScratchForCurrentDevice(uint64_t** out) {
             if (e != cudaSuccess || !addr)
                 return Fail(TSP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
             p = static_cast<uint64_t*>(addr);
+            // One n = 1 build on this device, its input and outputs carved out of the scratch
+            // beyond the one tile partial it needs: with lazy module loading (the CUDA 12
+            // default) this loads the scan kernels now, so no later call loads device code.
+            uint64_t* cid = p + 8;
+            uint32_t* start = reinterpret_cast<uint32_t*>(p + 10);
+            e = cudaMemsetAsync(cid, 0, sizeof(uint64_t), 0);
+            if (e == cudaSuccess) {
+                BuildCellTable(cid, 1u, p + 9, start, p + 11, p, 0);
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+            if (e != cudaSuccess)
+                return Fail(TSP_ERR_CUDA, std::string("noalloc setup build: ") + cudaGetErrorString(e));
             g_scratchAddr[dev].store(p, std::memory_order_release);
         }
     }
@@ -95,10 +109,16 @@ int tsp_b200_build_cell_table_noalloc(const uint64_t* d_cell_ids_sorted, uint32_
     const int rc = ScratchForCurrentDevice(&scratch);
     if (rc != TSP_OK) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // an error left pending by the caller's earlier work is neither reported nor cleared here;
+    // only an error that appears with this call's launches is
+    const cudaError_t before = cudaPeekAtLastError();
+    if (n == 0 && d_start_out) cudaMemsetAsync(d_start_out, 0, sizeof(uint32_t), s);  // start[0] = n = 0
     BuildCellTable(d_cell_ids_sorted, n, d_unique_out, d_start_out, d_num_cells_out, scratch, s);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess)
-        return Fail(TSP_ERR_CUDA, std::string("tsp_b200_build_cell_table_noalloc: ") + cudaGetErrorString(e));
+    const cudaError_t after = cudaPeekAtLastError();
+    if (before == cudaSuccess && after != cudaSuccess) {
+        cudaGetLastError();
+        return Fail(TSP_ERR_CUDA, std::string("tsp_b200_build_cell_table_noalloc: ") + cudaGetErrorString(after));
+    }
     return TSP_OK;
 }
 
