@@ -13,12 +13,19 @@ compared with the oracle's through statistics with stated bounds, not particle b
   within 15 % relative + 1e-4 absolute, average velocity magnitude and kinetic energy within
   1 %, Jacobi iterations within +-3;
 - over 40 steps of the floating-cubes scene: rigid centres of mass within 1 mm, velocities within
-  2 % of the largest body speed.
+  2 % of the largest body speed;
+- the 32K dam's full run length, 1,000 steps (1 s of the collapse): at every step the GPU's
+  average positive density error is at most the solver target 0.1 % whenever the solver stopped
+  before its iteration limit, and no particle leaves the tank; every 100 steps the kinetic
+  energy is within KE_RTOL_1000 of the oracle's, the average velocity magnitude within
+  VEL_RTOL_1000, and the mean Jacobi iteration count of the last 100 steps within
+  ITERS_RTOL_1000 of the oracle's.
 """
 import numpy as np
 import pytest
 
 from oracle import OracleBackend
+from parity_util import report
 from turbospharticles_b200 import abi, scene as S
 from turbospharticles_b200.backend import SimBackendB200
 
@@ -87,3 +94,40 @@ def test_gpu_long_run_rigid_trajectories_within_bounds():
     speed = max(float(np.max(np.abs(getattr(os_, c)))) for c in ("xVelRB", "yVelRB", "zVelRB"))
     for c in ("xVelRB", "yVelRB", "zVelRB"):
         assert np.max(np.abs(getattr(gs, c).astype(np.float64) - getattr(os_, c))) <= 0.02 * speed, c
+
+
+KE_RTOL_1000 = 0.05
+VEL_RTOL_1000 = 0.05
+ITERS_RTOL_1000 = 0.25
+
+
+def test_gpu_dam_32k_full_run_1000_steps():
+    g, o, p = loaded(S.dam_32k)
+    st0 = g.push()
+    lo = np.array([min(st0.xPosB.min(), 0.0), min(st0.yPosB.min(), 0.0), min(st0.zPosB.min(), 0.0)]) - 1e-3
+    hi = np.array([st0.xPosB.max(), st0.yPosB.max(), st0.zPosB.max()]) + 1e-3
+    rows = []
+    it_g, it_o = [], []
+    for step in range(1, 1001):
+        g.step(p)
+        o.step(p)
+        sg, so = g.stats(), o.stats()
+        it_g.append(sg.solverIters)
+        it_o.append(so.solverIters)
+        if sg.solverIters < p.maxSolverIters:
+            assert sg.avgRelDensityErrPos <= float(np.float32(p.densityDevTarget)), (step, sg.avgRelDensityErrPos)
+        if step % 100 == 0:
+            gs, os_ = g.push(), o.push()
+            pos = np.stack([gs.xPosF, gs.yPosF, gs.zPosF], 1)
+            assert np.all(np.isfinite(pos)) and np.all(pos >= lo) and np.all(pos <= hi), step
+            rg, ro = g.statistics(p), o.statistics(p)
+            ke_g, ke_o = kinetic_energy(gs, p.massF), kinetic_energy(os_, p.massF)
+            mi_g, mi_o = float(np.mean(it_g[-100:])), float(np.mean(it_o[-100:]))
+            rows.append(dict(step=step, ke_gpu=ke_g, ke_oracle=ke_o, vel_gpu=rg["VelMag_Avg"],
+                             vel_oracle=ro["VelMag_Avg"], iters_gpu=mi_g, iters_oracle=mi_o,
+                             dens_err_gpu=rg["DensRelError_Pos_Avg"], dens_err_oracle=ro["DensRelError_Pos_Avg"]))
+    report("dam_32k_1000_steps", rows)
+    for r in rows:
+        assert abs(r["ke_gpu"] - r["ke_oracle"]) <= KE_RTOL_1000 * r["ke_oracle"], r
+        assert abs(r["vel_gpu"] - r["vel_oracle"]) <= VEL_RTOL_1000 * r["vel_oracle"], r
+        assert abs(r["iters_gpu"] - r["iters_oracle"]) <= ITERS_RTOL_1000 * r["iters_oracle"], r
