@@ -20,7 +20,7 @@ def written_slot_mask(meta, n_f, fmt, batch_chunks=4096):
     chunks = np.nonzero((meta["format"] == fmt) & (meta["pitch"] > 0))[0]
     if chunks.size == 0:
         return mask
-    cnt = np.zeros(chunks.max() * 32 + 32, np.int64)
+    cnt = np.zeros(max(int(chunks.max()) * 32 + 32, n_f), np.int64)
     cnt[:n_f] = meta["counts"][:n_f]
     off = meta["offset"].astype(np.int64)
     pitch = meta["pitch"].astype(np.int64)

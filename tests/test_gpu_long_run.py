@@ -96,9 +96,11 @@ def test_gpu_long_run_rigid_trajectories_within_bounds():
         assert np.max(np.abs(getattr(gs, c).astype(np.float64) - getattr(os_, c))) <= 0.02 * speed, c
 
 
-KE_RTOL_1000 = 0.05
-VEL_RTOL_1000 = 0.05
-ITERS_RTOL_1000 = 0.25
+# measured on a B200: kinetic energy within 0.31 %, average speed within 0.2 %, mean iteration
+# counts within 0.7 % of the oracle's at every 100th step
+KE_RTOL_1000 = 0.02
+VEL_RTOL_1000 = 0.01
+ITERS_RTOL_1000 = 0.1
 
 
 def test_gpu_dam_32k_full_run_1000_steps():

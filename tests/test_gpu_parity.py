@@ -195,16 +195,15 @@ def test_gpu_stages_match_oracle_from_identical_state():
     for be in (g, o):
         be.neighbor_search(p)
     # identical start state for every stage (fields copied from the oracle); element-wise
-    # bounds rtol * |oracle| + atol with physical floors: density and source term 1e-3 kg/m^3,
-    # predicted velocity 1e-5 g dt, pressure 1e-2 Pa, pressure acceleration 1e-5 g, the
-    # diagonal 1e-6 of its largest magnitude
-    dscale = None
+    # bounds rtol * |oracle| + atol with floors: density and source term 1e-3 kg/m^3, predicted
+    # velocity 1e-5 g dt, pressure 1e-2 Pa; the diagonal and the pressure acceleration, sums of
+    # cancelling terms, 1e-6 of their largest magnitude
     for stage, fields in (
             (abi.STAGE_DENSITY, [(abi.FIELD_DENSITY, 2e-6, 1e-3)]),
             (abi.STAGE_NON_PRESSURE, [(abi.FIELD_VEL_PRED, 2e-6, 1e-5 * 9.81 * 1e-3)]),
             (abi.STAGE_SOURCE_DIAG_INIT, [(abi.FIELD_SOURCE, 1e-4, 1e-3), (abi.FIELD_DIAG, 2e-5, None),
                                           (abi.FIELD_PRESSURE, 1e-4, 1e-2)]),
-            (abi.STAGE_PRESSURE_ACC, [(abi.FIELD_ACC_PRESS, 1e-4, 1e-5 * 9.81)]),
+            (abi.STAGE_PRESSURE_ACC, [(abi.FIELD_ACC_PRESS, 1e-4, None)]),
             (abi.STAGE_JACOBI_UPDATE, [(abi.FIELD_PRESSURE, 1e-4, 1e-2)])):
         for f in (abi.FIELD_DENSITY, abi.FIELD_VEL_PRED, abi.FIELD_SOURCE, abi.FIELD_DIAG, abi.FIELD_PRESSURE,
                   abi.FIELD_ACC_PRESS):
@@ -214,8 +213,7 @@ def test_gpu_stages_match_oracle_from_identical_state():
         for f, rtol, atol in fields:
             ref = o.read_field(f)
             if atol is None:
-                dscale = float(np.abs(ref).max())
-                atol = 1e-6 * dscale
+                atol = 1e-6 * float(np.abs(ref).max())
             assert_elementwise(g.read_field(f), ref, rtol, atol, f"stage {stage} field {f}")
         if stage == abi.STAGE_JACOBI_UPDATE:
             assert_elementwise(eg, eo, 1e-9, 0.0, "FP64 error sums")
@@ -239,9 +237,9 @@ def test_gpu_steps_match_oracle():
         s1 = k + 1
         for name, rtol, atol in (("densityF", 1e-5 * s1, 1e-2 * s1), ("pressureF", 1e-3 * s1, 1.0 * s1),
                                  ("xPosF", 1e-6, 1e-7 * s1), ("yVelF", 1e-3 * s1, 1e-5 * s1),
-                                 ("xAccPressF", 1e-3 * s1, 1e-3 * s1), ("sourceTermF", 1e-3 * s1, 1e-2 * s1),
+                                 ("xAccPressF", 1e-3 * s1, None), ("sourceTermF", 1e-3 * s1, 1e-2 * s1),
                                  ("diagElemF", 1e-4 * s1, None)):
             ref = getattr(os_, name)
-            if atol is None:
+            if atol is None:  # sums of cancelling terms: floor relative to the field's magnitude
                 atol = 1e-5 * float(np.abs(ref).max()) * s1
             assert_elementwise(getattr(gs, name), ref, rtol, atol, f"step {k} {name}")

@@ -10,9 +10,15 @@ from the FP32 oracle before the stage) and its output is compared element by ele
 - against the FP64 oracle run on the same FP32 inputs: the FP32 error of the stage, asserted
   against the north-star 1e-4 relative with the field's stated absolute floor.
 
-Floors (atol) are physical: density, source term 1e-3 kg/m^3 (1e-6 of the rest density);
-pressure 1e-2 Pa; accelerations and velocities 1e-5 of g; the diagonal a_ii 1e-6 of its
-largest magnitude in the scene. Below a floor a value is compared in absolute terms.
+Floors (atol): density, source term 1e-3 kg/m^3 (1e-6 of the rest density); pressure 1e-2 Pa;
+predicted velocity 1e-5 g dt; the diagonal a_ii and the pressure acceleration, sums of
+cancelling terms, 1e-6 of their largest magnitude in the scene. Below a floor a value is
+compared in absolute terms.
+
+Measured on a B200 (largest relative error above the floor, GPU against the FP64 oracle):
+density 5.2e-7, predicted velocity 6.3e-7, source term 6.2e-7, diagonal 1.2e-6, initial
+pressure 3.2e-5, pressure acceleration 9.3e-5, pressure after one Jacobi update 3.4e-6 and after
+1 / 3 / 10 sweeps 4.8e-5 / 4.4e-5 / 6.1e-5; FP64 error sums 3.2e-9 relative.
 """
 import numpy as np
 import pytest
@@ -37,9 +43,9 @@ STAGES = ((abi.STAGE_DENSITY, (abi.FIELD_DENSITY,)),
           (abi.STAGE_JACOBI_UPDATE, (abi.FIELD_PRESSURE,)))
 
 
-def floors(diag_scale):
+def floors(diag_scale, acc_scale):
     return {abi.FIELD_DENSITY: 1e-3, abi.FIELD_VEL_PRED: 1e-5 * G * 5e-4, abi.FIELD_SOURCE: 1e-3,
-            abi.FIELD_DIAG: 1e-6 * diag_scale, abi.FIELD_PRESSURE: 1e-2, abi.FIELD_ACC_PRESS: 1e-5 * G}
+            abi.FIELD_DIAG: 1e-6 * diag_scale, abi.FIELD_PRESSURE: 1e-2, abi.FIELD_ACC_PRESS: 1e-6 * acc_scale}
 
 
 # element-wise relative bound against the FP32 oracle, per field (floors above)
@@ -81,7 +87,7 @@ def stage_reports(developed):
     assert np.array_equal(g.push().idF, ids_o)
     to_d = np.argsort(ids_o)[np.searchsorted(ids_o[np.argsort(ids_o)], ids_d)]  # d order -> o index
     from_d = np.argsort(to_d)
-    diag_scale = None
+    diag_scale = acc_scale = None
     out = {}
     for stage, fields in STAGES:
         for f in FIELDS:
@@ -93,7 +99,9 @@ def stage_reports(developed):
             a, b, c = g.read_field(f), o.read_field(f), d.read_field(f)[from_d]
             if diag_scale is None and f == abi.FIELD_DIAG:
                 diag_scale = float(np.abs(c).max())
-            fl = floors(diag_scale or 1.0)[f]
+            if acc_scale is None and f == abi.FIELD_ACC_PRESS:
+                acc_scale = float(np.abs(c).max())
+            fl = floors(diag_scale or 1.0, acc_scale or 1.0)[f]
             out[f"stage{stage}_field{f}"] = (elementwise_errors(a, b, RTOL_FP32[f], fl)[1],
                                              elementwise_errors(a, c, RTOL_FP64, fl)[1])
         if stage == abi.STAGE_JACOBI_UPDATE:

@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 from oracle import OracleBackend
-from test_gpu_parity import assert_neighbor_structures_equal
+from parity_util import assert_neighbor_structures_equal
 from turbospharticles_b200 import abi, scene as S
 from turbospharticles_b200.backend import SimBackendB200
 

@@ -1,6 +1,8 @@
 """Rigid coupling at full size: the double dam break with 2,000,000 fluid particles
 (two 100 x 125 x 80 blocks, dx = 0.008 m, 4 x 1.5 x 1.5 m tank) and 8 hollow cubes of edge
-0.15 m (3,088 boundary particles each; 4 at 500 kg/m^3, 4 at 2,000 kg/m^3) at seeded poses.
+0.15 m (3,088 boundary particles each; 4 at 500 kg/m^3, 4 at 2,000 kg/m^3) with seeded
+orientations, dropped at 1 m/s onto the two blocks' top faces, so that fluid-rigid forces and
+torques act from the first step.
 
 - Rigid trajectories against the FP64 oracle over a prefix of PREFIX_STEPS coupled steps (the
   GPU computes per-particle terms in FP32, body sums and the body integrator in FP64): centres
@@ -20,8 +22,8 @@ from turbospharticles_b200.backend import SimBackendB200
 
 pytestmark = pytest.mark.gpu
 
-PREFIX_STEPS = 10
-LONG_STEPS = 490
+PREFIX_STEPS = 20
+LONG_STEPS = 480
 CM_ATOL = 1e-5
 VEL_RTOL = 2e-3
 

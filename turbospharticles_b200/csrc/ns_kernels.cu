@@ -498,7 +498,9 @@ __device__ __forceinline__ void QueryWalk(const QueryArgs& a, const QueryScene& 
 }
 
 // count walk of the fluid and boundary species, QUERY_WALK_U candidates of the current range per
-// iteration (their loads in flight together); same candidates, same order, same rows as QueryWalk
+// iteration (their loads in flight together, addressed from one pointer to the range's current
+// candidate); same candidates, same order, same rows as QueryWalk. Hits are handled without
+// branches: the row store is predicated, the slot count and the running maximum are selects.
 #ifndef QUERY_WALK_U
 #define QUERY_WALK_U 4
 #endif
@@ -514,28 +516,30 @@ __device__ __forceinline__ void QueryWalkCountU(const QueryArgs& a, const QueryS
     const uint32_t gl = mine ? q.g - g0 : 0u;
     const uint32_t n = mine ? w.nne[gl] : 0u;
     const uint2* rows = w.srt + gl * sv;
+    const float xi = q.pi.x, yi = q.pi.y, zi = q.pi.z, r2 = a.r2;
     uint32_t k = 0, j = 0, e = 0;
     if (n > 0) { const uint2 v = rows[0]; j = v.x; e = v.y; }
-    uint32_t* sp = scr + (uint64_t)ref.cnt * SELL_W;
+    uint32_t cnt = ref.cnt, mx = ref.mx;
     while (k < n) {
         const uint32_t m = min(U, e - j);  // candidates of this iteration, all in the current range
+        const float4* pp = pos + j;
         float4 p[U];
 #pragma unroll
-        for (uint32_t u = 0; u < U; u++) p[u] = (u < m) ? pos[j + u] : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t u = 0; u < U; u++) p[u] = (u < m) ? pp[u] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (uint32_t u = 0; u < U; u++) {
-            if (u < m && IsNeighbor(q.pi.x, q.pi.y, q.pi.z, p[u].x, p[u].y, p[u].z, a.r2)) {
-                if (ref.cnt < ks) *sp = j + u;
-                sp += SELL_W;
-                ref.cnt++;
-                ref.mx = j + u;
-            }
+            const bool h = (u < m) && IsNeighbor(xi, yi, zi, p[u].x, p[u].y, p[u].z, r2);
+            if (h && cnt < ks) scr[(size_t)cnt * SELL_W] = j + u;
+            cnt += h ? 1u : 0u;
+            mx = h ? j + u : mx;
         }
         j += m;
         if (j == e) {
             if (++k < n) { const uint2 v = rows[k]; j = v.x; e = v.y; }
         }
     }
+    ref.cnt = cnt;
+    ref.mx = mx;
 }
 
 // whole-chunk walk of one species in group batches

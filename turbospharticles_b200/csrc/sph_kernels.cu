@@ -26,11 +26,6 @@ constexpr uint32_t SPH_THREADS = 256;
 #ifndef TSP_SPH_PERSISTENT
 #define TSP_SPH_PERSISTENT 1
 #endif
-// 1: the list entries of the next slot group are loaded before the gathers of the current group
-// (one group of loads always in flight)
-#ifndef TSP_SPH_PIPELINE
-#define TSP_SPH_PIPELINE 1
-#endif
 // FF slots per group of the pressure sweeps (pressure acceleration, Jacobi); measured on the 1M
 // dam with the kernel-gradient factor computed per pair: 3 / 2 slots (0.109 / 0.146 ms per
 // launch) against 2 / 2 (0.110 / 0.146) and 4 / 4 (0.116 / 0.158)
@@ -78,61 +73,34 @@ struct ChunkCursor {
     }
 };
 
-// Visits the slots of a lane in order, U slots at a time: the U list entries are loaded
-// together, then the U neighbor gathers (one or two float4 each), then the U pair terms are
-// applied in slot order. The sum order is unchanged; the loads of a group are independent, so
-// up to 3U memory requests per lane are in flight. The chunk's format is resolved once per
-// chunk (D16: Delta16x2, else Abs32), not per slot.
-template <int U, bool TWO, bool D16, typename Body>
-__device__ __forceinline__ void SweepFmt(const ChunkCursor& cur, const SellView& v, uint32_t lane,
-                                         const float4* A, const float4* B, Body&& body) {
-    for (uint32_t k0 = 0; k0 < cur.pitch; k0 += U) {
-        uint32_t j[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            const bool ok = k0 + u < cur.cnt;
-            const uint64_t lin = cur.off + (uint64_t)(k0 + u) * SELL_W + lane;
-            if constexpr (D16) {
-                const uint32_t e = ok ? v.list16[lin] : 0u;
-                j[u] = ok ? ((e & 0x8000u) ? cur.base2 + (e & 0x7fffu) : cur.base + e) : EMPTY_32;
-            } else {
-                j[u] = ok ? v.list32[lin] : EMPTY_32;
-            }
-        }
-        float4 a[U], b[U];
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            a[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-            b[u] = a[u];
-            if (j[u] != EMPTY_32) {
-                a[u] = A[j[u]];
-                if constexpr (TWO) b[u] = B[j[u]];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            if (j[u] == EMPTY_32) continue;
-            body(k0 + u, j[u], a[u], b[u]);
-        }
-    }
-}
-#if TSP_SPH_PIPELINE
-// pipelined: the list entries of group g + 1 are loaded before the gathers of group g, so one
-// group of stream loads is always in flight; same slots, same order
+// Visits the slots of a lane in order, U slots at a time, pipelined: the list entries of group
+// g + 1 are loaded before the neighbor gathers of group g, so one group of stream loads is always
+// in flight; then the U gathers (one or two float4 each) and the U pair terms in slot order (the
+// sum order is that of one slot after the other). The chunk's format is resolved once per chunk
+// (D16: Delta16x2, else Abs32). Slots past the lane's count are not branched around: their entry
+// is not loaded, they gather a valid dummy (element 0 of the array) and the body receives
+// ok = false and leaves its sums unchanged, so the whole warp runs one instruction stream.
+// Addressing: one 64-bit pointer to the lane's column of the chunk's slice, slots at 32-entry
+// strides from it; Delta16x2 decodes as j = base + e - (e >> 15) * (base + 0x8000 - base2)
+// (= base + e below 0x8000, base2 + (e & 0x7fff) above: StoreNeighbor_CompressedSell32,
+// neighbor_search_kernels.cu:193-247).
 template <int U, bool TWO, bool D16, typename Body>
 __device__ __forceinline__ void SweepFmtPipe(const ChunkCursor& cur, const SellView& v, uint32_t lane,
                                              const float4* A, const float4* B, Body&& body) {
+    const uint16_t* p16 = v.list16 + cur.off + lane;
+    const uint32_t* p32 = v.list32 + cur.off + lane;
+    const uint32_t delta = cur.base + 0x8000u - cur.base2;
     uint32_t jn[U];
     auto fetch = [&](uint32_t k0) {
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            const bool ok = k0 + u < cur.cnt;
-            const uint64_t lin = cur.off + (uint64_t)(k0 + u) * SELL_W + lane;
+            const uint32_t k = k0 + u;
+            const bool ok = k < cur.cnt;
             if constexpr (D16) {
-                const uint32_t e = ok ? v.list16[lin] : 0u;
-                jn[u] = ok ? ((e & 0x8000u) ? cur.base2 + (e & 0x7fffu) : cur.base + e) : EMPTY_32;
+                const uint32_t e = ok ? (uint32_t)__ldg(p16 + (size_t)k * SELL_W) : 0u;
+                jn[u] = ok ? cur.base + e - (e >> 15) * delta : 0u;
             } else {
-                jn[u] = ok ? v.list32[lin] : EMPTY_32;
+                jn[u] = ok ? __ldg(p32 + (size_t)k * SELL_W) : 0u;
             }
         }
     };
@@ -145,29 +113,19 @@ __device__ __forceinline__ void SweepFmtPipe(const ChunkCursor& cur, const SellV
         float4 a[U], b[U];
 #pragma unroll
         for (int u = 0; u < U; u++) {
-            a[u] = make_float4(0.f, 0.f, 0.f, 0.f);
-            b[u] = a[u];
-            if (j[u] != EMPTY_32) {
-                a[u] = A[j[u]];
-                if constexpr (TWO) b[u] = B[j[u]];
-            }
+            a[u] = A[j[u]];
+            if constexpr (TWO) b[u] = B[j[u]];
+            else b[u] = a[u];
         }
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-            if (j[u] == EMPTY_32) continue;
-            body(k0 + u, j[u], a[u], b[u]);
-        }
+        for (int u = 0; u < U; u++) body(k0 + u < cur.cnt, j[u], a[u], b[u]);
     }
 }
-#define TSP_SWEEP_IMPL SweepFmtPipe
-#else
-#define TSP_SWEEP_IMPL SweepFmt
-#endif
 template <int U, bool TWO, typename Body>
 __device__ __forceinline__ void SweepSlots(const ChunkCursor& cur, const SellView& v, uint32_t lane,
                                            const float4* A, const float4* B, Body&& body) {
-    if (cur.fmt == FMT_DELTA16X2) TSP_SWEEP_IMPL<U, TWO, true>(cur, v, lane, A, B, body);
-    else TSP_SWEEP_IMPL<U, TWO, false>(cur, v, lane, A, B, body);
+    if (cur.fmt == FMT_DELTA16X2) SweepFmtPipe<U, TWO, true>(cur, v, lane, A, B, body);
+    else SweepFmtPipe<U, TWO, false>(cur, v, lane, A, B, body);
 }
 // as SweepSlots, handing the body the pair's kernel-gradient factor, computed from the gathered
 // position (A holds positions) with one reciprocal square root
@@ -175,9 +133,9 @@ template <int U, bool TWO, typename Body>
 __device__ __forceinline__ void SweepSlotsGrad(const ChunkCursor& cur, const SellView& v, uint32_t lane,
                                                const float4& pi, const Consts& c, const float4* A, const float4* B,
                                                Body&& body) {
-    SweepSlots<U, TWO>(cur, v, lane, A, B, [&](uint32_t, uint32_t, const float4& a, const float4& b) {
+    SweepSlots<U, TWO>(cur, v, lane, A, B, [&](bool ok, uint32_t, const float4& a, const float4& b) {
         const float dx = pi.x - a.x, dy = pi.y - a.y, dz = pi.z - a.z;
-        body(GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c), a, b);
+        body(ok, GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c), a, b);
     });
 }
 
@@ -237,16 +195,19 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_DENSITY_MIN_BLOCKS) KDensity(
         float dF = 0.f, dB = 0.f, dR = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<TSP_SPH_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](uint32_t, uint32_t, const float4& pj, const float4&) {
-            dF = fmaf(c.massF, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dF);
+        SweepSlots<TSP_SPH_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](bool ok, uint32_t, const float4& pj, const float4&) {
+            const float t = fmaf(c.massF, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dF);
+            dF = ok ? t : dF;
         });
         cur.load(nv.fb, chunk, i, act);
-        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](uint32_t, uint32_t, const float4& pj, const float4&) {
-            dB = fmaf(pj.w, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dB);
+        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](bool ok, uint32_t, const float4& pj, const float4&) {
+            const float t = fmaf(pj.w, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dB);
+            dB = ok ? t : dB;
         });
         cur.load(nv.fr, chunk, i, act);
-        SweepSlots<2, false>(cur, nv.fr, lane, r.pos, nullptr, [&](uint32_t, uint32_t, const float4& pj, const float4&) {
-            dR = fmaf(pj.w, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dR);
+        SweepSlots<2, false>(cur, nv.fr, lane, r.pos, nullptr, [&](bool ok, uint32_t, const float4& pj, const float4&) {
+            const float t = fmaf(pj.w, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dR);
+            dR = ok ? t : dR;
         });
         if (act) reinterpret_cast<float*>(f.velRho)[4ull * i + 3] = dF + dB + dR;
     }
@@ -263,37 +224,40 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_NP_MIN_BLOCKS) KNonPressure(C
         float fx = 0.f, fy = 0.f, fz = 0.f, bx = 0.f, by = 0.f, bz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<TSP_NPSD_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velRho, [&](uint32_t, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<TSP_NPSD_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velRho, [&](bool ok, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float kg = GradFactor(d2, c);
             const float dot = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
             const float rhoJ = fmaxf(vj.w, 1e-7f);
-            const float a = (c.massF * dot) / (rhoJ * (d2 + c.hEps)) * kg;
-            fx = fmaf(a, dx, fx); fy = fmaf(a, dy, fy); fz = fmaf(a, dz, fz);
+            const float a = ok ? (c.massF * dot) / (rhoJ * (d2 + c.hEps)) * kg : 0.0f;
+            const float tx = fmaf(a, dx, fx), ty = fmaf(a, dy, fy), tz = fmaf(a, dz, fz);
+            fx = ok ? tx : fx; fy = ok ? ty : fy; fz = ok ? tz : fz;
         });
         cur.load(nv.fb, chunk, i, act);
-        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](uint32_t, uint32_t j, const float4& pj, const float4&) {
+        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](bool ok, uint32_t j, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float dvx = vi.x - 0.0f, dvy = vi.y - 0.0f, dvz = vi.z - 0.0f;
             const float dot = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float a = (b.vol[j] * dot) / (d2 + c.hEps);
-            bx = fmaf(a, gx, bx); by = fmaf(a, gy, by); bz = fmaf(a, gz, bz);
+            const float a = ok ? (b.vol[j] * dot) / (d2 + c.hEps) : 0.0f;
+            const float tx = fmaf(a, gx, bx), ty = fmaf(a, gy, by), tz = fmaf(a, gz, bz);
+            bx = ok ? tx : bx; by = ok ? ty : by; bz = ok ? tz : bz;
         });
         cur.load(nv.fr, chunk, i, act);
-        SweepSlots<2, true>(cur, nv.fr, lane, r.pos, r.vel, [&](uint32_t, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<2, true>(cur, nv.fr, lane, r.pos, r.vel, [&](bool ok, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float dot = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float a = (vj.w * dot) / (d2 + c.hEps);
-            rx = fmaf(a, gx, rx); ry = fmaf(a, gy, ry); rz = fmaf(a, gz, rz);
+            const float a = ok ? (vj.w * dot) / (d2 + c.hEps) : 0.0f;
+            const float tx = fmaf(a, gx, rx), ty = fmaf(a, gy, ry), tz = fmaf(a, gz, rz);
+            rx = ok ? tx : rx; ry = ok ? ty : ry; rz = ok ? tz : rz;
         });
         if (!act) continue;
         const float ax = fx * c.visFacF + (bx + rx) * c.visFacB + c.gx;
@@ -315,35 +279,38 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagIn
         float cxB = 0.f, cyB = 0.f, czB = 0.f, cxR = 0.f, cyR = 0.f, czR = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<TSP_NPSD_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velPred, [&](uint32_t k, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<TSP_NPSD_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velPred, [&](bool ok, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float kg = GradFactor(d2, c);
             const float st = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
-            sF = fmaf(kg, st, sF);
-            cxF = fmaf(kg, dx, cxF); cyF = fmaf(kg, dy, cyF); czF = fmaf(kg, dz, czF);
-            g2 = fmaf(kg, kg * d2, g2);  // (kgFac * distSqu first keeps the self pair exactly zero)
+            const float t0 = fmaf(kg, st, sF);
+            const float t1 = fmaf(kg, dx, cxF), t2 = fmaf(kg, dy, cyF), t3 = fmaf(kg, dz, czF);
+            const float t4 = fmaf(kg, kg * d2, g2);  // (kgFac * distSqu first keeps the self pair exactly zero)
+            sF = ok ? t0 : sF; cxF = ok ? t1 : cxF; cyF = ok ? t2 : cyF; czF = ok ? t3 : czF; g2 = ok ? t4 : g2;
         });
         cur.load(nv.fb, chunk, i, act);
-        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](uint32_t k, uint32_t, const float4& pj, const float4&) {
+        SweepSlots<2, false>(cur, nv.fb, lane, b.pos, nullptr, [&](bool ok, uint32_t, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float dvx = vi.x - 0.0f, dvy = vi.y - 0.0f, dvz = vi.z - 0.0f;
             const float st = fmaf(dvx, gx, fmaf(dvy, gy, dvz * gz));
-            sB = fmaf(pj.w, st, sB);
-            cxB = fmaf(pj.w, gx, cxB); cyB = fmaf(pj.w, gy, cyB); czB = fmaf(pj.w, gz, czB);
+            const float t0 = fmaf(pj.w, st, sB);
+            const float t1 = fmaf(pj.w, gx, cxB), t2 = fmaf(pj.w, gy, cyB), t3 = fmaf(pj.w, gz, czB);
+            sB = ok ? t0 : sB; cxB = ok ? t1 : cxB; cyB = ok ? t2 : cyB; czB = ok ? t3 : czB;
         });
         cur.load(nv.fr, chunk, i, act);
-        SweepSlots<2, true>(cur, nv.fr, lane, r.pos, r.velPred, [&](uint32_t k, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<2, true>(cur, nv.fr, lane, r.pos, r.velPred, [&](bool ok, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float kg = GradFactor(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), c);
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float st = fmaf(dvx, gx, fmaf(dvy, gy, dvz * gz));
-            sR = fmaf(pj.w, st, sR);
-            cxR = fmaf(pj.w, gx, cxR); cyR = fmaf(pj.w, gy, cyR); czR = fmaf(pj.w, gz, czR);
+            const float t0 = fmaf(pj.w, st, sR);
+            const float t1 = fmaf(pj.w, gx, cxR), t2 = fmaf(pj.w, gy, cyR), t3 = fmaf(pj.w, gz, czR);
+            sR = ok ? t0 : sR; cxR = ok ? t1 : cxR; cyR = ok ? t2 : cyR; czR = ok ? t3 : czR;
         });
         if (!act) continue;
         sF *= c.massF;
@@ -377,24 +344,27 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_PACC_MIN_BLOCKS) KPressureAcc
         float ax = 0.f, ay = 0.f, az = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsGrad<TSP_PACC_FF_SLOTS, false>(cur, nv.ff, lane, pi, c, f.posP, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<TSP_PACC_FF_SLOTS, false>(cur, nv.ff, lane, pi, c, f.posP, nullptr, [&](bool ok, float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float a = (fOuter + c.massF * pj.w * c.densInvSqu) * kg;
-            ax = fmaf(a, dx, ax); ay = fmaf(a, dy, ay); az = fmaf(a, dz, az);
+            const float tx = fmaf(a, dx, ax), ty = fmaf(a, dy, ay), tz = fmaf(a, dz, az);
+            ax = ok ? tx : ax; ay = ok ? ty : ay; az = ok ? tz : az;
         });
         cur.load(nv.fb, chunk, i, act);
-        SweepSlotsGrad<2, false>(cur, nv.fb, lane, pi, c, b.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<2, false>(cur, nv.fb, lane, pi, c, b.pos, nullptr, [&](bool ok, float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float a = c.accCoeffB * pj.w * pi.w;
-            ax = fmaf(a, gx, ax); ay = fmaf(a, gy, ay); az = fmaf(a, gz, az);
+            const float tx = fmaf(a, gx, ax), ty = fmaf(a, gy, ay), tz = fmaf(a, gz, az);
+            ax = ok ? tx : ax; ay = ok ? ty : ay; az = ok ? tz : az;
         });
         cur.load(nv.fr, chunk, i, act);
-        SweepSlotsGrad<2, false>(cur, nv.fr, lane, pi, c, r.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<2, false>(cur, nv.fr, lane, pi, c, r.pos, nullptr, [&](bool ok, float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float a = c.accCoeffB * pj.w * pi.w;
-            ax = fmaf(a, gx, ax); ay = fmaf(a, gy, ay); az = fmaf(a, gz, az);
+            const float tx = fmaf(a, gx, ax), ty = fmaf(a, gy, ay), tz = fmaf(a, gz, az);
+            ax = ok ? tx : ax; ay = ok ? ty : ay; az = ok ? tz : az;
         });
         if (act) f.acc[i] = make_float4(0.0f - ax, 0.0f - ay, 0.0f - az, 0.0f);
     }
@@ -416,26 +386,29 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_JACOBI_MIN_BLOCKS) KJacobi(Co
         float sF = 0.f, sB = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsGrad<TSP_JACOBI_FF_SLOTS, true>(cur, nv.ff, lane, pi, c, f.posP, f.acc, [&](float kg, const float4& pj, const float4& aj) {
+        SweepSlotsGrad<TSP_JACOBI_FF_SLOTS, true>(cur, nv.ff, lane, pi, c, f.posP, f.acc, [&](bool ok, float kg, const float4& pj, const float4& aj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
             const float sv = fmaf(dax, dx, fmaf(day, dy, daz * dz));
-            sF = fmaf(kg, sv, sF);
+            const float t = fmaf(kg, sv, sF);
+            sF = ok ? t : sF;
         });
         sF *= c.massF;
         cur.load(nv.fb, chunk, i, act);
-        SweepSlotsGrad<2, false>(cur, nv.fb, lane, pi, c, b.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<2, false>(cur, nv.fb, lane, pi, c, b.pos, nullptr, [&](bool ok, float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
-            sB = sB + pj.w * sv;
+            const float t = sB + pj.w * sv;
+            sB = ok ? t : sB;
         });
         cur.load(nv.fr, chunk, i, act);
-        SweepSlotsGrad<2, false>(cur, nv.fr, lane, pi, c, r.pos, nullptr, [&](float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<2, false>(cur, nv.fr, lane, pi, c, r.pos, nullptr, [&](bool ok, float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float gx = kg * dx, gy = kg * dy, gz = kg * dz;
             const float sv = fmaf(ai.x, gx, fmaf(ai.y, gy, ai.z * gz));
-            sB = sB + pj.w * sv;
+            const float t = sB + pj.w * sv;
+            sB = ok ? t : sB;
         });
         if (act) {
             const float2 sd = f.srcDiag[i];

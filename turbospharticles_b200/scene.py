@@ -346,13 +346,16 @@ def _rotation(rng):
         [2 * (qx * qz - qy * qw), 2 * (qy * qz + qx * qw), 1 - 2 * (qx * qx + qy * qy)]])
 
 
-def rigid_dam(block=(100, 125, 80), dx=0.008, tank=(4.0, 1.5, 1.5), cubes=8, edge=0.15, dt=4e-4, seed=7):
+def rigid_dam(block=(100, 125, 80), dx=0.008, tank=(4.0, 1.5, 1.5), cubes=8, edge=0.15, dt=4e-4, seed=7,
+              drop_speed=1.0):
     """Two-sided dam with floating hollow cubes: two fluid blocks of block[0] x block[1] x
     block[2] lattice particles (spacing dx) in opposite corners of the tank, `cubes` hollow
-    rigid cubes (edge `edge`, 2 particle layers, BuildRigidBody_OBB_Hollow) at seeded positions
-    between the blocks with seeded random orientations; the first half of the cubes have
-    density 500 kg/m^3, the rest 2000 kg/m^3. Defaults: 2,000,000 fluid particles, 8 cubes
-    of 3,088 particles."""
+    rigid cubes (edge `edge`, 2 particle layers, BuildRigidBody_OBB_Hollow) with seeded random
+    orientations resting on the blocks' top faces (half of them on each block, in a 2 x n grid
+    over the face, seeded jitter, the lowest rigid particles level with the top fluid layer), dropped
+    onto it at `drop_speed` m/s, so fluid-rigid forces act from the first steps; the first half
+    of the cubes have density 500 kg/m^3, the rest 2000 kg/m^3. Defaults: 2,000,000 fluid
+    particles, 8 cubes of 3,088 particles."""
     from .params import dam_params
     p = dam_params(dx, dt)
     p.jitterFracF = 0.01
@@ -362,18 +365,24 @@ def rigid_dam(block=(100, 125, 80), dx=0.008, tank=(4.0, 1.5, 1.5), cubes=8, edg
     fluids = [OBB((0.0, 0.0, 0.0), tuple(ext)),
               OBB((tank[0] - ext[0], 0.0, tank[2] - ext[2]), tuple(ext))]
     rng = np.random.default_rng(seed)
-    gap = (ext[0] + edge, tank[0] - ext[0] - edge)
-    cols = max(1, (cubes + 1) // 2)
+    per_block = max(1, (cubes + 1) // 2)
+    cols = max(1, (per_block + 1) // 2)
+    corners = np.array([[i, j, k] for i in (0, 1) for j in (0, 1) for k in (0, 1)], np.float64) * edge
     rigid = []
     for k in range(cubes):
-        cx = gap[0] + (gap[1] - gap[0]) * (k % cols + 0.5) / cols
-        cz = tank[2] * (0.3 if k // cols == 0 else 0.7)
-        cy = edge + rng.random() * max(tank[1] * 0.5 - edge, 0.0)
+        b, slot = divmod(k, per_block)
+        fo = fluids[min(b, 1)].origin
+        # cell of a 2 x cols grid over the block's top face, centre jittered by up to a tenth of the cell
+        fx = (slot % cols + 0.5 + 0.2 * (rng.random() - 0.5)) / cols
+        fz = (slot // cols + 0.5 + 0.2 * (rng.random() - 0.5)) / 2.0
         R = _rotation(rng)
-        u, v, w = (tuple(float(x) for x in R[:, c]) for c in range(3))
-        origin = tuple(float(c) for c in np.array([cx, cy, cz]) - R @ np.full(3, 0.5 * edge))
+        low = float(((corners - 0.5 * edge) @ R.T)[:, 1].min())  # lowest corner below the centre
+        c = np.array([fo[0] + fx * ext[0], ext[1] - 1.25 * dx - low, fo[2] + fz * ext[2]])
+        u, v, w = (tuple(float(x) for x in R[:, cc]) for cc in range(3))
+        origin = tuple(float(x) for x in c - R @ np.full(3, 0.5 * edge))
         rigid.append((OBB(origin, (edge, edge, edge), u, v, w), 500.0 if k < cubes // 2 else 2000.0))
     st, dmin, dmax = breaking_dam(container, fluids, p, rigid)
+    st.yVelRB[:] = -drop_speed
     return st, dmin, dmax, p
 
 
