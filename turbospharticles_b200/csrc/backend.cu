@@ -198,6 +198,7 @@ public:
     float bMin[3] = {0, 0, 0}, bMax[3] = {0, 0, 0};
     DBuf<uint64_t> keysA, keysB;
     DBuf<uint32_t> valsA, valsB, tileHist, digitTotals;
+    DBuf<uint64_t> keyOrNot;  // OR of the sort keys and of their complements (constant-digit passes)
     DBuf<uint32_t> permF, permB, permR;
     DBuf<uint64_t> cidF, cidB, cidR, cidRs;
     DBuf<uint64_t> uniqF, uniqB, uniqR;
@@ -784,6 +785,7 @@ public:
         valsA.ensure(std::max<uint32_t>(nMax, 1)); valsB.ensure(std::max<uint32_t>(nMax, 1));
         tileHist.ensure(RadixTileHistItems(std::max<uint32_t>(nMax, 1)));
         digitTotals.ensure(256);
+        keyOrNot.ensure(2);
         scanScratch.ensure(ScanScratchItems(std::max<uint32_t>(nMax, 1) + 1));
         scanScratch2.ensure(ScanScratchItems(std::max<uint32_t>(nMax, 1) + 1));
         permF.ensure(std::max<uint32_t>(nF, 1)); permB.ensure(std::max<uint32_t>(nB, 1));
@@ -819,7 +821,7 @@ public:
         CK(cudaEventRecord(pev[1], s));
         if (!frameValid) { listsValid = false; return; }
         EnsureNsScratch();
-        SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p};
+        SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p, keyOrNot.p};
         // boundary: sorted under this frame unless it already is (then its permutation this
         // step is the identity, or, on the first build after a pull that kept a sort of the same
         // raw boundary, that sort's permutation)
@@ -1363,7 +1365,7 @@ public:
             EnsureNsScratch();
             if (gridCells > gridB.cap) bSortedValid = false;
             gridF.ensure(gridCells); gridB.ensure(gridCells); gridR.ensure(gridCells);
-            SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p};
+            SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p, keyOrNot.p};
             EnsureBoundarySorted(sc);
             psiTmpB.ensure(nB);
             LaunchBoundaryVolumes(c, posB.p, nB, startB.p, gridB.p, fr, defVol, defPsi, prm.restDensity, volB.p,

@@ -46,6 +46,7 @@ struct SortScratch {
     uint32_t* valsB;
     uint32_t* tileHist;
     uint32_t* digitTotals;
+    uint64_t* keyOrNot;  // 2 words: OR of the keys and of their complements (NULL: every pass runs)
 };
 
 struct QueryArgs {

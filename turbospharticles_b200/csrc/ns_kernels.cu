@@ -101,15 +101,41 @@ void LaunchProbe(const float4* pos, uint32_t n, const Frame& fr, bool frameValid
 }
 
 // ----------------------------------------------------------------------------- keys
+// clamped keys; with `orNot`, also the OR of all keys and of all complemented keys (block
+// reduction, one atomic pair per block), from which the sort skips passes of constant digits
 template <typename K>
 __global__ void __launch_bounds__(256) KKeys(const float4* __restrict__ pos, uint32_t n, Frame fr, uint64_t emptyKey,
-                                            K* __restrict__ keys, uint32_t* __restrict__ idx) {
+                                            K* __restrict__ keys, uint32_t* __restrict__ idx,
+                                            unsigned long long* __restrict__ orNot) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4 p = pos[i];
-    const uint64_t c = CellIdOf(p.x, p.y, p.z, fr);
-    keys[i] = (K)(c < emptyKey ? c : emptyKey);
-    idx[i] = i;
+    uint64_t k = 0, kn = 0;
+    if (i < n) {
+        const float4 p = pos[i];
+        const uint64_t c = CellIdOf(p.x, p.y, p.z, fr);
+        k = c < emptyKey ? c : emptyKey;
+        kn = ~k;
+        keys[i] = (K)k;
+        idx[i] = i;
+    }
+    if (orNot == nullptr) return;
+    __shared__ uint64_t so[8], sn[8];
+    uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)k), hi = __reduce_or_sync(0xffffffffu, (uint32_t)(k >> 32));
+    uint32_t nlo = __reduce_or_sync(0xffffffffu, (uint32_t)kn), nhi = __reduce_or_sync(0xffffffffu, (uint32_t)(kn >> 32));
+    const uint32_t warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        so[warp] = ((uint64_t)hi << 32) | lo;
+        sn[warp] = ((uint64_t)nhi << 32) | nlo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint64_t a = 0, b = 0;
+        for (uint32_t w = 0; w < (blockDim.x >> 5); w++) { a |= so[w]; b |= sn[w]; }
+        // a block whose threads all lie past n contributes nothing (no keys)
+        if (blockIdx.x * blockDim.x < n) {
+            atomicOr(orNot + 0, (unsigned long long)a);
+            atomicOr(orNot + 1, (unsigned long long)b);
+        }
+    }
 }
 
 // (unclamped) cell IDs in storage order (rigid particles)
@@ -134,18 +160,20 @@ void SortByCell(const float4* pos, uint32_t n, const Frame& fr, SortScratch& sc,
     if (n == 0) return;
     const uint64_t emptyKey = 1ull << (fr.keyBits - 1u);
     const uint32_t g = (n + 255) / 256;
+    unsigned long long* orNot = reinterpret_cast<unsigned long long*>(sc.keyOrNot);
+    if (orNot) cudaMemsetAsync(orNot, 0, 2 * sizeof(uint64_t), s);
     if (fr.keyBits <= 32) {
         uint32_t* k0 = reinterpret_cast<uint32_t*>(sc.keysA);
         uint32_t* k1 = reinterpret_cast<uint32_t*>(sc.keysB);
-        KKeys<uint32_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, k0, sc.valsA);
+        KKeys<uint32_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, k0, sc.valsA, orNot);
         const bool alt = RadixSortPairs<uint32_t, uint32_t>(k0, sc.valsA, k1, sc.valsB, n, fr.keyBits, sc.tileHist,
-                                                            sc.digitTotals, s);
+                                                            sc.digitTotals, s, sc.keyOrNot);
         KKeysToCellIds<uint32_t><<<g, 256, 0, s>>>(alt ? k1 : k0, n, emptyKey, cidSorted);
         cudaMemcpyAsync(perm, alt ? sc.valsB : sc.valsA, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     } else {
-        KKeys<uint64_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, sc.keysA, sc.valsA);
+        KKeys<uint64_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, sc.keysA, sc.valsA, orNot);
         const bool alt = RadixSortPairs<uint64_t, uint32_t>(sc.keysA, sc.valsA, sc.keysB, sc.valsB, n, fr.keyBits,
-                                                            sc.tileHist, sc.digitTotals, s);
+                                                            sc.tileHist, sc.digitTotals, s, sc.keyOrNot);
         KKeysToCellIds<uint64_t><<<g, 256, 0, s>>>(alt ? sc.keysB : sc.keysA, n, emptyKey, cidSorted);
         cudaMemcpyAsync(perm, alt ? sc.valsB : sc.valsA, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     }

@@ -145,9 +145,20 @@ constexpr int RS_ITEMS = 8;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_WARPS = RS_THREADS / 32;
 
+// Passes whose digit is the same in every key are the identity permutation. When the caller
+// gives `orNot` = {OR of all keys, OR of all complemented keys} (computed while the keys are
+// made), such a pass skips its histogram and scan and its scatter becomes a plain copy.
+__device__ __forceinline__ bool RadixPassConstant(const uint64_t* orNot, uint32_t shift) {
+    if (orNot == nullptr) return false;
+    const uint64_t varying = orNot[0] & orNot[1];  // bits that are 1 in some key and 0 in another
+    return ((varying >> shift) & 255u) == 0u;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(RS_THREADS) KRadixUpsweep(const K* __restrict__ keys, uint32_t n, uint32_t shift,
-                                                          uint32_t* __restrict__ tileHist, uint32_t nTiles) {
+                                                          uint32_t* __restrict__ tileHist, uint32_t nTiles,
+                                                          const uint64_t* __restrict__ orNot) {
+    if (RadixPassConstant(orNot, shift)) return;
     __shared__ uint32_t h[256];
     h[threadIdx.x] = 0;
     __syncthreads();
@@ -166,7 +177,9 @@ __global__ void __launch_bounds__(RS_THREADS) KRadixUpsweep(const K* __restrict_
 
 // one block per digit: exclusive scan of that digit's row across tiles, digit total out
 static __global__ void __launch_bounds__(256) KRadixScanRows(uint32_t* __restrict__ tileHist, uint32_t nTiles,
-                                                      uint32_t* __restrict__ digitTotals) {
+                                                      uint32_t* __restrict__ digitTotals, uint32_t shift,
+                                                      const uint64_t* __restrict__ orNot) {
+    if (RadixPassConstant(orNot, shift)) return;
     __shared__ uint32_t ws[8];
     uint32_t* row = tileHist + (uint64_t)blockIdx.x * nTiles;
     uint32_t carry = 0;
@@ -198,7 +211,16 @@ template <typename K, typename V>
 __global__ void __launch_bounds__(RS_THREADS) KRadixDownsweep(const K* __restrict__ kin, const V* __restrict__ vin,
                                                             K* __restrict__ kout, V* __restrict__ vout, uint32_t n,
                                                             uint32_t shift, const uint32_t* __restrict__ tileHist,
-                                                            const uint32_t* __restrict__ digitTotals, uint32_t nTiles) {
+                                                            const uint32_t* __restrict__ digitTotals, uint32_t nTiles,
+                                                            const uint64_t* __restrict__ orNot) {
+    if (RadixPassConstant(orNot, shift)) {  // identity pass: copy the tile
+        const uint32_t base = blockIdx.x * RS_TILE;
+        for (uint32_t li = threadIdx.x; li < (uint32_t)RS_TILE && base + li < n; li += RS_THREADS) {
+            kout[base + li] = kin[base + li];
+            vout[base + li] = vin[base + li];
+        }
+        return;
+    }
     __shared__ uint32_t digitBase[256];
     __shared__ uint32_t tileStart[256];
     __shared__ uint32_t cnt[256];
@@ -302,15 +324,16 @@ __global__ void __launch_bounds__(RS_THREADS) KRadixDownsweep(const K* __restric
 // and returns true when the result ended up in the alternate buffers (kAlt, vAlt)
 template <typename K, typename V>
 bool RadixSortPairs(K* keys, V* vals, K* kAlt, V* vAlt, uint32_t n, uint32_t bits, uint32_t* tileHist,
-                    uint32_t* digitTotals, cudaStream_t s) {
+                    uint32_t* digitTotals, cudaStream_t s, const uint64_t* orNot = nullptr) {
     if (n < 2) return false;
     const uint32_t nTiles = (n + RS_TILE - 1) / RS_TILE;
     K* ks = keys; V* vs = vals; K* kd = kAlt; V* vd = vAlt;
     bool alt = false;
     for (uint32_t shift = 0; shift < bits; shift += 8) {
-        KRadixUpsweep<K><<<nTiles, RS_THREADS, 0, s>>>(ks, n, shift, tileHist, nTiles);
-        KRadixScanRows<<<256, 256, 0, s>>>(tileHist, nTiles, digitTotals);
-        KRadixDownsweep<K, V><<<nTiles, RS_THREADS, 0, s>>>(ks, vs, kd, vd, n, shift, tileHist, digitTotals, nTiles);
+        KRadixUpsweep<K><<<nTiles, RS_THREADS, 0, s>>>(ks, n, shift, tileHist, nTiles, orNot);
+        KRadixScanRows<<<256, 256, 0, s>>>(tileHist, nTiles, digitTotals, shift, orNot);
+        KRadixDownsweep<K, V><<<nTiles, RS_THREADS, 0, s>>>(ks, vs, kd, vd, n, shift, tileHist, digitTotals, nTiles,
+                                                            orNot);
         K* tk = ks; ks = kd; kd = tk;
         V* tv = vs; vs = vd; vd = tv;
         alt = !alt;
