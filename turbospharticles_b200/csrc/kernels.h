@@ -83,7 +83,7 @@ struct QueryArgs {
     uint32_t epoch;
     struct U64x2* sellTotals;
 };
-constexpr uint32_t LB_WORDS = 16;  // look-back record: state word, 6 aggregate and 6 inclusive sums (128 bytes)
+constexpr uint32_t LB_WORDS = 8;  // look-back record: state word + 6 sums + padding (64 bytes)
 struct SceneGeom {
     Frame fr;
     uint64_t gridOffF, gridOffB;

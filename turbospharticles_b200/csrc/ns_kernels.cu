@@ -788,16 +788,12 @@ __device__ __forceinline__ ChunkDecision DecideChunkMeta(uint32_t chunk, const L
 constexpr uint32_t LB_AGGREGATE = 1u, LB_INCLUSIVE = 2u;
 constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;  // bounded wait per record (~seconds), then ERR_LOOKBACK
 
-// record layout: word 0 state (epoch << 2 | state), words 1-6 the aggregate, words 7-12 the
-// inclusive prefix. The two sums have their own words: a reader that saw "aggregate" may still be
-// reading when the owner publishes its inclusive prefix, and must not see those values instead.
 __device__ __forceinline__ void LbPublish(unsigned long long* rec, uint32_t epoch, uint32_t state, const uint64_t v[6]) {
-    volatile unsigned long long* r = rec + (state == LB_INCLUSIVE ? 7 : 1);
+    volatile unsigned long long* r = rec;
 #pragma unroll
-    for (int k = 0; k < 6; k++) r[k] = v[k];
+    for (int k = 0; k < 6; k++) r[1 + k] = v[k];
     __threadfence();
-    volatile unsigned long long* f = rec;
-    f[0] = ((unsigned long long)epoch << 2) | state;
+    r[0] = ((unsigned long long)epoch << 2) | state;
 }
 
 // exclusive prefix of the six sums at `chunk`, 32 predecessors per round (lane l reads chunk
@@ -825,9 +821,8 @@ __device__ __forceinline__ bool LbExclusive(const unsigned long long* lb, uint32
         const bool take = p >= 0 && lane <= first;
         uint64_t v[6];
         __threadfence();
-        const uint32_t at = state == LB_INCLUSIVE ? 7u : 1u;
 #pragma unroll
-        for (int k = 0; k < 6; k++) v[k] = take ? r[at + k] : 0ull;
+        for (int k = 0; k < 6; k++) v[k] = take ? r[1 + k] : 0ull;
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1)
 #pragma unroll
