@@ -24,11 +24,7 @@ LIST_FF, LIST_FB, LIST_FR, LIST_RF, LIST_RB, LIST_RR = range(6)
 NOALLOC_MAX_PARTICLES = 1 << 24  # TSP_NOALLOC_MAX_PARTICLES
 # Stats::StatMetric (source/eval/stats/metrics.h:23-86), the record of tsp_b200_fill_statistics
 STAT_NAMES = ("NumF", "NumB", "NumR", "NumNbrFF_Avg", "NumNbrFF_Min", "NumNbrFF_Max", "NumNbrFF_P99", "NumNbrFB_Avg", "NumNbrFB_Min", "NumNbrFB_Max", "NumNbrFB_P99", "NumNbrFR_Avg", "NumNbrFR_Min", "NumNbrFR_Max", "NumNbrFR_P99", "NumNbrRF_Avg", "NumNbrRF_Min", "NumNbrRF_Max", "NumNbrRF_P99", "NumNbrRB_Avg", "NumNbrRB_Min", "NumNbrRB_Max", "NumNbrRB_P99", "NumNbrRR_Avg", "NumNbrRR_Min", "NumNbrRR_Max", "NumNbrRR_P99", "DensRelError_Raw_Avg", "DensRelError_Pos_Avg", "DensRelError_Abs_Avg", "NumSolverIters", "CFL_Number", "VelMag_Avg", "VelMag_Min", "VelMag_Max")
-# phases of one step (device times between the backend's phase events): the fluid neighbor query
-# is one single-pass launch ("query"); "query_readback" holds the rigid CSR scans and the read-back
-# of the list totals; "query_regrow_rigid_fill" the rare repeat of the query after list growth and
-# the rigid fill
-PHASE_NAMES = ("frame", "sort_reorder_tables", "query", "query_readback", "query_regrow_rigid_fill", "density",
+PHASE_NAMES = ("frame", "sort_reorder_tables", "query_count", "finalize_readback", "query_fill", "density",
                "non_pressure", "source_diag_init", "jacobi_loop", "pressure_acc_final", "integration",
                "stats_readback")
 STAGE_DENSITY, STAGE_NON_PRESSURE, STAGE_SOURCE_DIAG_INIT = 1, 2, 3

@@ -221,15 +221,11 @@ public:
     DBuf<unsigned long long> nbrTot;
     StepEnd* seDev = nullptr;   // device view of hm->se (mapped pinned memory)
     NsTotals* nsDev = nullptr;  // device view of hm->ns
-    // rows of the single-pass fluid query, one [slot][lane] block per resident warp of its grid;
-    // rows longer than KS_* slots make that chunk walk its stencil again when it writes
+    // count-pass rows of the fluid query ([chunk][slot][lane]); rows longer than KS_* slots make
+    // the fill walk that chunk's stencil again
     static constexpr uint32_t KS_F = 64, KS_B = 48, KS_R = 16;
     DBuf<uint32_t> scrF, scrB, scrR;
     DBuf<uint8_t> scrOver;
-    uint32_t queryWarps = 0, queryWarpsFor = 0, queryWarpsReach = 0;  // warp slots of the query grid
-    DBuf<unsigned long long> lookback;  // per-chunk look-back records of the query's offsets
-    DBuf<uint32_t> ticket;              // chunk ticket counter of the query grid
-    uint32_t lbEpoch = 0;
     uint64_t nNbr[3] = {0, 0, 0};
     DBuf<uint16_t> cntR[3];
     DBuf<uint64_t> offR[3];
@@ -363,8 +359,6 @@ public:
             throw Error(TSP_ERR_UNSUPPORTED, "a rigid contact particle touches more than 8 bodies");
         if (e & ERR_QUERY_CAP) throw Error(TSP_ERR_UNSUPPORTED, "query stencil exceeds the shared-memory staging");
         if (e & ERR_COUNT_U16) throw Error(TSP_ERR_OVERFLOW, "a neighbor count exceeds uint16 storage");
-        if (e & ERR_LOOKBACK)
-            throw Error(TSP_ERR_CUDA, "neighbor query: a chunk's offset look-back gave up waiting for its predecessors");
         throw Error(TSP_ERR_NEIGHBOR_LIST, "SELL32 neighbor-list fill overflow / delta range error");
     }
 
@@ -814,21 +808,10 @@ public:
         }
         velPred2.ensure(std::max<uint32_t>(nF, 1)); acc2.ensure(std::max<uint32_t>(nF, 1));
         srcDiag2.ensure(std::max<uint32_t>(nF, 1));
-        if (queryWarpsFor != nF || queryWarpsReach != reach) {
-            queryWarps = QueryFusedWarps(nF, reach);
-            queryWarpsFor = nF;
-            queryWarpsReach = reach;
-        }
-        scrF.ensure(std::max<size_t>(QueryScratchWords(queryWarps, KS_F), 1));
-        scrB.ensure(std::max<size_t>(QueryScratchWords(queryWarps, KS_B), 1));
-        scrR.ensure(std::max<size_t>(QueryScratchWords(queryWarps, nR ? KS_R : 0), 1));
-        scrOver.ensure(1);
-        const size_t lbWords = (size_t)std::max<uint32_t>(nChunks, 1) * LB_WORDS;
-        if (lookback.cap < lbWords) {
-            lookback.ensure(lbWords);
-            CK(cudaMemsetAsync(lookback.p, 0, lbWords * sizeof(unsigned long long), s));
-        }
-        ticket.ensure(1);
+        scrF.ensure(std::max<size_t>(QueryScratchWords(nChunks, KS_F), 1));
+        scrB.ensure(std::max<size_t>(QueryScratchWords(nChunks, KS_B), 1));
+        scrR.ensure(std::max<size_t>(QueryScratchWords(nChunks, nR ? KS_R : 0), 1));
+        scrOver.ensure(std::max<uint32_t>(nChunks, 1));
     }
     // ReOrderParticleData + Construct + Query_Count + Finalize_Count + Query_Fill
     void NeighborBuild(bool permuteAll) {
@@ -877,52 +860,33 @@ public:
         SellMeta m0 = Meta(0), m1 = Meta(1), m2 = Meta(2);
         RigidLists rl = RLists();
         CK(cudaEventRecord(pev[2], s));
-        // fluid: one single-pass launch (counts, chunk meta, offsets, packed lists) into the
-        // current list capacities; rigid sources: count pass
-        QueryFluidSinglePass(qa, m0, m1, m2);
+        CK(cudaMemsetAsync(nbrTot.p, 0, 3 * sizeof(unsigned long long), s));
+        LaunchQueryFluid(false, qa, m0, m1, m2, s);
         LaunchQueryRigid(false, qa, rl, s);
         CK(cudaEventRecord(pev[3], s));
+        const uint32_t nChunks = (nF + SELL_W - 1) / SELL_W;
+        FinalizeSell3(Meta(0), Meta(1), Meta(2), nChunks, scanScratch2.p, sellTot.p, s);
         if (nR)
             for (int k = 0; k < 3; k++) FinalizeCsr(cntR[k].p, offR[k].p, nR, scanScratch.p, csrTot.p + k, s);
         KGatherNsTotals<<<1, 32, 0, s>>>(sellTot.p, csrTot.p, nCellsDev.p, nbrTot.p, nR ? 1 : 0, nsDev);
         CK(cudaEventRecord(pev[4], s));
         Sync();
-        bool shortLists = false;
         for (int k = 0; k < 3; k++) {
             nNbr[k] = nF ? hm->ns.nbrTot[k] : 0;
             sell[k].n16 = hm->ns.sellTot[k].a;
             sell[k].n32 = hm->ns.sellTot[k].b;
-            shortLists |= sell[k].n16 > sell[k].l16.cap || sell[k].n32 > sell[k].l32.cap;
             sell[k].l16.grow(sell[k].n16, LIST_GROWTH);
             sell[k].l32.grow(sell[k].n32, LIST_GROWTH);
             csrN[k] = hm->ns.csrTot[k];
             listR[k].grow(csrN[k], LIST_GROWTH);
         }
-        if (shortLists) {
-            // the lists outgrew their capacities (entries past them were not written): the same
-            // build again into the grown lists (same counts, meta and offsets)
-            m0 = Meta(0); m1 = Meta(1); m2 = Meta(2);
-            QueryFluidSinglePass(qa, m0, m1, m2);
-            listRebuilds++;
-        }
+        m0 = Meta(0); m1 = Meta(1); m2 = Meta(2);
         rl = RLists();
+        LaunchQueryFluid(true, qa, m0, m1, m2, s);
         LaunchQueryRigid(true, qa, rl, s);
         CK(cudaEventRecord(pev[5], s));
-        launches += (nF ? (shortLists ? 2u : 1u) : 0u) + 2u * (nR ? 1u : 0u) + (nR ? 9u : 0u) + 1u;
+        launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + FinalizeSell3Launches(nChunks) + (nR ? 9u : 0u) + 1u;
         listsValid = true;
-    }
-    uint64_t listRebuilds = 0;  // builds repeated because the packed lists outgrew their capacity
-    void QueryFluidSinglePass(QueryArgs qa, const SellMeta& m0, const SellMeta& m1, const SellMeta& m2) {
-        CK(cudaMemsetAsync(nbrTot.p, 0, 3 * sizeof(unsigned long long), s));
-        CK(cudaMemsetAsync(sellTot.p, 0, 3 * sizeof(U64x2), s));
-        CK(cudaMemsetAsync(ticket.p, 0, sizeof(uint32_t), s));
-        lbEpoch = (lbEpoch + 1u) & 0x3fffffffu;
-        if (lbEpoch == 0) lbEpoch = 1;
-        qa.ticket = ticket.p;
-        qa.lookback = lookback.p;
-        qa.epoch = lbEpoch;
-        qa.sellTotals = sellTot.p;
-        LaunchQueryFluidFused(qa, m0, m1, m2, s);
     }
     QueryArgs MakeQueryArgs() {
         QueryArgs qa{};

@@ -75,15 +75,7 @@ struct QueryArgs {
     const uint8_t* chunkLen;
     const uint32_t* chunkScene;
     const struct SceneGeom* scenes;
-    // single-pass build (KQueryFluidFused) only: chunk ticket counter (zero at launch), look-back
-    // records (LB_WORDS words per chunk, state words tagged with `epoch`), list totals out; the
-    // row scratch is then per resident warp (ks* slots of 32 lanes per warp slot)
-    uint32_t* ticket;
-    unsigned long long* lookback;
-    uint32_t epoch;
-    struct U64x2* sellTotals;
 };
-constexpr uint32_t LB_WORDS = 8;  // look-back record: state word + 6 sums + padding (64 bytes)
 struct SceneGeom {
     Frame fr;
     uint64_t gridOffF, gridOffB;
@@ -198,13 +190,6 @@ size_t QueryScratchWords(uint32_t nChunks, uint32_t ks);
 size_t QuerySmemBytes(uint32_t reach);  // dynamic shared memory of one fluid-query block
 void LaunchQueryFluid(bool fill, const QueryArgs& a, const SellMeta& ff, const SellMeta& fb, const SellMeta& fr,
                       cudaStream_t s);
-// single pass: counts, chunk meta, offsets (decoupled look-back over the chunks) and the packed
-// lists in one launch; entries beyond a list's capacity are not written (the host compares the
-// totals with the capacities and launches again after growing). Returns the grid's warp count,
-// the number of row-scratch slots it needs.
-uint32_t QueryFusedWarps(uint32_t nF, uint32_t reach);
-void LaunchQueryFluidFused(const QueryArgs& a, const SellMeta& ff, const SellMeta& fb, const SellMeta& fr,
-                           cudaStream_t s);
 void LaunchQueryRigid(bool fill, const QueryArgs& a, const RigidLists& L, cudaStream_t s);
 void FinalizeSell(const SellMeta& m, uint32_t nChunks, U64x2* scratch, U64x2* totals, cudaStream_t s);
 // the FF, FB and FR finalize scans in one launch (up to 65,536 chunks; three scans beyond)

@@ -304,12 +304,9 @@ struct LaneWriter {
     uint32_t wr, pitch, base, base2;
     uint64_t off;
     uint8_t fmt;
-    bool capSilent;  // single-pass build: an entry beyond the list capacity is skipped (the host
-                     // sees the total, grows the list and builds again); otherwise it is an error
     __device__ void init(const SellMeta& m, uint32_t chunk) {
         wr = 0; pitch = m.pitch[chunk]; base = m.base[chunk]; base2 = m.base2[chunk]; off = m.offset[chunk];
         fmt = m.format[chunk];
-        capSilent = false;
     }
     // StoreNeighbor_CompressedSell32 (neighbor_search_kernels.cu:193-247)
     __device__ void store(const SellMeta& m, uint32_t lane, uint32_t j, uint32_t* err) {
@@ -317,11 +314,10 @@ struct LaneWriter {
         const uint64_t lin = off + (uint64_t)wr * SELL_W + lane;
         if (fmt == FMT_DELTA16X2) {
             const bool first = (j >= base) && (j - base <= 0x7fffu);
-            if (!first && (j < base2 || j - base2 > 0x7fffu)) { atomicOr(err, ERR_DELTA_RANGE); return; }
-            if (lin >= m.cap16) { if (!capSilent) atomicOr(err, ERR_DELTA_RANGE); wr++; return; }
+            if ((!first && (j < base2 || j - base2 > 0x7fffu)) || lin >= m.cap16) { atomicOr(err, ERR_DELTA_RANGE); return; }
             m.list16[lin] = first ? (uint16_t)(j - base) : (uint16_t)(0x8000u | (j - base2));
         } else {
-            if (lin >= m.cap32) { if (!capSilent) atomicOr(err, ERR_FILL_OVERFLOW); wr++; return; }
+            if (lin >= m.cap32) { atomicOr(err, ERR_FILL_OVERFLOW); return; }
             m.list32[lin] = j;
         }
         wr++;
@@ -732,270 +728,6 @@ __global__ void __launch_bounds__(QUERY_THREADS, TSP_FILL_MIN_BLOCKS) KQueryFlui
         if (over & 4u) QuerySpecies<2, WALK_FILL>(a, sc, w, q, lane, 0u, 0u, none, nullptr, 0u, wFR, mFR);
     }
     if (inRange && wFR.wr > 1) SortRowSell(mFR, wFR, lane);
-}
-
-// ---- single-pass build: count, chunk meta, offsets and packed lists in one launch
-//
-// The reference (and the two-pass form above) counts every chunk, scans the chunk sizes for the
-// offsets, then fills. Here a persistent grid takes chunks in ascending order from a ticket
-// counter; after its walk a warp knows its chunk's pitch and format per list, publishes the six
-// slice sizes (FF, FB, FR x Delta16x2, Abs32) as an aggregate, finds the exclusive prefix by a
-// decoupled look-back over its predecessors' records (a predecessor publishes its aggregate
-// before it looks back, so every wait ends), publishes its inclusive prefix and writes its rows
-// straight from its own row scratch (one slot per resident warp, reused chunk after chunk, so it
-// stays in L2) into the packed lists. Offsets and words equal the two-pass build's: the offsets
-// are the same exclusive prefixes of pitch x 32 per format, in chunk order.
-
-// chunk meta of one list from the lanes' row statistics, the same decision as CommitChunkMeta,
-// known to every lane
-struct ChunkDecision {
-    uint32_t pitch, base, base2;
-    uint8_t fmt;
-};
-__device__ __forceinline__ ChunkDecision DecideChunkMeta(uint32_t chunk, const LaneRefs& r, bool split) {
-    uint32_t pitch = r.cnt & 0xffffu, mn = r.mn, mx = r.mx, hm = r.homeMin, flm = r.farLoMax, fhm = r.farHiMin;
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) {
-        pitch = max(pitch, __shfl_xor_sync(0xffffffffu, pitch, d));
-        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
-        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
-        if (split) {
-            hm = min(hm, __shfl_xor_sync(0xffffffffu, hm, d));
-            flm = max(flm, __shfl_xor_sync(0xffffffffu, flm, d));
-            fhm = min(fhm, __shfl_xor_sync(0xffffffffu, fhm, d));
-        }
-    }
-    ChunkDecision c;
-    c.pitch = pitch;
-    if (pitch == 0) { c.base = 0; c.base2 = 0x8000u; c.fmt = FMT_ABS32; return c; }
-    const uint32_t span = (mx >= mn) ? (mx - mn) : 0xffffffffu;
-    if (mx >= mn && span <= 0xffffu) { c.base = mn; c.base2 = mn + 0x8000u; c.fmt = FMT_DELTA16X2; return c; }
-    if (split) {
-        uint32_t lo, hi;
-        HomeWindow(chunk, lo, hi);
-        const bool hasLo = mn < lo, hasHi = mx > hi;
-        const uint32_t farMin = hasLo ? mn : fhm;
-        const uint32_t farMax = hasLo ? flm : mx;
-        if (hasLo != hasHi && hm <= hi && farMax - farMin <= 0x7fffu) {
-            c.base = hm; c.base2 = farMin; c.fmt = FMT_DELTA16X2;
-            return c;
-        }
-    }
-    c.base = mn; c.base2 = mn + 0x8000u; c.fmt = FMT_ABS32;
-    return c;
-}
-
-constexpr uint32_t LB_AGGREGATE = 1u, LB_INCLUSIVE = 2u;
-constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;  // bounded wait per record (~seconds), then ERR_LOOKBACK
-
-__device__ __forceinline__ void LbPublish(unsigned long long* rec, uint32_t epoch, uint32_t state, const uint64_t v[6]) {
-    volatile unsigned long long* r = rec;
-#pragma unroll
-    for (int k = 0; k < 6; k++) r[1 + k] = v[k];
-    __threadfence();
-    r[0] = ((unsigned long long)epoch << 2) | state;
-}
-
-// exclusive prefix of the six sums at `chunk`, 32 predecessors per round (lane l reads chunk
-// - 1 - l - 32 * round); the nearest inclusive record ends the walk. False if a record never
-// appeared within the spin limit.
-__device__ __forceinline__ bool LbExclusive(const unsigned long long* lb, uint32_t chunk, uint32_t epoch, uint32_t lane,
-                                            uint64_t out[6]) {
-#pragma unroll
-    for (int k = 0; k < 6; k++) out[k] = 0;
-    int64_t top = (int64_t)chunk - 1;
-    while (top >= 0) {
-        const int64_t p = top - (int64_t)lane;
-        uint32_t state = LB_INCLUSIVE;  // before chunk 0: an inclusive zero
-        const volatile unsigned long long* r = lb + (p >= 0 ? (size_t)p * LB_WORDS : 0);
-        if (p >= 0) {
-            state = 0;
-            for (uint32_t spins = 0; spins < LB_SPIN_LIMIT; spins++) {
-                const unsigned long long w = r[0];
-                if ((uint32_t)(w >> 2) == (epoch & 0x3fffffffu) && (w & 3ull) != 0ull) { state = (uint32_t)(w & 3ull); break; }
-            }
-        }
-        if (__any_sync(0xffffffffu, state == 0)) return false;
-        const uint32_t incMask = __ballot_sync(0xffffffffu, state == LB_INCLUSIVE);
-        const uint32_t first = incMask ? (uint32_t)(__ffs(incMask) - 1) : 31u;
-        const bool take = p >= 0 && lane <= first;
-        uint64_t v[6];
-        __threadfence();
-#pragma unroll
-        for (int k = 0; k < 6; k++) v[k] = take ? r[1 + k] : 0ull;
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1)
-#pragma unroll
-            for (int k = 0; k < 6; k++) v[k] += __shfl_xor_sync(0xffffffffu, v[k], d);
-#pragma unroll
-        for (int k = 0; k < 6; k++) out[k] += v[k];
-        if (incMask) break;
-        top -= 32;
-    }
-    return true;
-}
-
-#ifndef TSP_FUSED_MIN_BLOCKS
-#define TSP_FUSED_MIN_BLOCKS 8
-#endif
-__global__ void __launch_bounds__(QUERY_THREADS, TSP_FUSED_MIN_BLOCKS) KQueryFluidFused(QueryArgs a, SellMeta mFF, SellMeta mFB,
-                                                                                        SellMeta mFR) {
-    extern __shared__ uint2 qsm[];
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t slot = blockIdx.x * (QUERY_THREADS / 32) + warp;
-    const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
-    uint32_t* sF = a.scrF + (uint64_t)slot * a.ksF * SELL_W + lane;
-    uint32_t* sB = a.scrB + (uint64_t)slot * a.ksB * SELL_W + lane;
-    uint32_t* sR = a.scrR + (uint64_t)slot * a.ksR * SELL_W + lane;
-    const QueryWarp w = QueryWarpSmem(qsm, warp, a.fr.reach);
-    for (;;) {
-        uint32_t chunk = 0;
-        if (lane == 0) chunk = atomicAdd(a.ticket, 1u);
-        chunk = __shfl_sync(0xffffffffu, chunk, 0);
-        if (chunk >= nChunks) return;  // uniform per warp
-        const QueryScene sc = ResolveScene(a, chunk);
-        const QueryLaneInfo q = QuerySetup(a, chunk, lane, w);
-        uint32_t homeLo, homeHi;
-        HomeWindow(chunk, homeLo, homeHi);
-        LaneRefs rFF, rFB, rFR;
-        rFF.init(); rFB.init(); rFR.init();
-        LaneWriter none;
-        QuerySpecies<0, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFF, sF, a.ksF, none, mFF);
-        QuerySpecies<1, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFB, sB, a.ksB, none, mFB);
-        QuerySpecies<2, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFR, sR, a.ksR, none, mFR);
-        if (rFF.cnt) rFF.mn = sF[0];
-        if (rFB.cnt) rFB.mn = sB[0];
-        const uint32_t over = (__any_sync(0xffffffffu, rFF.cnt > a.ksF) ? 1u : 0u) |
-                              (__any_sync(0xffffffffu, rFB.cnt > a.ksB) ? 2u : 0u) |
-                              (__any_sync(0xffffffffu, rFR.cnt > a.ksR) ? 4u : 0u);
-        {
-            uint32_t mn = rFF.mn, mx = rFF.mx;
-#pragma unroll
-            for (int d = 16; d > 0; d >>= 1) {
-                mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, d));
-                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, d));
-            }
-            if (mx >= mn && mx - mn > 0xffffu) {
-                if (!(over & 1u)) {
-                    HomeStatsFromScratch(sF, rFF, homeLo, homeHi);
-                } else {
-                    LaneRefs st;
-                    st.init();
-                    QuerySpecies<0, WALK_STATS>(a, sc, w, q, lane, homeLo, homeHi, st, nullptr, 0, none, mFF);
-                    rFF.homeMin = st.homeMin; rFF.farLoMax = st.farLoMax; rFF.farHiMin = st.farHiMin;
-                }
-            }
-        }
-        if (q.inRange) {
-            if ((rFF.cnt | rFB.cnt | rFR.cnt) > 0xffffu) atomicOr(a.err, ERR_COUNT_U16);
-            mFF.counts[q.i] = (uint16_t)rFF.cnt;
-            mFB.counts[q.i] = (uint16_t)rFB.cnt;
-            mFR.counts[q.i] = (uint16_t)rFR.cnt;
-        }
-        {
-            uint32_t t0 = rFF.cnt & 0xffffu, t1 = rFB.cnt & 0xffffu, t2 = rFR.cnt & 0xffffu;
-#pragma unroll
-            for (int d = 16; d > 0; d >>= 1) {
-                t0 += __shfl_xor_sync(0xffffffffu, t0, d);
-                t1 += __shfl_xor_sync(0xffffffffu, t1, d);
-                t2 += __shfl_xor_sync(0xffffffffu, t2, d);
-            }
-            if (lane == 0 && a.nbrTotals) {
-                atomicAdd(a.nbrTotals + 0, (unsigned long long)t0);
-                atomicAdd(a.nbrTotals + 1, (unsigned long long)t1);
-                atomicAdd(a.nbrTotals + 2, (unsigned long long)t2);
-            }
-        }
-        const ChunkDecision dF = DecideChunkMeta(chunk, rFF, true);
-        const ChunkDecision dB = DecideChunkMeta(chunk, rFB, false);
-        const ChunkDecision dR = DecideChunkMeta(chunk, rFR, false);
-        // slice sizes of this chunk: (FF, FB, FR) x (Delta16x2, Abs32)
-        uint64_t agg[6];
-        agg[0] = dF.fmt == FMT_DELTA16X2 ? (uint64_t)dF.pitch * SELL_W : 0ull;
-        agg[1] = dF.fmt == FMT_DELTA16X2 ? 0ull : (uint64_t)dF.pitch * SELL_W;
-        agg[2] = dB.fmt == FMT_DELTA16X2 ? (uint64_t)dB.pitch * SELL_W : 0ull;
-        agg[3] = dB.fmt == FMT_DELTA16X2 ? 0ull : (uint64_t)dB.pitch * SELL_W;
-        agg[4] = dR.fmt == FMT_DELTA16X2 ? (uint64_t)dR.pitch * SELL_W : 0ull;
-        agg[5] = dR.fmt == FMT_DELTA16X2 ? 0ull : (uint64_t)dR.pitch * SELL_W;
-        unsigned long long* rec = a.lookback + (size_t)chunk * LB_WORDS;
-        uint64_t excl[6];
-        if (chunk == 0) {
-            if (lane == 0) LbPublish(rec, a.epoch & 0x3fffffffu, LB_INCLUSIVE, agg);
-#pragma unroll
-            for (int k = 0; k < 6; k++) excl[k] = 0;
-        } else {
-            if (lane == 0) LbPublish(rec, a.epoch & 0x3fffffffu, LB_AGGREGATE, agg);
-            if (!LbExclusive(a.lookback, chunk, a.epoch, lane, excl) && lane == 0) atomicOr(a.err, ERR_LOOKBACK);
-            uint64_t inc[6];
-#pragma unroll
-            for (int k = 0; k < 6; k++) inc[k] = excl[k] + agg[k];
-            if (lane == 0) LbPublish(rec, a.epoch & 0x3fffffffu, LB_INCLUSIVE, inc);
-        }
-        if (chunk == nChunks - 1 && lane == 0 && a.sellTotals) {
-            for (int k = 0; k < 3; k++) a.sellTotals[k] = U64x2{excl[2 * k] + agg[2 * k], excl[2 * k + 1] + agg[2 * k + 1]};
-        }
-        // chunk meta and offsets for the sweeps
-        const uint64_t oF = dF.fmt == FMT_DELTA16X2 ? excl[0] : excl[1];
-        const uint64_t oB = dB.fmt == FMT_DELTA16X2 ? excl[2] : excl[3];
-        const uint64_t oR = dR.fmt == FMT_DELTA16X2 ? excl[4] : excl[5];
-        if (lane == 0) {
-            const SellMeta* ms[3] = {&mFF, &mFB, &mFR};
-            const ChunkDecision* ds[3] = {&dF, &dB, &dR};
-            const uint64_t os[3] = {oF, oB, oR};
-            for (int k = 0; k < 3; k++) {
-                ms[k]->pitch[chunk] = (uint16_t)ds[k]->pitch;
-                ms[k]->format[chunk] = ds[k]->fmt;
-                ms[k]->base[chunk] = ds[k]->base;
-                ms[k]->base2[chunk] = ds[k]->base2;
-                ms[k]->offset[chunk] = os[k];
-            }
-        }
-        // rows -> packed lists
-        LaneWriter wFF, wFB, wFR;
-        wFF.wr = 0; wFF.pitch = dF.pitch; wFF.base = dF.base; wFF.base2 = dF.base2; wFF.off = oF; wFF.fmt = dF.fmt;
-        wFB.wr = 0; wFB.pitch = dB.pitch; wFB.base = dB.base; wFB.base2 = dB.base2; wFB.off = oB; wFB.fmt = dB.fmt;
-        wFR.wr = 0; wFR.pitch = dR.pitch; wFR.base = dR.base; wFR.base2 = dR.base2; wFR.off = oR; wFR.fmt = dR.fmt;
-        wFF.capSilent = wFB.capSilent = wFR.capSilent = true;
-        if (!(over & 1u)) EncodeFromScratch(mFF, wFF, sF, q.inRange ? rFF.cnt : 0u, lane, a.err);
-        if (!(over & 2u)) EncodeFromScratch(mFB, wFB, sB, q.inRange ? rFB.cnt : 0u, lane, a.err);
-        if (!(over & 4u)) EncodeFromScratch(mFR, wFR, sR, q.inRange ? rFR.cnt : 0u, lane, a.err);
-        if (over) {
-            LaneRefs nr;
-            nr.init();
-            if (over & 1u) QuerySpecies<0, WALK_FILL>(a, sc, w, q, lane, 0u, 0u, nr, nullptr, 0u, wFF, mFF);
-            if (over & 2u) QuerySpecies<1, WALK_FILL>(a, sc, w, q, lane, 0u, 0u, nr, nullptr, 0u, wFB, mFB);
-            if (over & 4u) QuerySpecies<2, WALK_FILL>(a, sc, w, q, lane, 0u, 0u, nr, nullptr, 0u, wFR, mFR);
-        }
-        if (q.inRange && wFR.wr > 1) {
-            const uint64_t last = wFR.off + (uint64_t)(wFR.wr - 1u) * SELL_W + lane;
-            if (last < (wFR.fmt == FMT_DELTA16X2 ? mFR.cap16 : mFR.cap32)) SortRowSell(mFR, wFR, lane);
-        }
-        __syncwarp();
-    }
-}
-
-uint32_t QueryFusedWarps(uint32_t nF, uint32_t reach) {
-    const uint32_t nChunks = (nF + SELL_W - 1) / SELL_W;
-    if (nChunks == 0) return 0;
-    int dev = 0, sms = 0, perSM = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = QueryWarpSmemBytes(reach) * (QUERY_THREADS / 32);
-    cudaFuncSetAttribute(KQueryFluidFused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, KQueryFluidFused, QUERY_THREADS, smem);
-    if (perSM <= 0) perSM = 1;
-    const uint32_t warpsPerBlock = QUERY_THREADS / 32;
-    const uint32_t blocks = std::min<uint32_t>((nChunks + warpsPerBlock - 1) / warpsPerBlock,
-                                               (uint32_t)perSM * (uint32_t)std::max(sms, 1));
-    return blocks * warpsPerBlock;
-}
-
-void LaunchQueryFluidFused(const QueryArgs& a, const SellMeta& ff, const SellMeta& fb, const SellMeta& fr,
-                           cudaStream_t s) {
-    const uint32_t warps = QueryFusedWarps(a.nF, a.fr.reach);
-    if (warps == 0) return;
-    const size_t smem = QueryWarpSmemBytes(a.fr.reach) * (QUERY_THREADS / 32);
-    KQueryFluidFused<<<warps / (QUERY_THREADS / 32), QUERY_THREADS, smem, s>>>(a, ff, fb, fr);
 }
 
 uint32_t QueryCap(uint32_t reach) { return QueryRangeCap(reach); }
