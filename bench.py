@@ -11,6 +11,9 @@ working set (~0.3 GB) is larger than L2, so no flush is needed between steps.
 value: fluid particles x steps / device time (CUDA events on the backend stream, timed region
 bracketed by a barrier and device synchronisation, max over ranks). Multi-GPU: independent
 replicas (one scene per GPU, no inter-GPU traffic) -> weak scaling.
+developed: the same run continued to step 1,000 (the collapse under way, more Jacobi sweeps per
+step), then 20 steps timed the same way.
+tuned: the autotuner's launch configurations (tune.cu), chosen during the first warm-up step.
 e2e: the same metric through the C ABI with pinned host buffers: per step pull_state (H2D of
 the step's particle state) + step + push_state (D2H of positions, velocities, pressure,
 density).
@@ -136,6 +139,44 @@ def profiled_traffic():
     return None
 
 
+def profiled_issue():
+    """Issue and L1 figures of the KJacobi launch from its committed ncu summary (lines
+    `issue_active_pct = X`, `l1_wavefronts_pct_of_peak = Y`): what bounds the sweep besides HBM."""
+    p = os.path.join(ROOT, "profiles", "KJacobi_iisph_dam_1M.md")
+    out = {}
+    try:
+        with open(p) as f:
+            for line in f:
+                t = line.strip()
+                for key in ("issue_active_pct", "l1_wavefronts_pct_of_peak", "warp_instructions_per_pair_slot"):
+                    if t.startswith(key):
+                        out[key] = float(t.split("=")[1].strip().split()[0])
+    except (OSError, ValueError, IndexError):
+        pass
+    return out or None
+
+
+def cpu_description():
+    """Host CPU model and the widest x86 SIMD extension it reports (for the CPU baselines)."""
+    model, flags = None, set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name") and model is None:
+                    model = line.split(":", 1)[1].strip()
+                elif line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    break
+    except OSError:
+        pass
+    simd = "avx512f" if "avx512f" in flags else "avx2" if "avx2" in flags else "sse4_2" if "sse4_2" in flags else None
+    return {"cpu_model": model, "simd": simd}
+
+
+DEVELOPED_AT = 1000
+DEVELOPED_STEPS = 20
+
+
 def build_workload(rank=0):
     from turbospharticles_b200 import scene as S
     st, dmin, dmax, p = S.dam_1m(seed=replica_seed(42, rank))
@@ -172,7 +213,8 @@ def run_b200(args):
     be.run_stage(abi.STAGE_BOUNDARY_VOLUMES, p)
     stream = torch.cuda.ExternalStream(be.stream_handle(), device=dev)
     for _ in range(args.warmup):
-        be.step(p)
+        be.step(p)  # the first step also runs the autotuner (tune.cu) for this size class
+    tuned = abi.tuning(local)
     # ---- device-timed region (clock sampling already running when it starts)
     step_ms, iters, phases = [], [], []
     with ClockSampler(local) as clk:
@@ -204,6 +246,8 @@ def run_b200(args):
     bytes_per_particle = 32.0 + L + 4.0
     jac_ms = be.time_stage(abi.STAGE_JACOBI_UPDATE, reps=20, params=p)
     pacc_ms = be.time_stage(abi.STAGE_PRESSURE_ACC, reps=20, params=p)
+    phase_p50 = {k: float(np.median([ph[k] for ph in phases if k in ph])) for k in (phases[-1] if phases else {})}
+    largest = max(phase_p50, key=phase_p50.get) if phase_p50 else None
     achieved = bytes_per_particle * nF / (jac_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
     traffic = profiled_traffic()
@@ -212,7 +256,35 @@ def run_b200(args):
             "peak_source": peak_kind, "traffic": (traffic or {}).get("bytes_per_launch_scaled"),
             "algorithmic_bytes_per_launch": int(bytes_per_particle * nF), "ms_per_launch": round(jac_ms, 4),
             "pressure_acc_ms_per_launch": round(pacc_ms, 4),
-            "bytes_per_particle": round(bytes_per_particle, 2), "list_bytes_per_particle": round(L, 2)}
+            "bytes_per_particle": round(bytes_per_particle, 2), "list_bytes_per_particle": round(L, 2),
+            "issue": profiled_issue(),
+            "largest_phase_of_window": {"phase": largest, "p50_ms": round(phase_p50.get(largest, 0.0), 4)}}
+    # ---- developed flow: the same run continued to step DEVELOPED_AT (the collapse under way,
+    # more Jacobi sweeps per step), then DEVELOPED_STEPS steps timed the same way
+    developed = None
+    if not args.no_developed:
+        done = args.warmup + args.steps
+        if DEVELOPED_AT > done:
+            be.step(p, DEVELOPED_AT - done)
+        barrier(dist, dev)
+        torch.cuda.synchronize(dev)
+        d_ms, d_it = [], []
+        e4 = torch.cuda.Event(enable_timing=True)
+        e5 = torch.cuda.Event(enable_timing=True)
+        e4.record(stream)
+        for _ in range(DEVELOPED_STEPS):
+            be.step(p)
+            sd = be.stats()
+            d_ms.append(sd.lastStepMs)
+            d_it.append(sd.solverIters - 1)
+        e5.record(stream)
+        torch.cuda.synchronize(dev)
+        dev_ms = max_over_ranks(dist, e4.elapsed_time(e5), dev)
+        dq = np.percentile(d_ms, [50, 99])
+        developed = {"from_step": max(DEVELOPED_AT, done), "steps": DEVELOPED_STEPS, "unit": UNIT,
+                     "value": round(aggregate_rate(nF * DEVELOPED_STEPS, ws, dev_ms), 1),
+                     "p50_step_ms": round(float(dq[0]), 4), "p99_step_ms": round(float(dq[1]), 4),
+                     "jacobi_sweeps_per_step": round(float(np.mean(d_it)), 2)}
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -266,10 +338,9 @@ def run_b200(args):
         "p50_step_ms": round(float(q[0]), 4), "p99_step_ms": round(float(q[1]), 4),
         "jacobi_sweeps": sweeps, "jacobi_iters_per_s": round(sweeps * ws / (elapsed_ms / 1e3), 1),
         "neighbor_ms_last": round(s.lastNeighborMs, 4), "jacobi_ms_last": round(s.lastJacobiMs, 4),
-        "phase_ms_p50": {k: round(float(np.median([ph[k] for ph in phases if k in ph])), 4)
-                         for k in (phases[-1] if phases else {})},
-        "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches),
-        "clocks": clk.summary(), "served": served, "impl": "b200",
+        "phase_ms_p50": {k: round(v, 4) for k, v in phase_p50.items()},
+        "roofline": roof, "developed": developed, "tuned": tuned, "e2e": e2e, "cpu_baseline": cpu,
+        "gpu_launches": int(launches), "clocks": clk.summary(), "served": served, "impl": "b200",
     }
     print(json.dumps(line), flush=True)
 
@@ -308,8 +379,10 @@ def cpu_baseline_from(be, p, dmin, dmax):
         sweeps += o.stats().solverIters - 1
     dt = time.perf_counter() - t0
     return {"value": round(st.N_F * steps / dt, 1), "unit": UNIT, "cores": threads, "kind": "port",
+            **cpu_description(),
             "sample": f"{steps} IISPH steps of the 1M dam from the GPU state after warm-up ({sweeps} Jacobi "
-                      f"sweeps, {dt:.1f} s, oracle/ CPU restatement, OpenMP over {threads} threads)"}
+                      f"sweeps, {dt:.1f} s, oracle/ CPU restatement, scalar per particle (the compiler may "
+                      f"vectorise), OpenMP over {threads} threads)"}
 
 
 def run_reference(args):
@@ -348,6 +421,7 @@ def run_reference(args):
                        "parallelism": f"{threads} host threads"},
             "p50_step_ms": round(float(q[0]), 2), "p99_step_ms": round(float(q[1]), 2), "impl": "reference",
             "cpu_baseline": {"value": round(value, 1), "unit": UNIT, "cores": threads, "kind": "port",
+                             **cpu_description(),
                              "sample": f"{len(times)} IISPH steps of the 1M dam after {args.warmup} warm-up steps "
                                        "(oracle/ CPU restatement; the reference CPU backend needs oneTBB/xsimd/"
                                        "glm/Boost which are not installed)"},
@@ -363,6 +437,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-developed", action="store_true", help="skip the developed-flow sub-measure")
     ap.add_argument("--served-scenes", type=int, default=256,
                     help="scenes of the served-stream sub-measure (0: skip; 256 = the full stream)")
     ap.add_argument("--served-steps", type=int, default=500)

@@ -404,6 +404,22 @@ int tsp_b200_batch_info(const tsp_batch* b, uint32_t* scenes, uint64_t* fluid_pa
 /* device bytes a scene is charged at admission (host arithmetic, no GPU work) */
 uint64_t tsp_b200_batch_scene_bytes(uint32_t n_fluid, uint32_t n_boundary, uint64_t grid_cells);
 
+/* ---- autotuner (no counterpart in the reference: its CUDA kernels use one fixed block size,
+ * source/simulation/GPU/backend/common.cuh:13-14) ---------------------------------------------
+ * The neighbor sweeps and the fluid-query passes exist in several launch configurations (FF
+ * slots per pipelined group, minimum resident blocks per SM). The first step of a backend times
+ * every configuration of each kernel on its live state, once per size class (particle count
+ * rounded to a power of two) and device, and keeps the fastest for all later launches of that
+ * class in the process; the served batch launches the same kernels with the same choices. The
+ * configurations differ in registers and load grouping only, so results are identical whichever
+ * is chosen. tsp_b200_set_autotune(0) makes every launch use the untuned configuration;
+ * tsp_b200_reset_tuning() forgets all choices; tsp_b200_get_tuning writes the choices of a device
+ * as a JSON object ("kernel/nN": {slots, min_blocks, ms, untuned_ms, worst_ms, candidates}) and
+ * its length (without the terminating zero) to *len; out may be NULL to query the length. */
+int tsp_b200_set_autotune(int enabled);
+int tsp_b200_reset_tuning(void);
+int tsp_b200_get_tuning(int device, char* out, uint32_t cap, uint32_t* len);
+
 /* ---- host helpers (no GPU work) -------------------------------------------------------- */
 /* Sim::TryBuildCellCoordFrame (source/simulation/core/cell_frame.h:32-66): inclusive signed
  * cell bounds -> frame origin and dimensions. Fails with TSP_ERR_FRAME, leaving origin/dims

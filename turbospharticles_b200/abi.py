@@ -185,6 +185,9 @@ EXPORTS = {
     "tsp_b200_batch_info": (C.c_int, [_VP, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                       C.POINTER(C.c_uint64), C.POINTER(C.c_float), C.POINTER(C.c_uint64)]),
     "tsp_b200_batch_scene_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint64]),
+    "tsp_b200_set_autotune": (C.c_int, [C.c_int]),
+    "tsp_b200_reset_tuning": (C.c_int, []),
+    "tsp_b200_get_tuning": (C.c_int, [C.c_int, C.c_char_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "tsp_b200_noalloc_setup": (C.c_int, []),
     "tsp_b200_build_cell_table_noalloc": (C.c_int, [_VP, C.c_uint32, _VP, _VP, _VP, _VP]),
     "tsp_b200_noalloc_last_error": (C.c_char_p, []),
@@ -221,3 +224,24 @@ def load_library(path: str | None = None) -> C.CDLL:
     if path is None:
         _LIB = lib
     return lib
+
+
+def set_autotune(enabled: bool) -> None:
+    """Autotuner on (default) or off (every launch uses the untuned configuration)."""
+    load_library().tsp_b200_set_autotune(1 if enabled else 0)
+
+
+def reset_tuning() -> None:
+    load_library().tsp_b200_reset_tuning()
+
+
+def tuning(device: int = 0) -> dict:
+    """The autotuner's choices on a device: {"kernel/nN": {slots, min_blocks, ms, untuned_ms,
+    worst_ms, candidates}}."""
+    import json
+    L = load_library()
+    n = C.c_uint32()
+    L.tsp_b200_get_tuning(device, None, 0, C.byref(n))
+    buf = C.create_string_buffer(n.value + 1)
+    L.tsp_b200_get_tuning(device, buf, n.value + 1, C.byref(n))
+    return json.loads(buf.value.decode() or "{}")

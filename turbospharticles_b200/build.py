@@ -10,11 +10,12 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 from .abi import LIB_PATH, PKG_DIR
 
 CSRC = os.path.join(PKG_DIR, "csrc")
-SOURCES = ["backend.cu", "ns_kernels.cu", "sph_kernels.cu", "rigid_kernels.cu", "noalloc.cu", "batch.cu", "contact_kernels.cu", "stats_kernels.cu", "export_kernels.cu", "surface_kernels.cu"]
+SOURCES = ["backend.cu", "ns_kernels.cu", "sph_kernels.cu", "rigid_kernels.cu", "noalloc.cu", "batch.cu", "contact_kernels.cu", "stats_kernels.cu", "export_kernels.cu", "surface_kernels.cu", "tune.cu"]
 HEADERS = ["common.cuh", "kernels.h", "primitives.cuh", "host_common.h"]
 INCLUDE = os.path.join(os.path.dirname(PKG_DIR), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -42,6 +43,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags=()) -> str:
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(INCLUDE, "tsp_b200.h")]
     objs = []
     host_cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else None
+    cmds = []
     for src in SOURCES:
         obj = os.path.join(build_dir, src.replace(".cu", ".o"))
         objs.append(obj)
@@ -52,7 +54,12 @@ def build(force: bool = False, verbose: bool = False, extra_flags=()) -> str:
                 cmd[1:1] = ["-ccbin", host_cxx]
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     if force or _stale(LIB_PATH, objs):
         cmd = [_nvcc(), *ARCH, "-shared", "-o", LIB_PATH, *objs, "-lcudart"]
         if host_cxx:

@@ -227,6 +227,8 @@ public:
     DBuf<uint32_t> scrF, scrB, scrR;
     DBuf<uint8_t> scrOver;
     uint64_t nNbr[3] = {0, 0, 0};
+    DBuf<float4> tunePos;           // posP kept aside while kernels that rewrite it are tuned
+    DBuf<SolverState> tuneSt;
     DBuf<uint16_t> cntR[3];
     DBuf<uint64_t> offR[3];
     VBuf<uint32_t> listR[3];
@@ -860,6 +862,11 @@ public:
         SellMeta m0 = Meta(0), m1 = Meta(1), m2 = Meta(2);
         RigidLists rl = RLists();
         CK(cudaEventRecord(pev[2], s));
+        EnsureTuned(TUNE_QUERY_COUNT, nF, [&](int v) {
+            QueryArgs t = qa;
+            t.nbrTotals = nullptr;  // tuning runs leave the neighbor totals alone
+            LaunchQueryFluid(false, t, m0, m1, m2, s, v);
+        });
         CK(cudaMemsetAsync(nbrTot.p, 0, 3 * sizeof(unsigned long long), s));
         LaunchQueryFluid(false, qa, m0, m1, m2, s);
         LaunchQueryRigid(false, qa, rl, s);
@@ -882,11 +889,31 @@ public:
         }
         m0 = Meta(0); m1 = Meta(1); m2 = Meta(2);
         rl = RLists();
+        EnsureTuned(TUNE_QUERY_FILL, nF, [&](int v) { LaunchQueryFluid(true, qa, m0, m1, m2, s, v); });
         LaunchQueryFluid(true, qa, m0, m1, m2, s);
         LaunchQueryRigid(true, qa, rl, s);
         CK(cudaEventRecord(pev[5], s));
         launches += 2u * ((nF ? 1u : 0u) + (nR ? 1u : 0u)) + FinalizeSell3Launches(nChunks) + (nR ? 9u : 0u) + 1u;
         listsValid = true;
+    }
+    // first run of a kernel for this size class on this device: time its candidates on the live
+    // state (the autotuner, tune.cu); kernels that rewrite their own inputs run between a save and
+    // a restore of those inputs (positions with pressure, solver state)
+    void EnsureTuned(TuneKernel k, uint32_t n, const std::function<void(int)>& launch, bool savePos = false,
+                     bool saveSolver = false) {
+        if (n == 0 || !TuneEnabled() || TuneChoice(k, n) >= 0) return;
+        if (savePos) {
+            tunePos.ensure(nF);
+            CK(cudaMemcpyAsync(tunePos.p, posP.p, nF * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+        }
+        if (saveSolver) {
+            tuneSt.ensure(1);
+            CK(cudaMemcpyAsync(tuneSt.p, st.p, sizeof(SolverState), cudaMemcpyDeviceToDevice, s));
+        }
+        TuneRun(k, n, launch, s);
+        if (savePos) CK(cudaMemcpyAsync(posP.p, tunePos.p, nF * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+        if (saveSolver) CK(cudaMemcpyAsync(st.p, tuneSt.p, sizeof(SolverState), cudaMemcpyDeviceToDevice, s));
+        CheckErrors();
     }
     QueryArgs MakeQueryArgs() {
         QueryArgs qa{};
@@ -930,6 +957,8 @@ public:
         std::memcpy(&tb, &ctl.target, 4);
         k.push_back(tb); k.push_back(ctl.nF);
         P(st.p); P(partials.p);
+        k.push_back((uint64_t)(int64_t)TuneChoice(TUNE_PRESSURE_ACC, f.n));  // the launched instantiations
+        k.push_back((uint64_t)(int64_t)TuneChoice(TUNE_JACOBI, f.n));
         return k;
     }
     cudaGraphExec_t JacobiGraphFor(const Consts& c, const SolverControl& ctl) {
@@ -1203,9 +1232,11 @@ public:
         CK(cudaEventRecord(ev[1], s));
         FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
         RigidParticlesDev rp = RigidView(); BodyDev bd = BodyView();
+        EnsureTuned(TUNE_DENSITY, nF, [&](int v) { LaunchDensity(c, f, b, r, nv, s, v); });
         LaunchDensity(c, f, b, r, nv, s);
         if (nRB) LaunchRigidClearAddGravity(bd, prm.gravity[0], prm.gravity[1], prm.gravity[2], s);
         CK(cudaEventRecord(pev[6], s));
+        EnsureTuned(TUNE_NON_PRESSURE, nF, [&](int v) { LaunchNonPressure(c, f, b, r, nv, s, v); });
         LaunchNonPressure(c, f, b, r, nv, s);
         if (nRB) {
             LaunchRigidViscousForces(c, rp, f, offR[0].p, listR[0].p, s);
@@ -1214,12 +1245,17 @@ public:
             LaunchRigidUpdateParticles(rp, bd, true, err.p, s);
         }
         CK(cudaEventRecord(pev[7], s));
+        EnsureTuned(TUNE_SOURCE_DIAG, nF, [&](int v) { LaunchSourceDiagInit(c, f, b, r, nv, nullptr, s, v); }, true);
         LaunchSourceDiagInit(c, f, b, r, nv, st.p, s);
         CK(cudaEventRecord(ev[2], s));
         CK(cudaEventRecord(pev[8], s));
         if (nF) {
             partials.ensure(3ull * JacobiBlocks(nF) + 3);
             const SolverControl ctl = Control();
+            EnsureTuned(TUNE_PRESSURE_ACC, nF, [&](int v) { LaunchPressureAcc(c, f, b, r, nv, s, v); });
+            EnsureTuned(TUNE_JACOBI, nF, [&](int v) {
+                LaunchJacobi(c, f, b, r, nv, ctl, st.p, partials.p, 0ull, false, s, v);
+            }, true, true);
             cudaGraphExec_t ex = JacobiGraphFor(c, ctl);
             CK(cudaGraphLaunch(ex, s));
         }
@@ -1584,6 +1620,29 @@ int tsp_b200_destroy(tsp_backend* h) {
     return TSP_OK;
 }
 const char* tsp_b200_name(const tsp_backend*) { return "B200 (sm_100a) IISPH"; }
+int tsp_b200_set_autotune(int enabled) {
+    tsp::SetTuneEnabled(enabled != 0);
+    return TSP_OK;
+}
+int tsp_b200_reset_tuning(void) {
+    tsp::TuneReset();
+    return TSP_OK;
+}
+int tsp_b200_get_tuning(int device, char* out, uint32_t cap, uint32_t* len) {
+    if (!len) { g_lastError = "NULL argument"; return TSP_ERR_INVALID; }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (device >= 0 && cudaSetDevice(device) != cudaSuccess) { g_lastError = "no such device"; return TSP_ERR_NO_DEVICE; }
+    const std::string r = tsp::TuneReport();
+    if (device >= 0) cudaSetDevice(prev);
+    *len = (uint32_t)r.size();
+    if (out && cap) {
+        const size_t n = std::min<size_t>(r.size(), cap - 1);
+        std::memcpy(out, r.data(), n);
+        out[n] = 0;
+    }
+    return TSP_OK;
+}
 int tsp_b200_try_build_cell_frame(const int64_t cell_min[3], const int64_t cell_max[3], int32_t origin[3],
                                   uint32_t dims[3]) {
     if (!cell_min || !cell_max || !origin || !dims) return TSP_ERR_INVALID;

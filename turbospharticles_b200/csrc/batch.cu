@@ -880,6 +880,8 @@ public:
         std::memcpy(&tb, &ctl.target, 4);
         k.push_back(tb);
         P(dSc.p); P(dSolver.p); P(dActive.p); P(dNActive.p); k.push_back(sceneCap);
+        k.push_back((uint64_t)(int64_t)TuneChoice(TUNE_PRESSURE_ACC, f.n));  // the launched instantiations
+        k.push_back((uint64_t)(int64_t)TuneChoice(TUNE_JACOBI, f.n));
         return k;
     }
     cudaGraphExec_t LoopGraphFor(const Consts& c, const SolverControl& ctl) {
@@ -922,6 +924,16 @@ public:
         return ex;
     }
 
+    // the autotuner on the batch's live state, as the one-scene backend does it (tune.cu): kernels
+    // that rewrite the positions' pressure run between a save into the reorder's alternate array
+    // and a restore
+    void EnsureTuned(TuneKernel k, uint32_t n, const std::function<void(int)>& launch, bool savePos = false) {
+        if (n == 0 || !TuneEnabled() || TuneChoice(k, n) >= 0) return;
+        if (savePos) CK(cudaMemcpyAsync(posP2.p, posP.p, (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+        TuneRun(k, n, launch, s);
+        if (savePos) CK(cudaMemcpyAsync(posP.p, posP2.p, (size_t)n * sizeof(float4), cudaMemcpyDeviceToDevice, s));
+        CheckErrors();
+    }
     void Substep(const tsp_params& p) {
         CK(cudaSetDevice(device));
         if (p.kernelRadius != prm.kernelRadius || p.gridCellSizeRatio != prm.gridCellSizeRatio)
@@ -1005,6 +1017,11 @@ public:
         qa.scrF = scrF.p; qa.scrB = scrB.p; qa.scrR = scrR.p; qa.ksF = KS_F; qa.ksB = KS_B; qa.ksR = 0;
         qa.scrOver = scrOver.p;
         qa.chunkLen = chunkLen.p; qa.chunkScene = chunkScene.p; qa.scenes = dGeom.p;
+        EnsureTuned(TUNE_QUERY_COUNT, n, [&](int v) {
+            QueryArgs t = qa;
+            t.nbrTotals = nullptr;
+            LaunchQueryFluid(false, t, Meta(0), Meta(1), Meta(2), s, v);
+        });
         CK(cudaMemsetAsync(nbrTot.p, 0, 3 * sizeof(unsigned long long), s));
         LaunchQueryFluid(false, qa, Meta(0), Meta(1), Meta(2), s);
         FinalizeSell3(Meta(0), Meta(1), Meta(2), nChunks, scanScratch2.p, sellTot.p, s);
@@ -1015,6 +1032,7 @@ public:
             sell[k].n16 = tot[k].a; sell[k].n32 = tot[k].b;
             sell[k].l16.grow(tot[k].a, BATCH_LIST_GROWTH); sell[k].l32.grow(tot[k].b, BATCH_LIST_GROWTH);
         }
+        EnsureTuned(TUNE_QUERY_FILL, n, [&](int v) { LaunchQueryFluid(true, qa, Meta(0), Meta(1), Meta(2), s, v); });
         LaunchQueryFluid(true, qa, Meta(0), Meta(1), Meta(2), s);
         launches += 2 + FinalizeSell3Launches(nChunks);
         // ---- solver stages; the Jacobi loop skips converged scenes
@@ -1023,9 +1041,20 @@ public:
         const BoundaryDev b{posB.p, volB.p, (uint32_t)allocB.cap};
         const RigidDev rd{nullptr, nullptr, nullptr, 0};
         const NeighborView nv{View(0), View(1), View(2)};
+        EnsureTuned(TUNE_DENSITY, f.n, [&](int v) { LaunchDensity(c, f, b, rd, nv, s, v); });
         LaunchDensity(c, f, b, rd, nv, s);
+        EnsureTuned(TUNE_NON_PRESSURE, f.n, [&](int v) { LaunchNonPressure(c, f, b, rd, nv, s, v); });
         LaunchNonPressure(c, f, b, rd, nv, s);
+        EnsureTuned(TUNE_SOURCE_DIAG, f.n, [&](int v) { LaunchSourceDiagInit(c, f, b, rd, nv, nullptr, s, v); }, true);
         LaunchSourceDiagInit(c, f, b, rd, nv, nullptr, s);
+        EnsureTuned(TUNE_PRESSURE_ACC, f.n, [&](int v) { LaunchPressureAcc(c, f, b, rd, nv, s, v); });
+        {
+            const SolverControl tctl{prm.minSolverIters, prm.maxSolverIters, prm.fixedIters, prm.solverTerminationCond,
+                                     prm.densityDevTarget, 0u};
+            EnsureTuned(TUNE_JACOBI, f.n, [&](int v) {
+                LaunchJacobi(c, f, b, rd, nv, tctl, nullptr, nullptr, 0ull, false, s, v);
+            }, true);
+        }
         KBatchSolverReset<<<(sceneCap + 1 + 127) / 128, 128, 0, s>>>(dSolver.p, dActive.p, dSc.p, sceneCap + 1);
         const SolverControl ctl{prm.minSolverIters, prm.maxSolverIters, prm.fixedIters, prm.solverTerminationCond,
                                 prm.densityDevTarget, 0u};

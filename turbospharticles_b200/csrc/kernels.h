@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <functional>
+#include <string>
 #include <vector>
 #include <cuda_runtime.h>
 
@@ -13,6 +15,16 @@
 namespace tsp {
 
 struct U64x2;
+
+// kernels with autotuned launch configurations (tune.cu) and one configuration of a candidate list
+enum TuneKernel : int {
+    TUNE_DENSITY, TUNE_NON_PRESSURE, TUNE_SOURCE_DIAG, TUNE_PRESSURE_ACC, TUNE_JACOBI, TUNE_QUERY_COUNT,
+    TUNE_QUERY_FILL, TUNE_KERNELS
+};
+struct TuneCandidate {
+    uint16_t slots;      // FF list slots per pipelined group (sweeps); 0 where not a parameter
+    uint16_t minBlocks;  // __launch_bounds__ minimum resident blocks per SM
+};
 
 constexpr uint32_t QUERY_THREADS = 128;  // 4 warps = 4 SELL32 chunks per block
 constexpr uint32_t MAX_JACOBI_SWEEPS = 100000;  // hard bound of the device-driven Jacobi loop
@@ -188,8 +200,9 @@ void BuildGrid(const uint64_t* unique, const uint64_t* nCellsDev, uint32_t nMax,
 uint32_t QueryCap(uint32_t reach);
 size_t QueryScratchWords(uint32_t nChunks, uint32_t ks);
 size_t QuerySmemBytes(uint32_t reach);  // dynamic shared memory of one fluid-query block
+const TuneCandidate* QueryCandidates(bool fill, int* n);
 void LaunchQueryFluid(bool fill, const QueryArgs& a, const SellMeta& ff, const SellMeta& fb, const SellMeta& fr,
-                      cudaStream_t s);
+                      cudaStream_t s, int variant = -1);
 void LaunchQueryRigid(bool fill, const QueryArgs& a, const RigidLists& L, cudaStream_t s);
 void FinalizeSell(const SellMeta& m, uint32_t nChunks, U64x2* scratch, U64x2* totals, cudaStream_t s);
 // the FF, FB and FR finalize scans in one launch (up to 65,536 chunks; three scans beyond)
@@ -199,20 +212,34 @@ inline uint32_t FinalizeSell3Launches(uint32_t nChunks) { return nChunks == 0 ? 
 void FinalizeCsr(const uint16_t* counts, uint64_t* off, uint32_t n, uint64_t* scratch, uint64_t* total, cudaStream_t s);
 void LaunchDecodeSellRows(const SellMeta& m, uint32_t nF, const uint64_t* rowOff, uint32_t* out, cudaStream_t s);
 
-// ---- sph_kernels.cu
+// ---- tune.cu: autotuner of launch configurations (block residency, slots in flight)
+const TuneCandidate* TuneCandidates(TuneKernel k, int* n);
+const char* TuneKernelName(TuneKernel k);
+int TuneDefault(TuneKernel k);                 // candidate used while untuned / with tuning off
+int TuneChoice(TuneKernel k, uint32_t n);      // chosen candidate for the size class of n, -1 if none
+bool TuneEnabled();
+void SetTuneEnabled(bool on);
+void TuneReset();
+// times every candidate (one warm-up and three timed launches each, CUDA events on s) with
+// `launch(i)` and records the fastest for the size class of n; returns the choice
+int TuneRun(TuneKernel k, uint32_t n, const std::function<void(int)>& launch, cudaStream_t s);
+std::string TuneReport();  // JSON object of every recorded choice on the current device
+
+// ---- sph_kernels.cu (variant < 0: the autotuner's choice for the size class, else that candidate)
+const TuneCandidate* SweepCandidates(int* n);
 void LaunchDensity(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
-                   cudaStream_t s);
+                   cudaStream_t s, int variant = -1);
 void LaunchNonPressure(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
-                       const NeighborView& nv, cudaStream_t s);
+                       const NeighborView& nv, cudaStream_t s, int variant = -1);
 void LaunchSourceDiagInit(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
-                          const NeighborView& nv, SolverState* st, cudaStream_t s);
+                          const NeighborView& nv, SolverState* st, cudaStream_t s, int variant = -1);
 void LaunchPressureAcc(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
-                       const NeighborView& nv, cudaStream_t s);
+                       const NeighborView& nv, cudaStream_t s, int variant = -1);
 // one relaxed Jacobi sweep with the FP64 error reduction; the last block applies the
 // termination rule and, when `cond` is non-zero, sets the graph's loop condition
 void LaunchJacobi(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
                   const SolverControl& ctl, SolverState* st, double* partials, unsigned long long cond,
-                  bool hasCond, cudaStream_t s);
+                  bool hasCond, cudaStream_t s, int variant = -1);
 uint32_t JacobiBlocks(uint32_t nF);
 void LaunchIntegration(const Consts& c, const FluidDev& f, cudaStream_t s);
 void LaunchBoundaryVolumes(const Consts& c, const float4* posB, uint32_t nB, const uint32_t* startB,

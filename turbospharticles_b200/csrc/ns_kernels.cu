@@ -604,12 +604,13 @@ __device__ __forceinline__ void HomeStatsFromScratch(const uint32_t* scr, LaneRe
 }
 
 // count pass: neighbor counts, chunk compression meta, rows into the per-chunk scratch.
-// Minimum resident blocks per SM, measured on the 1M dam (ms per count pass): 1 (78 registers)
+// Instantiated per minimum resident blocks per SM (QUERY_COUNT_CANDIDATES), chosen by the
+// autotuner; an earlier hand sweep on the 1M dam (ms per count pass): 1 block (78 registers)
 // 0.393, none given (64 registers) 0.350, 9 (56) 0.332, 10 (48) 0.348, 12 (40, spills) 0.338
-#ifndef TSP_QUERY_MIN_BLOCKS
-#define TSP_QUERY_MIN_BLOCKS 9
-#endif
-__global__ void __launch_bounds__(QUERY_THREADS, TSP_QUERY_MIN_BLOCKS) KQueryFluidCount(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
+#define QUERY_COUNT_CANDIDATES(X) X(6) X(8) X(9) X(10) X(12)
+#define QUERY_FILL_CANDIDATES(X) X(8) X(10) X(12) X(16)
+template <int MB>
+__global__ void __launch_bounds__(QUERY_THREADS, MB) KQueryFluidCount(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
     extern __shared__ uint2 qsm[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t chunk = blockIdx.x * (QUERY_THREADS / 32) + warp;
@@ -694,13 +695,11 @@ __device__ __forceinline__ void EncodeFromScratch(const SellMeta& m, LaneWriter&
     }
 }
 
-// fill pass: scratch rows -> SELL32 (a chunk whose scratch overflowed walks its stencil again)
-// fill pass: minimum resident blocks per SM, measured on the 1M dam (ms per fill pass):
-// none given 0.088, 8 0.086, 10 0.084, 12 0.095, 16 0.103
-#ifndef TSP_FILL_MIN_BLOCKS
-#define TSP_FILL_MIN_BLOCKS 10
-#endif
-__global__ void __launch_bounds__(QUERY_THREADS, TSP_FILL_MIN_BLOCKS) KQueryFluidFill(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
+// fill pass: scratch rows -> SELL32 (a chunk whose scratch overflowed walks its stencil again);
+// instantiated per minimum resident blocks per SM (QUERY_FILL_CANDIDATES), an earlier hand sweep
+// on the 1M dam (ms per fill pass): none given 0.088, 8 0.086, 10 0.084, 12 0.095, 16 0.103
+template <int MB>
+__global__ void __launch_bounds__(QUERY_THREADS, MB) KQueryFluidFill(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
     extern __shared__ uint2 qsm[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t chunk = blockIdx.x * (QUERY_THREADS / 32) + warp;
@@ -734,20 +733,41 @@ uint32_t QueryCap(uint32_t reach) { return QueryRangeCap(reach); }
 size_t QuerySmemBytes(uint32_t reach) { return QueryWarpSmemBytes(reach) * (QUERY_THREADS / 32); }
 size_t QueryScratchWords(uint32_t nChunks, uint32_t ks) { return (size_t)nChunks * ks * SELL_W; }
 
+#define TSP_QC_ENTRY(mb) TuneCandidate{0, mb},
+static const TuneCandidate kCountCandidates[] = {QUERY_COUNT_CANDIDATES(TSP_QC_ENTRY)};
+static const TuneCandidate kFillCandidates[] = {QUERY_FILL_CANDIDATES(TSP_QC_ENTRY)};
+#undef TSP_QC_ENTRY
+using QueryKernel = void (*)(QueryArgs, SellMeta, SellMeta, SellMeta);
+#define TSP_QC_FN(mb) &KQueryFluidCount<mb>,
+#define TSP_QF_FN(mb) &KQueryFluidFill<mb>,
+static const QueryKernel kCountFns[] = {QUERY_COUNT_CANDIDATES(TSP_QC_FN)};
+static const QueryKernel kFillFns[] = {QUERY_FILL_CANDIDATES(TSP_QF_FN)};
+#undef TSP_QC_FN
+#undef TSP_QF_FN
+const TuneCandidate* QueryCandidates(bool fill, int* n) {
+    *n = fill ? (int)(sizeof(kFillCandidates) / sizeof(kFillCandidates[0]))
+              : (int)(sizeof(kCountCandidates) / sizeof(kCountCandidates[0]));
+    return fill ? kFillCandidates : kCountCandidates;
+}
+
 void LaunchQueryFluid(bool fill, const QueryArgs& a, const SellMeta& ff, const SellMeta& fb, const SellMeta& fr,
-                      cudaStream_t s) {
+                      cudaStream_t s, int variant) {
     const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
     if (nChunks == 0) return;
     const uint32_t warps = QUERY_THREADS / 32;
     const size_t smem = QueryWarpSmemBytes(a.fr.reach) * warps;
     const uint32_t blocks = (nChunks + warps - 1) / warps;
-    if (fill) {
-        cudaFuncSetAttribute(KQueryFluidFill, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        KQueryFluidFill<<<blocks, QUERY_THREADS, smem, s>>>(a, ff, fb, fr);
-    } else {
-        cudaFuncSetAttribute(KQueryFluidCount, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        KQueryFluidCount<<<blocks, QUERY_THREADS, smem, s>>>(a, ff, fb, fr);
+    int nc = 0;
+    QueryCandidates(fill, &nc);
+    const TuneKernel k = fill ? TUNE_QUERY_FILL : TUNE_QUERY_COUNT;
+    int v = variant;
+    if (v < 0 || v >= nc) {
+        v = TuneChoice(k, a.nF);
+        if (v < 0) v = TuneDefault(k);
     }
+    const QueryKernel fn = fill ? kFillFns[v] : kCountFns[v];
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    fn<<<blocks, QUERY_THREADS, smem, s>>>(a, ff, fb, fr);
 }
 
 // ----------------------------------------------------------------------------- rigid query

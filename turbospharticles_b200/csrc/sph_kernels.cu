@@ -15,49 +15,15 @@
 namespace tsp {
 
 constexpr uint32_t SPH_THREADS = 256;
-// tuning of the neighbor sweeps: FF slots in flight per lane, minimum resident blocks per SM
-#ifndef TSP_SPH_FF_SLOTS
-#define TSP_SPH_FF_SLOTS 4
-#endif
-#ifndef TSP_SPH_MIN_BLOCKS
-#define TSP_SPH_MIN_BLOCKS 4
-#endif
 // 1: grid of resident blocks only (warps loop over chunks); 0: one warp per chunk
 #ifndef TSP_SPH_PERSISTENT
 #define TSP_SPH_PERSISTENT 1
 #endif
-// FF slots per group of the pressure sweeps (pressure acceleration, Jacobi); measured on the 1M
-// dam with the kernel-gradient factor computed per pair: 3 / 2 slots (0.109 / 0.146 ms per
-// launch) against 2 / 2 (0.110 / 0.146) and 4 / 4 (0.116 / 0.158)
-#ifndef TSP_PACC_FF_SLOTS
-#define TSP_PACC_FF_SLOTS 3
-#endif
-#ifndef TSP_JACOBI_FF_SLOTS
-#define TSP_JACOBI_FF_SLOTS 2
-#endif
-// minimum resident blocks per SM of the pressure sweeps; measured on the 1M dam with the
-// gradient factor computed per pair (ms per launch): KPressureAcc 4 / 5 / 6 blocks 0.120 /
-// 0.110 / 0.105 (40 registers at 6), KJacobi 3 / 4 / 5 / 6 blocks 0.148 / 0.147 / 0.153 / 0.16
-#ifndef TSP_PACC_MIN_BLOCKS
-#define TSP_PACC_MIN_BLOCKS 6
-#endif
-#ifndef TSP_JACOBI_MIN_BLOCKS
-#define TSP_JACOBI_MIN_BLOCKS 4
-#endif
-// density sweep: minimum resident blocks per SM, and FF slots per group of the non-pressure and
-// source/diagonal sweeps; measured on the 1M dam (ms per launch): KDensity at 5 (no bound) / 6 /
-// 8 blocks 0.120 / 0.100 / 0.097; KNonPressure / KSourceDiagInit with 4 / 3 / 2 slots 0.186 /
-// 0.175 / 0.176 and 0.149 / 0.147 / 0.138
-#ifndef TSP_DENSITY_MIN_BLOCKS
-#define TSP_DENSITY_MIN_BLOCKS 8
-#endif
-#ifndef TSP_NPSD_FF_SLOTS
-#define TSP_NPSD_FF_SLOTS 2
-#endif
-// non-pressure sweep with 2-slot groups: 4 / 5 / 6 blocks per SM 0.177 / 0.173 / 0.180 ms
-#ifndef TSP_NP_MIN_BLOCKS
-#define TSP_NP_MIN_BLOCKS 5
-#endif
+// Each neighbor sweep is instantiated for every (FF slots per group U, minimum resident blocks
+// per SM MB) pair of SWEEP_CANDIDATES; the autotuner (tune.cu) times them on the live state and
+// picks one per size class. U and MB change register allocation and load grouping, never the
+// order of a sum, so every candidate computes bit-identical results.
+#define TSP_SWEEP_CANDIDATES(X) X(2, 4) X(3, 4) X(4, 4) X(2, 5) X(3, 5) X(4, 5) X(2, 6) X(3, 6) X(4, 6) X(2, 8) X(3, 8) X(4, 8)
 
 struct ChunkCursor {
     uint32_t pitch, cnt, base, base2;
@@ -187,7 +153,8 @@ struct SlicePrefetch {
         if (pf_.issue(nv, lane), pf_.load(nv, chunk + 2u * warps_, nChunks_, lane), true)
 
 // ----------------------------------------------------------------------------- density
-__global__ void __launch_bounds__(SPH_THREADS, TSP_DENSITY_MIN_BLOCKS) KDensity(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv) {
+template <int U, int MB>
+__global__ void __launch_bounds__(SPH_THREADS, MB) KDensity(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv) {
     FOR_EACH_CHUNK_PF(f.n, nv) {
         const uint32_t i = chunk * SELL_W + lane;
         const bool act = LaneActive(f, chunk, lane, i);
@@ -195,7 +162,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_DENSITY_MIN_BLOCKS) KDensity(
         float dF = 0.f, dB = 0.f, dR = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<TSP_SPH_FF_SLOTS, false>(cur, nv.ff, lane, f.posP, nullptr, [&](bool ok, uint32_t, const float4& pj, const float4&) {
+        SweepSlots<U, false>(cur, nv.ff, lane, f.posP, nullptr, [&](bool ok, uint32_t, const float4& pj, const float4&) {
             const float t = fmaf(c.massF, KernelWeight(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z, c), dF);
             dF = ok ? t : dF;
         });
@@ -214,7 +181,8 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_DENSITY_MIN_BLOCKS) KDensity(
 }
 
 // ----------------------------------------------------------------------------- non-pressure
-__global__ void __launch_bounds__(SPH_THREADS, TSP_NP_MIN_BLOCKS) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+template <int U, int MB>
+__global__ void __launch_bounds__(SPH_THREADS, MB) KNonPressure(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
     FOR_EACH_CHUNK_PF(f.n, nv) {
         const uint32_t i = chunk * SELL_W + lane;
@@ -224,7 +192,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_NP_MIN_BLOCKS) KNonPressure(C
         float fx = 0.f, fy = 0.f, fz = 0.f, bx = 0.f, by = 0.f, bz = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<TSP_NPSD_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velRho, [&](bool ok, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<U, true>(cur, nv.ff, lane, f.posP, f.velRho, [&](bool ok, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -268,7 +236,8 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_NP_MIN_BLOCKS) KNonPressure(C
 }
 
 // ----------------------------------------------------------------------------- source / diagonal / init
-__global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagInit(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+template <int U, int MB>
+__global__ void __launch_bounds__(SPH_THREADS, MB) KSourceDiagInit(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                             NeighborView nv) {
     FOR_EACH_CHUNK_PF(f.n, nv) {
         const uint32_t i = chunk * SELL_W + lane;
@@ -279,7 +248,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagIn
         float cxB = 0.f, cyB = 0.f, czB = 0.f, cxR = 0.f, cyR = 0.f, czR = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlots<TSP_NPSD_FF_SLOTS, true>(cur, nv.ff, lane, f.posP, f.velPred, [&](bool ok, uint32_t, const float4& pj, const float4& vj) {
+        SweepSlots<U, true>(cur, nv.ff, lane, f.posP, f.velPred, [&](bool ok, uint32_t, const float4& pj, const float4& vj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
@@ -333,7 +302,8 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_SPH_MIN_BLOCKS) KSourceDiagIn
 }
 
 // ----------------------------------------------------------------------------- pressure acceleration
-__global__ void __launch_bounds__(SPH_THREADS, TSP_PACC_MIN_BLOCKS) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
+template <int U, int MB>
+__global__ void __launch_bounds__(SPH_THREADS, MB) KPressureAcc(Consts c, FluidDev f, BoundaryDev b, RigidDev r,
                                                          NeighborView nv) {
     FOR_EACH_CHUNK_PF(SweepCount(f), nv) {
         if (ChunkSkipped(f, chunk)) continue;  // converged scene of a batch
@@ -344,7 +314,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_PACC_MIN_BLOCKS) KPressureAcc
         float ax = 0.f, ay = 0.f, az = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsGrad<TSP_PACC_FF_SLOTS, false>(cur, nv.ff, lane, pi, c, f.posP, nullptr, [&](bool ok, float kg, const float4& pj, const float4&) {
+        SweepSlotsGrad<U, false>(cur, nv.ff, lane, pi, c, f.posP, nullptr, [&](bool ok, float kg, const float4& pj, const float4&) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float a = (fOuter + c.massF * pj.w * c.densInvSqu) * kg;
             const float tx = fmaf(a, dx, ax), ty = fmaf(a, dy, ay), tz = fmaf(a, dz, az);
@@ -372,7 +342,8 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_PACC_MIN_BLOCKS) KPressureAcc
 
 // ----------------------------------------------------------------------------- relaxed Jacobi sweep
 
-__global__ void __launch_bounds__(SPH_THREADS, TSP_JACOBI_MIN_BLOCKS) KJacobi(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv,
+template <int U, int MB>
+__global__ void __launch_bounds__(SPH_THREADS, MB) KJacobi(Consts c, FluidDev f, BoundaryDev b, RigidDev r, NeighborView nv,
                                                     SolverControl ctl, SolverState* st, double* partials,
                                                     cudaGraphConditionalHandle cond, int hasCond) {
     double eRaw = 0.0, ePos = 0.0, eAbs = 0.0;  // per-lane FP64 sums over the warp's chunks
@@ -386,7 +357,7 @@ __global__ void __launch_bounds__(SPH_THREADS, TSP_JACOBI_MIN_BLOCKS) KJacobi(Co
         float sF = 0.f, sB = 0.f;
         ChunkCursor cur;
         cur.load(nv.ff, chunk, i, act);
-        SweepSlotsGrad<TSP_JACOBI_FF_SLOTS, true>(cur, nv.ff, lane, pi, c, f.posP, f.acc, [&](bool ok, float kg, const float4& pj, const float4& aj) {
+        SweepSlotsGrad<U, true>(cur, nv.ff, lane, pi, c, f.posP, f.acc, [&](bool ok, float kg, const float4& pj, const float4& aj) {
             const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
             const float dax = ai.x - aj.x, day = ai.y - aj.y, daz = ai.z - aj.z;
             const float sv = fmaf(dax, dx, fmaf(day, dy, daz * dz));
@@ -593,30 +564,71 @@ static uint32_t PersistentBlocks(K kernel, uint32_t n) {
 static inline uint32_t SphBlocks(uint32_t n) { return (n + SPH_THREADS - 1) / SPH_THREADS; }
 uint32_t JacobiBlocks(uint32_t nF) { return SphBlocks(nF); }
 
+// candidate tables, in TSP_SWEEP_CANDIDATES order
+#define TSP_CAND_ENTRY(u, mb) TuneCandidate{u, mb},
+static const TuneCandidate kSweepCandidates[] = {TSP_SWEEP_CANDIDATES(TSP_CAND_ENTRY)};
+#undef TSP_CAND_ENTRY
+constexpr int kSweepCandidateCount = (int)(sizeof(kSweepCandidates) / sizeof(kSweepCandidates[0]));
+const TuneCandidate* SweepCandidates(int* n) {
+    *n = kSweepCandidateCount;
+    return kSweepCandidates;
+}
+using SweepKernel = void (*)(Consts, FluidDev, BoundaryDev, RigidDev, NeighborView);
+using JacobiKernel = void (*)(Consts, FluidDev, BoundaryDev, RigidDev, NeighborView, SolverControl, SolverState*,
+                              double*, cudaGraphConditionalHandle, int);
+#define TSP_FN_ENTRY_DENSITY(u, mb) &KDensity<u, mb>,
+#define TSP_FN_ENTRY_NP(u, mb) &KNonPressure<u, mb>,
+#define TSP_FN_ENTRY_SD(u, mb) &KSourceDiagInit<u, mb>,
+#define TSP_FN_ENTRY_PACC(u, mb) &KPressureAcc<u, mb>,
+#define TSP_FN_ENTRY_JAC(u, mb) &KJacobi<u, mb>,
+static const SweepKernel kDensityFns[] = {TSP_SWEEP_CANDIDATES(TSP_FN_ENTRY_DENSITY)};
+static const SweepKernel kNonPressureFns[] = {TSP_SWEEP_CANDIDATES(TSP_FN_ENTRY_NP)};
+static const SweepKernel kSourceDiagFns[] = {TSP_SWEEP_CANDIDATES(TSP_FN_ENTRY_SD)};
+static const SweepKernel kPressureAccFns[] = {TSP_SWEEP_CANDIDATES(TSP_FN_ENTRY_PACC)};
+static const JacobiKernel kJacobiFns[] = {TSP_SWEEP_CANDIDATES(TSP_FN_ENTRY_JAC)};
+#undef TSP_FN_ENTRY_DENSITY
+#undef TSP_FN_ENTRY_NP
+#undef TSP_FN_ENTRY_SD
+#undef TSP_FN_ENTRY_PACC
+#undef TSP_FN_ENTRY_JAC
+
+static int Pick(TuneKernel k, uint32_t n, int variant) {
+    if (variant >= 0 && variant < kSweepCandidateCount) return variant;
+    const int t = TuneChoice(k, n);
+    return t >= 0 ? t : TuneDefault(k);
+}
+static void LaunchSweep(const SweepKernel* fns, TuneKernel k, int variant, const Consts& c, const FluidDev& f,
+                        const BoundaryDev& b, const RigidDev& r, const NeighborView& nv, cudaStream_t s) {
+    if (!f.n) return;
+    const SweepKernel fn = fns[Pick(k, f.n, variant)];
+    fn<<<PersistentBlocks(fn, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+}
+
 void LaunchDensity(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
-                   cudaStream_t s) {
-    if (f.n) KDensity<<<PersistentBlocks(KDensity, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+                   cudaStream_t s, int variant) {
+    LaunchSweep(kDensityFns, TUNE_DENSITY, variant, c, f, b, r, nv, s);
 }
 void LaunchNonPressure(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
-                       const NeighborView& nv, cudaStream_t s) {
-    if (f.n) KNonPressure<<<PersistentBlocks(KNonPressure, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+                       const NeighborView& nv, cudaStream_t s, int variant) {
+    LaunchSweep(kNonPressureFns, TUNE_NON_PRESSURE, variant, c, f, b, r, nv, s);
 }
 void LaunchSourceDiagInit(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
-                          const NeighborView& nv, SolverState* st, cudaStream_t s) {
-    if (f.n) KSourceDiagInit<<<PersistentBlocks(KSourceDiagInit, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+                          const NeighborView& nv, SolverState* st, cudaStream_t s, int variant) {
+    LaunchSweep(kSourceDiagFns, TUNE_SOURCE_DIAG, variant, c, f, b, r, nv, s);
     if (st) KSolverReset<<<1, 1, 0, s>>>(st, f.n);
 }
 void LaunchSolverReset(SolverState* st, uint32_t nF, cudaStream_t s) { KSolverReset<<<1, 1, 0, s>>>(st, nF); }
 void LaunchPressureAcc(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r,
-                       const NeighborView& nv, cudaStream_t s) {
-    if (f.n) KPressureAcc<<<PersistentBlocks(KPressureAcc, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv);
+                       const NeighborView& nv, cudaStream_t s, int variant) {
+    LaunchSweep(kPressureAccFns, TUNE_PRESSURE_ACC, variant, c, f, b, r, nv, s);
 }
 void LaunchJacobi(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,
                   const SolverControl& ctl, SolverState* st, double* partials, unsigned long long cond, bool hasCond,
-                  cudaStream_t s) {
-    if (f.n)
-        KJacobi<<<PersistentBlocks(KJacobi, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv, ctl, st, partials,
-                                                      (cudaGraphConditionalHandle)cond, hasCond ? 1 : 0);
+                  cudaStream_t s, int variant) {
+    if (!f.n) return;
+    const JacobiKernel fn = kJacobiFns[Pick(TUNE_JACOBI, f.n, variant)];
+    fn<<<PersistentBlocks(fn, f.n), SPH_THREADS, 0, s>>>(c, f, b, r, nv, ctl, st, partials,
+                                                         (cudaGraphConditionalHandle)cond, hasCond ? 1 : 0);
 }
 void LaunchIntegration(const Consts& c, const FluidDev& f, cudaStream_t s) {
     if (f.n) KIntegration<<<(f.n + 255) / 256, 256, 0, s>>>(c, f);
