@@ -205,6 +205,9 @@ def run_b200(args):
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     dist = init_dist(ws, "nccl")
+    if args.tuning:
+        with open(args.tuning) as f:
+            abi.pin_tuning(json.load(f), local)
     dev = torch.device("cuda", local)
     st, dmin, dmax, p = build_workload(rank)
     be = SimBackendB200(p, device=local)
@@ -438,6 +441,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-developed", action="store_true", help="skip the developed-flow sub-measure")
+    ap.add_argument("--tuning", default=None,
+                    help="JSON file of launch configurations (a bench line's `tuned` object) to pin instead of tuning")
     ap.add_argument("--served-scenes", type=int, default=256,
                     help="scenes of the served-stream sub-measure (0: skip; 256 = the full stream)")
     ap.add_argument("--served-steps", type=int, default=500)

@@ -415,9 +415,13 @@ uint64_t tsp_b200_batch_scene_bytes(uint32_t n_fluid, uint32_t n_boundary, uint6
  * is chosen. tsp_b200_set_autotune(0) makes every launch use the untuned configuration;
  * tsp_b200_reset_tuning() forgets all choices; tsp_b200_get_tuning writes the choices of a device
  * as a JSON object ("kernel/nN": {slots, min_blocks, ms, untuned_ms, worst_ms, candidates}) and
- * its length (without the terminating zero) to *len; out may be NULL to query the length. */
+ * its length (without the terminating zero) to *len; out may be NULL to query the length.
+ * tsp_b200_set_tuning pins a configuration (one of the kernel's candidates, as the report names
+ * them) for n's size class on a device, e.g. to replay a table saved from an earlier run;
+ * TSP_ERR_INVALID if the kernel or configuration is unknown. */
 int tsp_b200_set_autotune(int enabled);
 int tsp_b200_reset_tuning(void);
+int tsp_b200_set_tuning(int device, const char* kernel, uint32_t n, uint32_t slots, uint32_t min_blocks);
 int tsp_b200_get_tuning(int device, char* out, uint32_t cap, uint32_t* len);
 
 /* ---- host helpers (no GPU work) -------------------------------------------------------- */

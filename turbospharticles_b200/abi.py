@@ -187,6 +187,7 @@ EXPORTS = {
     "tsp_b200_batch_scene_bytes": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint64]),
     "tsp_b200_set_autotune": (C.c_int, [C.c_int]),
     "tsp_b200_reset_tuning": (C.c_int, []),
+    "tsp_b200_set_tuning": (C.c_int, [C.c_int, C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint32]),
     "tsp_b200_get_tuning": (C.c_int, [C.c_int, C.c_char_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "tsp_b200_noalloc_setup": (C.c_int, []),
     "tsp_b200_build_cell_table_noalloc": (C.c_int, [_VP, C.c_uint32, _VP, _VP, _VP, _VP]),
@@ -245,3 +246,13 @@ def tuning(device: int = 0) -> dict:
     buf = C.create_string_buffer(n.value + 1)
     L.tsp_b200_get_tuning(device, buf, n.value + 1, C.byref(n))
     return json.loads(buf.value.decode() or "{}")
+
+
+def pin_tuning(table: dict, device: int = 0) -> None:
+    """Pins the configurations of a tuning report (the dict `tuning()` returns) on a device."""
+    L = load_library()
+    for key, v in table.items():
+        kernel, n = key.split("/n")
+        rc = L.tsp_b200_set_tuning(device, kernel.encode(), int(n), int(v["slots"]), int(v["min_blocks"]))
+        if rc != 0:
+            raise TspError(rc, f"cannot pin {key}: {v}")

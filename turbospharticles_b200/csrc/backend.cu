@@ -1624,6 +1624,16 @@ int tsp_b200_set_autotune(int enabled) {
     tsp::SetTuneEnabled(enabled != 0);
     return TSP_OK;
 }
+int tsp_b200_set_tuning(int device, const char* kernel, uint32_t n, uint32_t slots, uint32_t min_blocks) {
+    if (!kernel) { g_lastError = "NULL argument"; return TSP_ERR_INVALID; }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (device >= 0 && cudaSetDevice(device) != cudaSuccess) { g_lastError = "no such device"; return TSP_ERR_NO_DEVICE; }
+    const bool ok = tsp::TuneSet(kernel, n, slots, min_blocks);
+    if (device >= 0) cudaSetDevice(prev);
+    if (!ok) { g_lastError = "not a tuned kernel or not one of its configurations"; return TSP_ERR_INVALID; }
+    return TSP_OK;
+}
 int tsp_b200_reset_tuning(void) {
     tsp::TuneReset();
     return TSP_OK;

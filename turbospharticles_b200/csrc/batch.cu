@@ -1047,17 +1047,19 @@ public:
         LaunchNonPressure(c, f, b, rd, nv, s);
         EnsureTuned(TUNE_SOURCE_DIAG, f.n, [&](int v) { LaunchSourceDiagInit(c, f, b, rd, nv, nullptr, s, v); }, true);
         LaunchSourceDiagInit(c, f, b, rd, nv, nullptr, s);
-        EnsureTuned(TUNE_PRESSURE_ACC, f.n, [&](int v) { LaunchPressureAcc(c, f, b, rd, nv, s, v); });
-        {
-            const SolverControl tctl{prm.minSolverIters, prm.maxSolverIters, prm.fixedIters, prm.solverTerminationCond,
-                                     prm.densityDevTarget, 0u};
-            EnsureTuned(TUNE_JACOBI, f.n, [&](int v) {
-                LaunchJacobi(c, f, b, rd, nv, tctl, nullptr, nullptr, 0ull, false, s, v);
-            }, true);
-        }
         KBatchSolverReset<<<(sceneCap + 1 + 127) / 128, 128, 0, s>>>(dSolver.p, dActive.p, dSc.p, sceneCap + 1);
         const SolverControl ctl{prm.minSolverIters, prm.maxSolverIters, prm.fixedIters, prm.solverTerminationCond,
                                 prm.densityDevTarget, 0u};
+        {
+            // the loop's kernels are tuned as the loop graph launches them: masked view (live count
+            // on the device, per-chunk FP64 partials, every scene active after the reset above)
+            const FluidDev fm = Fluid(true);
+            EnsureTuned(TUNE_PRESSURE_ACC, fm.n, [&](int v) { LaunchPressureAcc(c, fm, b, rd, nv, s, v); });
+            EnsureTuned(TUNE_JACOBI, fm.n, [&](int v) {
+                LaunchJacobi(c, fm, b, rd, nv, ctl, nullptr, nullptr, 0ull, false, s, v);
+            }, true);
+        }
+        EnsureTuned(TUNE_PRESSURE_ACC, f.n, [&](int v) { LaunchPressureAcc(c, f, b, rd, nv, s, v); });
         CK(cudaGraphLaunch(LoopGraphFor(c, ctl), s));
         LaunchPressureAcc(c, f, b, rd, nv, s);
         LaunchIntegration(c, f, s);

@@ -224,6 +224,9 @@ void TuneReset();
 // `launch(i)` and records the fastest for the size class of n; returns the choice
 int TuneRun(TuneKernel k, uint32_t n, const std::function<void(int)>& launch, cudaStream_t s);
 std::string TuneReport();  // JSON object of every recorded choice on the current device
+// records a given configuration as the choice of `kernel` (a TuneKernelName) for n's size class;
+// false if the kernel or the configuration is not one of the candidates
+bool TuneSet(const char* kernel, uint32_t n, uint32_t slots, uint32_t minBlocks);
 
 // ---- sph_kernels.cu (variant < 0: the autotuner's choice for the size class, else that candidate)
 const TuneCandidate* SweepCandidates(int* n);

@@ -122,6 +122,24 @@ int TuneRun(TuneKernel k, uint32_t n, const std::function<void(int)>& launch, cu
     return best;
 }
 
+bool TuneSet(const char* kernel, uint32_t n, uint32_t slots, uint32_t minBlocks) {
+    for (int k = 0; k < TUNE_KERNELS; k++) {
+        if (std::string(kNames[k]) != kernel) continue;
+        int nc = 0;
+        const TuneCandidate* cand = TuneCandidates((TuneKernel)k, &nc);
+        for (int c = 0; c < nc; c++) {
+            if (cand[c].slots != slots || cand[c].minBlocks != minBlocks) continue;
+            std::lock_guard<std::mutex> lock(g_mutex);
+            TuneEntry& e = g_tables[CurrentDevice()].e[k][SizeClass(n)];
+            e = TuneEntry{};
+            e.choice = c;
+            e.n = n;
+            return true;
+        }
+    }
+    return false;
+}
+
 std::string TuneReport() {
     std::lock_guard<std::mutex> lock(g_mutex);
     std::string out = "{";
