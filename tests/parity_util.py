@@ -39,36 +39,36 @@ def written_slot_mask(meta, n_f, fmt, batch_chunks=4096):
     return mask
 
 
-def assert_neighbor_structures_equal(g, o, n_f, n_b, n_r):
+def assert_neighbor_structures_equal(g, o, n_f, n_b, n_r, what=""):
     """Morton cell IDs, sort permutations, cell tables, all six neighbor row sets and the
     SELL32 encoding (counts, pitch, format, bases, offsets and every written packed word)."""
     for sp, n in ((0, n_f), (1, n_b), (2, n_r)):
         if n == 0:
             continue
-        assert np.array_equal(g.cell_ids(sp), o.cell_ids(sp)), f"cell ids {sp}"
-        assert np.array_equal(g.permutation(sp), o.permutation(sp)), f"permutation {sp}"
+        assert np.array_equal(g.cell_ids(sp), o.cell_ids(sp)), f"{what} cell ids {sp}"
+        assert np.array_equal(g.permutation(sp), o.permutation(sp)), f"{what} permutation {sp}"
         gu, gs = g.cell_table(sp)
         ou, os_ = o.cell_table(sp)
-        assert np.array_equal(gu, ou) and np.array_equal(gs, os_), f"cell table {sp}"
+        assert np.array_equal(gu, ou) and np.array_equal(gs, os_), f"{what} cell table {sp}"
     for lst in range(6):
         go, gi = g.rows(lst)
         oo, oi = o.rows(lst)
-        assert np.array_equal(go, oo), f"row offsets {lst}"
-        assert np.array_equal(gi, oi), f"rows {lst}"
+        assert np.array_equal(go, oo), f"{what} row offsets {lst}"
+        assert np.array_equal(gi, oi), f"{what} rows {lst}: {int((gi != oi).sum()) if gi.size == oi.size else -1} entries differ"
         del gi, oi
     if n_f == 0:
         return
     for lst in range(3):
         gm, om = g.sell32(lst), o.sell32(lst)
         for k in ("counts", "pitch", "format", "base", "offset"):
-            assert np.array_equal(gm[k], om[k]), f"sell32 {lst} {k}"
+            assert np.array_equal(gm[k], om[k]), f"{what} sell32 {lst} {k}"
         # second base: only meaningful for Delta16x2 chunks
         d = om["format"] == 0
-        assert np.array_equal(gm["base2"][d], om["base2"][d]), f"sell32 {lst} base2"
+        assert np.array_equal(gm["base2"][d], om["base2"][d]), f"{what} sell32 {lst} base2"
         assert gm["w16"].size == om["w16"].size and gm["w32"].size == om["w32"].size
         for key, fmt in (("w16", 0), ("w32", 1)):
             mask = written_slot_mask(om, n_f, fmt)
-            assert np.array_equal(gm[key][mask], om[key][mask]), f"sell32 {lst} {key}"
+            assert np.array_equal(gm[key][mask], om[key][mask]), f"{what} sell32 {lst} {key}"
 
 
 def elementwise_errors(a, b, rtol, atol):

@@ -40,7 +40,7 @@ def pull_search_compare(g, o, p, st, what):
     for be in (g, o):
         be.pull(st, p)
         be.neighbor_search(p)
-    assert_neighbor_structures_equal(g, o, st.N_F, st.N_B, 0)
+    assert_neighbor_structures_equal(g, o, st.N_F, st.N_B, 0, what)
     gs, os_ = g.push(), o.push()
     for n in BOUNDARY:
         assert np.array_equal(getattr(gs, n), getattr(os_, n)), (what, n)
