@@ -7,9 +7,17 @@ that has run its steps is retired and its slot and memory are reused. Arrival ti
 compared with the loop's own clock (device-timed substeps), so arrivals that happen while
 other scenes are on the GPU are admitted at the next substep.
 
+Accuracy: after every substep each active scene's average positive density error (the solver's
+own termination measure) must be at most the target (0.1 %) unless the scene's solver stopped at
+its iteration limit; the run reports the largest error seen, the count of scene-steps at the
+limit and `accuracy_ok`.
+
 The comparison path runs the same scenes one at a time on the one-scene backend
 (`SimBackendB200`), the plain path; to bound its run time it times a sample of steps of every
-scene and charges each scene its full step count at the sampled per-step time.
+scene (steps 3-12) and charges each scene its full step count at the sampled per-step time. A
+calibration subset of scenes is also run for the full step count, and the ratio of its full-run
+mean step time to its sampled mean is reported (`full_over_sampled`): the flow develops and
+later steps need more Jacobi sweeps, so the sample makes the plain path look faster than it is.
 
     python -m turbospharticles_b200.serve --scenes 256 --steps 500        # the full stream
 """
@@ -49,10 +57,13 @@ def run_served(prepared, steps, budget_bytes, max_substeps=None):
     queue.sort(key=lambda k: prepared[k][0].arrival_s)
     active = {}   # slot -> (scene index, steps done)
     clock_s = 0.0
-    sub_ms, n_active, particles_per_sub = [], [], []
+    sub_ms, n_active, particles_per_sub, changed_sub = [], [], [], []
     done_updates = 0
     refused = 0
     it = 0
+    target = float(np.float32(p.densityDevTarget))
+    max_err, at_limit, over_target, checked = 0.0, 0, 0, 0
+    changed = True  # admissions or retirements since the last substep (the batch relayouts then)
     t0 = time.perf_counter()
     while queue or active:
         # admit arrived scenes in arrival order while they fit
@@ -68,20 +79,31 @@ def run_served(prepared, steps, budget_bytes, max_substeps=None):
                 break
             active[slot] = [k, 0]
             queue.pop(0)
+            changed = True
         batch.substep(1)
         info = batch.info()
         ms = info["last_substep_ms"]
         sub_ms.append(ms)
+        changed_sub.append(changed)
+        changed = False
         clock_s += ms / 1e3
         nf = sum(prepared[k][0].n_fluid for k, _ in active.values())
         particles_per_sub.append(nf)
         n_active.append(len(active))
         done_updates += nf
         for slot in list(active):
+            s_ = batch.stats(slot)
+            checked += 1
+            if s_.solverIters >= p.maxSolverIters:
+                at_limit += 1
+            else:
+                max_err = max(max_err, float(s_.avgRelDensityErrPos))
+                over_target += 1 if s_.avgRelDensityErrPos > target else 0
             active[slot][1] += 1
             if active[slot][1] >= steps:
                 batch.retire(slot)
                 del active[slot]
+                changed = True
         it += 1
         if max_substeps and it >= max_substeps:
             break
@@ -89,17 +111,32 @@ def run_served(prepared, steps, budget_bytes, max_substeps=None):
     batch.close()
     dev_s = float(np.sum(sub_ms)) / 1e3
     q = np.percentile(sub_ms, [50, 99])
+    ms_a = np.asarray(sub_ms)
+    ch = np.asarray(changed_sub, bool)
+    # substep latency split: substeps after an admission or retirement include the relayout
+    # (whole chunks moved into the alternate arena, new scenes' boundaries sorted and gridded)
+    split = {"relayout_substeps": int(ch.sum()),
+             "relayout_p50_ms": round(float(np.percentile(ms_a[ch], 50)), 4) if ch.any() else None,
+             "steady_p50_ms": round(float(np.percentile(ms_a[~ch], 50)), 4) if (~ch).any() else None,
+             "steady_p99_ms": round(float(np.percentile(ms_a[~ch], 99)), 4) if (~ch).any() else None}
     return {"particle_updates": int(done_updates), "device_s": round(dev_s, 4), "wall_s": round(wall_s, 3),
             "value": round(done_updates / dev_s, 1), "value_wall": round(done_updates / wall_s, 1),
             "substeps": it, "p50_step_ms": round(float(q[0]), 4), "p99_step_ms": round(float(q[1]), 4),
+            "latency_split": split,
             "mean_active_scenes": round(float(np.mean(n_active)), 1), "max_active_scenes": int(np.max(n_active)),
-            "admissions_deferred": refused, "budget_bytes": int(budget_bytes)}
+            "admissions_deferred": refused, "budget_bytes": int(budget_bytes),
+            "accuracy": {"target": target, "max_avg_density_error": max_err, "scene_steps_checked": checked,
+                         "scene_steps_at_iteration_limit": at_limit, "scene_steps_over_target": over_target,
+                         "accuracy_ok": over_target == 0}}
 
 
-def run_plain(prepared, steps, sample_steps=10, warmup=2):
-    """The same scenes one at a time on the one-scene backend (device time per step)."""
+def run_plain(prepared, steps, sample_steps=10, warmup=2, calibrate=16):
+    """The same scenes one at a time on the one-scene backend (device time per step): steps
+    warmup+1 .. warmup+sample_steps of every scene timed and charged for `steps` steps; the
+    first `calibrate` scenes (in stream order) also run all `steps` steps for the sampling's bias."""
     total_updates, total_s, step_ms = 0, 0.0, []
-    for sp, st, dmin, dmax, p in prepared:
+    cal_full, cal_sampled = [], []
+    for idx, (sp, st, dmin, dmax, p) in enumerate(prepared):
         be = SimBackendB200(p)
         be.set_sim_domain_bounds(dmin, dmax)
         be.pull(st, p)
@@ -109,6 +146,13 @@ def run_plain(prepared, steps, sample_steps=10, warmup=2):
         for _ in range(sample_steps):
             be.step(p)
             ms.append(be.stats().lastStepMs)
+        if idx < calibrate:
+            full = list(ms)
+            for _ in range(steps - warmup - sample_steps):
+                be.step(p)
+                full.append(be.stats().lastStepMs)
+            cal_full.append(float(np.mean(full)))
+            cal_sampled.append(float(np.mean(ms)))
         be.close()
         per = float(np.mean(ms))
         step_ms.extend(ms)
@@ -117,7 +161,10 @@ def run_plain(prepared, steps, sample_steps=10, warmup=2):
     q = np.percentile(step_ms, [50, 99])
     return {"particle_updates": int(total_updates), "device_s": round(total_s, 4),
             "value": round(total_updates / total_s, 1), "p50_step_ms": round(float(q[0]), 4),
-            "p99_step_ms": round(float(q[1]), 4), "sampled_steps_per_scene": sample_steps}
+            "p99_step_ms": round(float(q[1]), 4), "sampled_steps_per_scene": sample_steps,
+            "sampling": f"steps {warmup + 1}-{warmup + sample_steps} of each scene timed, charged for {steps} steps",
+            "calibration_scenes": len(cal_full),
+            "full_over_sampled": round(float(np.sum(cal_full) / np.sum(cal_sampled)), 3) if cal_full else None}
 
 
 def main():
