@@ -14,6 +14,8 @@ replicas (one scene per GPU, no inter-GPU traffic) -> weak scaling.
 developed: the same run continued to step 1,000 (the collapse under way, more Jacobi sweeps per
 step), then 20 steps timed the same way.
 tuned: the autotuner's launch configurations (tune.cu), chosen during the first warm-up step.
+other_configs: the 32K dam for its 1,000 steps, the 2M-fluid rigid dam (50 steps) and the
+neighbor-search-only builds at 1M / 4M points, uniform and clustered (--no-configs skips them).
 e2e: the same metric through the C ABI with pinned host buffers: per step pull_state (H2D of
 the step's particle state) + step + push_state (D2H of positions, velocities, pressure,
 density).
@@ -320,6 +322,11 @@ def run_b200(args):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         cpu = cpu_baseline_from(be, p, dmin, dmax)
+    # ---- the other configurations of the workload set, timed the same way (device events)
+    others = None
+    if rank == 0 and ws == 1 and not args.no_configs:
+        be.close()
+        others = other_configs_measure(torch, dev)
     # ---- served mixed-size stream (continuous batching) vs the same scenes one at a time
     served = None
     if rank == 0 and ws == 1 and args.served_scenes > 0:
@@ -343,9 +350,82 @@ def run_b200(args):
         "neighbor_ms_last": round(s.lastNeighborMs, 4), "jacobi_ms_last": round(s.lastJacobiMs, 4),
         "phase_ms_p50": {k: round(v, 4) for k, v in phase_p50.items()},
         "roofline": roof, "developed": developed, "tuned": tuned, "e2e": e2e, "cpu_baseline": cpu,
-        "gpu_launches": int(launches), "clocks": clk.summary(), "served": served, "impl": "b200",
+        "gpu_launches": int(launches), "clocks": clk.summary(), "other_configs": others, "served": served,
+        "impl": "b200",
     }
     print(json.dumps(line), flush=True)
+
+
+def _timed_steps(torch, dev, be, p, steps):
+    stream = torch.cuda.ExternalStream(be.stream_handle(), device=dev)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms, sweeps = [], 0
+    e0.record(stream)
+    for _ in range(steps):
+        be.step(p)
+        s = be.stats()
+        ms.append(s.lastStepMs)
+        sweeps += s.solverIters - 1
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    return e0.elapsed_time(e1), ms, sweeps
+
+
+def other_configs_measure(torch, dev):
+    """The workload set's other configurations on this GPU: the 32K dam for its full 1,000
+    steps, the full-size rigid dam (2,000,000 fluid, 8 cubes) for 50 steps after 5 warm-up, and
+    the neighbor-search-only case (Morton keys, sort, reorder, cell tables, SELL32 count + fill)
+    at 1,048,576 and 4,194,304 points, uniform and clustered, 5 builds each after one warm-up
+    build; algorithmic bytes of a build per point: keys 24 + sort 24 x passes + reorder of every
+    field 68 + cell table 8 + count 18 + fill 12 + list bytes."""
+    from turbospharticles_b200 import abi, scene as S
+    from turbospharticles_b200.backend import SimBackendB200
+    out = {}
+    for name, builder, warm, steps in (("iisph_dam_32k_1000_steps", S.dam_32k, 0, 1000),
+                                       ("rigid_dam_2M_8_cubes", S.rigid_dam, 5, 50)):
+        st, dmin, dmax, p = builder()
+        be = SimBackendB200(p)
+        be.set_sim_domain_bounds(dmin, dmax)
+        be.pull(st, p)
+        be.run_stage(abi.STAGE_BOUNDARY_VOLUMES, p)
+        if warm:
+            be.step(p, warm)
+        el, ms, sweeps = _timed_steps(torch, dev, be, p, steps)
+        q = np.percentile(ms, [50, 99])
+        out[name] = {"n_fluid": st.N_F, "n_boundary": st.N_B, "n_rigid": st.N_R, "steps": steps,
+                     "from_step": warm + 1, "value": round(st.N_F * steps / (el / 1e3), 1), "unit": UNIT,
+                     "p50_step_ms": round(float(q[0]), 4), "p99_step_ms": round(float(q[1]), 4),
+                     "jacobi_sweeps_per_step": round(sweeps / steps, 2)}
+        be.close()
+    ns = {}
+    for n in (1 << 20, 1 << 22):
+        for dist in ("uniform", "clustered"):
+            st, dmin, dmax, p = S.neighbor_search_scene(n, dist, seed=7)
+            be = SimBackendB200(p)
+            be.set_sim_domain_bounds(dmin, dmax)
+            be.pull(st, p)
+            be.neighbor_search(p)
+            stream = torch.cuda.ExternalStream(be.stream_handle(), device=dev)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = 5
+            e0.record(stream)
+            for _ in range(reps):
+                be.neighbor_search(p)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            ms = e0.elapsed_time(e1) / reps
+            s = be.stats()
+            L = s.sellPackedBytes / n + 6.0
+            passes = (s.keyBits + 7) // 8
+            bpp = 24 + 24 * passes + 68 + 8 + 18 + 12 + L
+            ns[f"{dist}_{n}"] = {"ms_per_build": round(ms, 4), "points_per_s": round(n / (ms / 1e3), 1),
+                                 "algorithmic_GBps": round(bpp * n / (ms / 1e3) / 1e9, 1),
+                                 "neighbors_per_point": round(s.nNbrFF / n, 1), "sort_passes": int(passes)}
+            be.close()
+    out["neighbor_search_only"] = ns
+    return out
 
 
 def served_stream_measure(n_scenes, steps):
@@ -444,6 +524,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-developed", action="store_true", help="skip the developed-flow sub-measure")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' sub-measure")
     ap.add_argument("--tuning", default=None,
                     help="JSON file of launch configurations (a bench line's `tuned` object) to pin instead of tuning")
     ap.add_argument("--served-scenes", type=int, default=256,

@@ -198,7 +198,8 @@ public:
     float bMin[3] = {0, 0, 0}, bMax[3] = {0, 0, 0};
     DBuf<uint64_t> keysA, keysB;
     DBuf<uint32_t> valsA, valsB, tileHist, digitTotals;
-    DBuf<uint64_t> keyOrNot;  // OR of the sort keys and of their complements (constant-digit passes)
+    DBuf<uint32_t> osAux;     // one-pass sort: histograms, tickets, look-back status
+    DBuf<uint32_t> cellAux;   // single-pass cell table: ticket and look-back status
     DBuf<uint32_t> permF, permB, permR;
     DBuf<uint64_t> cidF, cidB, cidR, cidRs;
     DBuf<uint64_t> uniqF, uniqB, uniqR;
@@ -290,7 +291,8 @@ public:
     float lastStepMs = 0.f, lastNbrMs = 0.f, lastJacMs = 0.f;
     std::string lastErr;
     uint64_t launches = 0;  // kernels launched by this backend (graph nodes included)
-    static uint32_t SortLaunches(uint32_t n, uint32_t bits) { return n < 2 ? 2u : 2u + 3u * ((bits + 7u) / 8u); }
+    // one-pass sort: the key kernel (with the histograms) and one kernel per 8-bit pass
+    static uint32_t SortLaunches(uint32_t n, uint32_t bits) { return n < 2 ? 3u : 1u + (bits + 7u) / 8u; }
 
     explicit Backend(int dev) {
         int n = 0;
@@ -361,6 +363,8 @@ public:
             throw Error(TSP_ERR_UNSUPPORTED, "a rigid contact particle touches more than 8 bodies");
         if (e & ERR_QUERY_CAP) throw Error(TSP_ERR_UNSUPPORTED, "query stencil exceeds the shared-memory staging");
         if (e & ERR_COUNT_U16) throw Error(TSP_ERR_OVERFLOW, "a neighbor count exceeds uint16 storage");
+        if (e & ERR_SORT_LOOKBACK)
+            throw Error(TSP_ERR_CUDA, "cell sort / cell table: a tile's look-back gave up waiting for its predecessors");
         throw Error(TSP_ERR_NEIGHBOR_LIST, "SELL32 neighbor-list fill overflow / delta range error");
     }
 
@@ -608,9 +612,8 @@ public:
             GatherF4(permB.p, posB.p, posB2.p, nB, s); Swap(posB, posB2);
             GatherF1(permB.p, volB.p, volB2.p, nB, s); Swap(volB, volB2);
             GatherU64(permB.p, idB.p, idB2.p, nB, s); Swap(idB, idB2);
-            BuildCellTable(cidB.p, nB, uniqB.p, startB.p, nCellsDev.p + 1, scanScratch.p, s);
-            BuildGrid(uniqB.p, nCellsDev.p + 1, nB, fr, gridB.p, gridCells, s);
-            launches += SortLaunches(nB, fr.keyBits) + 3 + 3 + 1;
+            BuildCellTableGrid(cidB.p, nB, uniqB.p, startB.p, nCellsDev.p + 1, gridB.p, fr, gridCells, cellAux.p, err.p, s);
+            launches += SortLaunches(nB, fr.keyBits) + 3 + 1;
         }
         if (bState == B_RAW && nB) {
             rawPermB.ensure(nB);
@@ -787,7 +790,8 @@ public:
         valsA.ensure(std::max<uint32_t>(nMax, 1)); valsB.ensure(std::max<uint32_t>(nMax, 1));
         tileHist.ensure(RadixTileHistItems(std::max<uint32_t>(nMax, 1)));
         digitTotals.ensure(256);
-        keyOrNot.ensure(2);
+        osAux.ensure(OnesweepAuxWords(std::max<uint32_t>(nMax, 2), OS_MAX_PASSES));
+        cellAux.ensure(CellTableGridAuxWords(std::max<uint32_t>(nMax, 1)));
         scanScratch.ensure(ScanScratchItems(std::max<uint32_t>(nMax, 1) + 1));
         scanScratch2.ensure(ScanScratchItems(std::max<uint32_t>(nMax, 1) + 1));
         permF.ensure(std::max<uint32_t>(nF, 1)); permB.ensure(std::max<uint32_t>(nB, 1));
@@ -823,7 +827,7 @@ public:
         CK(cudaEventRecord(pev[1], s));
         if (!frameValid) { listsValid = false; return; }
         EnsureNsScratch();
-        SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p, keyOrNot.p};
+        SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p, osAux.p, err.p};
         // boundary: sorted under this frame unless it already is (then its permutation this
         // step is the identity, or, on the first build after a pull that kept a sort of the same
         // raw boundary, that sort's permutation)
@@ -846,17 +850,15 @@ public:
                 GatherF4(permF.p, acc.p, acc2.p, nF, s); Swap(acc, acc2);
                 GatherF2(permF.p, srcDiag.p, srcDiag2.p, nF, s); Swap(srcDiag, srcDiag2);
             }
-            BuildCellTable(cidF.p, nF, uniqF.p, startF.p, nCellsDev.p + 0, scanScratch.p, s);
-            BuildGrid(uniqF.p, nCellsDev.p + 0, nF, fr, gridF.p, gridCells, s);
-            launches += SortLaunches(nF, fr.keyBits) + 1 + (permuteAll ? 3 : 0) + 3 + 1;
+            BuildCellTableGrid(cidF.p, nF, uniqF.p, startF.p, nCellsDev.p + 0, gridF.p, fr, gridCells, cellAux.p, err.p, s);
+            launches += SortLaunches(nF, fr.keyBits) + 1 + (permuteAll ? 3 : 0) + 1;
         }
         // rigid: cell IDs in storage order, sorted index permutation (747-774)
         if (nR) {
             LaunchCellIds(posR.p, nR, fr, cidR.p, s);
             SortByCell(posR.p, nR, fr, sc, permR.p, cidRs.p, s);
-            BuildCellTable(cidRs.p, nR, uniqR.p, startR.p, nCellsDev.p + 2, scanScratch.p, s);
-            BuildGrid(uniqR.p, nCellsDev.p + 2, nR, fr, gridR.p, gridCells, s);
-            launches += 1 + SortLaunches(nR, fr.keyBits) + 3 + 1;
+            BuildCellTableGrid(cidRs.p, nR, uniqR.p, startR.p, nCellsDev.p + 2, gridR.p, fr, gridCells, cellAux.p, err.p, s);
+            launches += 1 + SortLaunches(nR, fr.keyBits) + 1;
         }
         QueryArgs qa = MakeQueryArgs();
         SellMeta m0 = Meta(0), m1 = Meta(1), m2 = Meta(2);
@@ -1401,7 +1403,7 @@ public:
             EnsureNsScratch();
             if (gridCells > gridB.cap) bSortedValid = false;
             gridF.ensure(gridCells); gridB.ensure(gridCells); gridR.ensure(gridCells);
-            SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p, keyOrNot.p};
+            SortScratch sc{keysA.p, keysB.p, valsA.p, valsB.p, tileHist.p, digitTotals.p, osAux.p, err.p};
             EnsureBoundarySorted(sc);
             psiTmpB.ensure(nB);
             LaunchBoundaryVolumes(c, posB.p, nB, startB.p, gridB.p, fr, defVol, defPsi, prm.restDensity, volB.p,

@@ -26,6 +26,7 @@ constexpr uint32_t ERR_RIGID_ATTACH = 1u << 6;     // rigid particle attached to
 constexpr uint32_t ERR_CONTACT_BODIES = 1u << 7;   // a contact element touches too many bodies
 constexpr uint32_t ERR_CONTACT_INVALID = 1u << 8;  // invalid contact diagonal / non-finite error or pressure
                                                    // (rigid_solver.cpp:332-336, 567, 595)
+constexpr uint32_t ERR_SORT_LOOKBACK = 1u << 9;    // a sort pass's look-back gave up waiting (bounded spin)
 
 // cell frame of the compact cell-linked list (source/simulation/core/cell_frame.h:18-26)
 struct Frame {

@@ -58,7 +58,10 @@ struct SortScratch {
     uint32_t* valsB;
     uint32_t* tileHist;
     uint32_t* digitTotals;
-    uint64_t* keyOrNot;  // 2 words: OR of the keys and of their complements (NULL: every pass runs)
+    // one-pass sort (OnesweepSortPairs) when set: its auxiliary words (OnesweepAuxWords; zeroed
+    // by the sort) and the error word of its bounded look-back; NULL: the three-kernel passes
+    uint32_t* osAux;
+    uint32_t* err;
 };
 
 struct QueryArgs {
@@ -197,6 +200,11 @@ void BuildCellTable(const uint64_t* cidSorted, uint32_t n, uint64_t* unique, uin
                     uint64_t* scanScratch, cudaStream_t s);
 void BuildGrid(const uint64_t* unique, const uint64_t* nCellsDev, uint32_t nMax, const Frame& fr, uint32_t* grid,
                uint64_t gridCells, cudaStream_t s);
+// the same table and grid by one single-pass kernel (decoupled look-back); aux: CellTableGridAuxWords(n)
+uint64_t CellTableGridAuxWords(uint32_t n);
+void BuildCellTableGrid(const uint64_t* cidSorted, uint32_t n, uint64_t* unique, uint32_t* start, uint64_t* nCellsDev,
+                        uint32_t* grid, const Frame& fr, uint64_t gridCells, uint32_t* aux, uint32_t* err,
+                        cudaStream_t s);
 uint32_t QueryCap(uint32_t reach);
 size_t QueryScratchWords(uint32_t nChunks, uint32_t ks);
 size_t QuerySmemBytes(uint32_t reach);  // dynamic shared memory of one fluid-query block

@@ -101,41 +101,28 @@ void LaunchProbe(const float4* pos, uint32_t n, const Frame& fr, bool frameValid
 }
 
 // ----------------------------------------------------------------------------- keys
-// clamped keys; with `orNot`, also the OR of all keys and of all complemented keys (block
-// reduction, one atomic pair per block), from which the sort skips passes of constant digits
+// clamped keys; with `hist`, also every sort pass's digit histogram (one-pass sort)
 template <typename K>
 __global__ void __launch_bounds__(256) KKeys(const float4* __restrict__ pos, uint32_t n, Frame fr, uint64_t emptyKey,
                                             K* __restrict__ keys, uint32_t* __restrict__ idx,
-                                            unsigned long long* __restrict__ orNot) {
+                                            uint32_t* __restrict__ hist, uint32_t passes) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t k = 0, kn = 0;
+    uint64_t k = 0;
     if (i < n) {
         const float4 p = pos[i];
         const uint64_t c = CellIdOf(p.x, p.y, p.z, fr);
         k = c < emptyKey ? c : emptyKey;
-        kn = ~k;
         keys[i] = (K)k;
         idx[i] = i;
     }
-    if (orNot == nullptr) return;
-    __shared__ uint64_t so[8], sn[8];
-    uint32_t lo = __reduce_or_sync(0xffffffffu, (uint32_t)k), hi = __reduce_or_sync(0xffffffffu, (uint32_t)(k >> 32));
-    uint32_t nlo = __reduce_or_sync(0xffffffffu, (uint32_t)kn), nhi = __reduce_or_sync(0xffffffffu, (uint32_t)(kn >> 32));
-    const uint32_t warp = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-        so[warp] = ((uint64_t)hi << 32) | lo;
-        sn[warp] = ((uint64_t)nhi << 32) | nlo;
-    }
+    if (hist == nullptr) return;
+    __shared__ uint32_t sh[OS_MAX_PASSES * 256];
+    for (uint32_t b = threadIdx.x; b < passes * 256u; b += blockDim.x) sh[b] = 0;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        uint64_t a = 0, b = 0;
-        for (uint32_t w = 0; w < (blockDim.x >> 5); w++) { a |= so[w]; b |= sn[w]; }
-        // a block whose threads all lie past n contributes nothing (no keys)
-        if (blockIdx.x * blockDim.x < n) {
-            atomicOr(orNot + 0, (unsigned long long)a);
-            atomicOr(orNot + 1, (unsigned long long)b);
-        }
-    }
+    OnesweepCountKey(k, i < n, passes, sh);
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < passes * 256u; b += blockDim.x)
+        if (sh[b]) atomicAdd(hist + b, sh[b]);
 }
 
 // (unclamped) cell IDs in storage order (rigid particles)
@@ -160,20 +147,37 @@ void SortByCell(const float4* pos, uint32_t n, const Frame& fr, SortScratch& sc,
     if (n == 0) return;
     const uint64_t emptyKey = 1ull << (fr.keyBits - 1u);
     const uint32_t g = (n + 255) / 256;
-    unsigned long long* orNot = reinterpret_cast<unsigned long long*>(sc.keyOrNot);
-    if (orNot) cudaMemsetAsync(orNot, 0, 2 * sizeof(uint64_t), s);
+    const uint32_t passes = (fr.keyBits + 7u) / 8u;
+    if (sc.osAux && n >= 2) {
+        // one-pass sort: keys + all histograms in one launch, then one launch per pass; the last
+        // pass writes the permutation and the sorted cell IDs directly
+        cudaMemsetAsync(sc.osAux, 0, OnesweepAuxWords(n, passes) * sizeof(uint32_t), s);
+        const OnesweepAux a = OnesweepLayout(sc.osAux, sc.err, ERR_SORT_LOOKBACK);
+        if (fr.keyBits <= 32) {
+            uint32_t* k0 = reinterpret_cast<uint32_t*>(sc.keysA);
+            uint32_t* k1 = reinterpret_cast<uint32_t*>(sc.keysB);
+            KKeys<uint32_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, k0, sc.valsA, a.hist, passes);
+            OnesweepSortPairs<uint32_t, uint32_t>(k0, sc.valsA, k1, sc.valsB, n, fr.keyBits, a, perm, cidSorted,
+                                                  emptyKey, s);
+        } else {
+            KKeys<uint64_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, sc.keysA, sc.valsA, a.hist, passes);
+            OnesweepSortPairs<uint64_t, uint32_t>(sc.keysA, sc.valsA, sc.keysB, sc.valsB, n, fr.keyBits, a, perm,
+                                                  cidSorted, emptyKey, s);
+        }
+        return;
+    }
     if (fr.keyBits <= 32) {
         uint32_t* k0 = reinterpret_cast<uint32_t*>(sc.keysA);
         uint32_t* k1 = reinterpret_cast<uint32_t*>(sc.keysB);
-        KKeys<uint32_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, k0, sc.valsA, orNot);
+        KKeys<uint32_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, k0, sc.valsA, nullptr, 0);
         const bool alt = RadixSortPairs<uint32_t, uint32_t>(k0, sc.valsA, k1, sc.valsB, n, fr.keyBits, sc.tileHist,
-                                                            sc.digitTotals, s, sc.keyOrNot);
+                                                            sc.digitTotals, s);
         KKeysToCellIds<uint32_t><<<g, 256, 0, s>>>(alt ? k1 : k0, n, emptyKey, cidSorted);
         cudaMemcpyAsync(perm, alt ? sc.valsB : sc.valsA, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     } else {
-        KKeys<uint64_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, sc.keysA, sc.valsA, orNot);
+        KKeys<uint64_t><<<g, 256, 0, s>>>(pos, n, fr, emptyKey, sc.keysA, sc.valsA, nullptr, 0);
         const bool alt = RadixSortPairs<uint64_t, uint32_t>(sc.keysA, sc.valsA, sc.keysB, sc.valsB, n, fr.keyBits,
-                                                            sc.tileHist, sc.digitTotals, s, sc.keyOrNot);
+                                                            sc.tileHist, sc.digitTotals, s);
         KKeysToCellIds<uint64_t><<<g, 256, 0, s>>>(alt ? sc.keysB : sc.keysA, n, emptyKey, cidSorted);
         cudaMemcpyAsync(perm, alt ? sc.valsB : sc.valsA, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     }
@@ -238,6 +242,97 @@ void BuildCellTable(const uint64_t* cidSorted, uint32_t n, uint64_t* unique, uin
                     uint64_t* scanScratch, cudaStream_t s) {
     DeviceScan<uint64_t>(RunFlagIn{cidSorted}, RunFlagOut{cidSorted, unique, start, n}, n, scanScratch, nCellsDev, s);
 }
+
+// Cell table and dense grid in one pass: run starts of the sorted cell IDs by a single-pass
+// scan (tiles of 1024 in ticket order, decoupled look-back on one status word per tile: state in
+// the two high bits, count in the low 30), each run start writing its unique ID, its start and
+// its dense-grid entry. Same tables as BuildCellTable + BuildGrid.
+constexpr uint32_t CT_ITEMS = 4, CT_THREADS = 256, CT_TILE = CT_ITEMS * CT_THREADS;
+inline uint64_t CellTableAuxWords(uint32_t n) { return (n + CT_TILE - 1) / CT_TILE + 64u; }
+__global__ void __launch_bounds__(CT_THREADS) KCellTableGrid(const uint64_t* __restrict__ cid, uint32_t n,
+                                                             uint64_t* __restrict__ unique, uint32_t* __restrict__ start,
+                                                             uint64_t* __restrict__ nCells, uint32_t* __restrict__ grid,
+                                                             Frame fr, uint32_t* __restrict__ aux, uint32_t* err) {
+    __shared__ uint32_t sTile;
+    __shared__ uint64_t sPrefix;
+    if (threadIdx.x == 0) sTile = atomicAdd(aux, 1u);
+    __syncthreads();
+    const uint32_t tile = sTile;
+    volatile uint32_t* status = aux + 64;
+    const uint64_t base = (uint64_t)tile * CT_TILE + (uint64_t)threadIdx.x * CT_ITEMS;
+    uint64_t c[CT_ITEMS];
+    uint32_t f[CT_ITEMS];
+    uint64_t own = 0;
+    const uint64_t prevId = (base > 0 && base - 1 < n) ? cid[base - 1] : 0ull;
+#pragma unroll
+    for (uint32_t k = 0; k < CT_ITEMS; k++) {
+        const uint64_t i = base + k;
+        c[k] = i < n ? cid[i] : 0ull;
+        const uint64_t before = k == 0 ? prevId : c[k - 1];
+        f[k] = (i < n && (i == 0 || c[k] != before)) ? 1u : 0u;
+        own += f[k];
+    }
+    uint64_t tileTotal;
+    uint64_t pre = BlockExclusiveScan<uint64_t>(own, tileTotal);
+    if (threadIdx.x == 0) {
+        uint32_t prefix = 0;
+        if (tile == 0) {
+            status[0] = OS_INC | (uint32_t)tileTotal;
+        } else {
+            status[tile] = OS_AGG | (uint32_t)tileTotal;
+            for (uint32_t p = tile - 1;; p--) {
+                uint32_t w = 0;
+                for (uint32_t spins = 0; spins < OS_SPIN_LIMIT; spins++) {
+                    w = status[p];
+                    if (w & ~OS_VAL) break;
+                }
+                if (!(w & ~OS_VAL)) {
+                    if (err) atomicOr(err, ERR_SORT_LOOKBACK);
+                    break;
+                }
+                prefix += w & OS_VAL;
+                if ((w & ~OS_VAL) == OS_INC || p == 0) break;
+            }
+            status[tile] = OS_INC | ((prefix + (uint32_t)tileTotal) & OS_VAL);
+        }
+        sPrefix = prefix;
+    }
+    __syncthreads();
+    uint64_t run = sPrefix + pre;
+#pragma unroll
+    for (uint32_t k = 0; k < CT_ITEMS; k++) {
+        const uint64_t i = base + k;
+        if (i >= n || run >= n) break;  // (run >= n only after a look-back that gave up)
+        if (f[k]) {
+            unique[run] = c[k];
+            start[run] = (uint32_t)i;
+            if (grid && c[k] != EMPTY_64) {
+                const uint32_t x = Compact21(c[k]), y = Compact21(c[k] >> 1), z = Compact21(c[k] >> 2);
+                grid[(uint64_t)x + (uint64_t)fr.nx * ((uint64_t)y + (uint64_t)fr.ny * z)] = (uint32_t)run;
+            }
+            run++;
+        }
+        if (i == n - 1) {  // sentinel = end of the last run, and the run count
+            start[run] = n;
+            *nCells = run;
+        }
+    }
+}
+// cell table of n sorted cell IDs and, when grid is set, the frame's dense grid (cleared here);
+// `aux` holds CellTableAuxWords(n) words (zeroed here)
+void BuildCellTableGrid(const uint64_t* cidSorted, uint32_t n, uint64_t* unique, uint32_t* start, uint64_t* nCellsDev,
+                        uint32_t* grid, const Frame& fr, uint64_t gridCells, uint32_t* aux, uint32_t* err,
+                        cudaStream_t s) {
+    if (grid) cudaMemsetAsync(grid, 0xff, gridCells * sizeof(uint32_t), s);
+    if (n == 0) {
+        cudaMemsetAsync(nCellsDev, 0, sizeof(uint64_t), s);
+        return;
+    }
+    cudaMemsetAsync(aux, 0, CellTableAuxWords(n) * sizeof(uint32_t), s);
+    const uint32_t tiles = (n + CT_TILE - 1) / CT_TILE;
+    KCellTableGrid<<<tiles, CT_THREADS, 0, s>>>(cidSorted, n, unique, start, nCellsDev, grid, fr, aux, err);
+}
+uint64_t CellTableGridAuxWords(uint32_t n) { return CellTableAuxWords(n); }
 
 __global__ void KGridScatter(const uint64_t* __restrict__ unique, const uint64_t* __restrict__ nCellsDev, Frame fr,
                              uint32_t* __restrict__ grid, uint32_t nMax) {
