@@ -313,6 +313,9 @@ int tsp_b200_fill_statistics(const tsp_backend* h, const tsp_params* params, dou
 int tsp_b200_get_contact_report(const tsp_backend* h, tsp_contact_report* out);
 /* number of CUDA kernels this backend launched since creation (graph nodes included) */
 int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count);
+/* device milliseconds of all steps this backend ran since creation (the sum of the per-step
+ * times of tsp_step_stats.lastStepMs, GetBenchOps analogue, backend_sim.h:255) and their count */
+int tsp_b200_get_step_time_total(const tsp_backend* h, double* ms, uint64_t* steps);
 
 /*
  * Host view of Sync::ExportSnapshot (source/simulation/sync/snapshots.h:37-66): the particles

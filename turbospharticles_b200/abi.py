@@ -164,6 +164,7 @@ EXPORTS = {
     "tsp_b200_write_field": (C.c_int, [_VP, _u32, _VP, _u32]),
     "tsp_b200_time_stage": (C.c_int, [_VP, C.POINTER(TspParams), _u32, _u32, _pf]),
     "tsp_b200_get_launch_count": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
+    "tsp_b200_get_step_time_total": (C.c_int, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "tsp_b200_get_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
     "tsp_b200_fill_statistics": (C.c_int, [_VP, C.POINTER(TspParams), C.POINTER(C.c_double), C.c_uint32]),
     "tsp_b200_get_contact_report": (C.c_int, [_VP, C.POINTER(TspContactReport)]),

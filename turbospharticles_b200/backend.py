@@ -221,6 +221,12 @@ class SimBackendB200:
         self._chk(self.L.tsp_b200_get_launch_count(self.h, C.byref(n)))
         return n.value
 
+    def step_time_total(self) -> tuple:
+        """(device milliseconds, steps) of all steps since creation."""
+        ms, n = C.c_double(), C.c_uint64()
+        self._chk(self.L.tsp_b200_get_step_time_total(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
     def stream_handle(self) -> int:
         s = C.c_void_p()
         self._chk(self.L.tsp_b200_get_stream(self.h, C.byref(s)))

@@ -289,6 +289,8 @@ public:
     }
     bool phaseValid = false;
     float lastStepMs = 0.f, lastNbrMs = 0.f, lastJacMs = 0.f;
+    double stepMsTotal = 0.0;   // device milliseconds of all steps since creation
+    uint64_t stepsTimed = 0;
     std::string lastErr;
     uint64_t launches = 0;  // kernels launched by this backend (graph nodes included)
     // one-pass sort: the key kernel (with the histograms) and one kernel per 8-bit pass
@@ -1291,6 +1293,8 @@ public:
         probeFresh = probeNext;
         float t = 0.f;
         cudaEventElapsedTime(&t, ev[0], pev[12]); lastStepMs = t;
+        stepMsTotal += t;
+        stepsTimed += 1;
         cudaEventElapsedTime(&t, ev[0], ev[1]); lastNbrMs = t;
         cudaEventElapsedTime(&t, ev[2], ev[3]); lastJacMs = t;
         phaseValid = listsValid;
@@ -1931,6 +1935,13 @@ int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count) {
     TSP_NEED(h);
     if (!count) return TSP_ERR_INVALID;
     *count = h->b->launches;
+    return TSP_OK;
+}
+int tsp_b200_get_step_time_total(const tsp_backend* h, double* ms, uint64_t* steps) {
+    TSP_NEED(h);
+    if (!ms || !steps) return TSP_ERR_INVALID;
+    *ms = h->b->stepMsTotal;
+    *steps = h->b->stepsTimed;
     return TSP_OK;
 }
 

@@ -137,20 +137,32 @@ __global__ void __launch_bounds__(256) KBatchProbe(const float4* __restrict__ po
 // empty key, so they stay behind the scene's particles (the sort is stable)
 __global__ void KBatchKeys(const float4* __restrict__ pos, uint32_t n, const uint8_t* __restrict__ chunkLen,
                            const uint32_t* __restrict__ chunkScene, const BatchSceneDev* __restrict__ sc,
-                           uint32_t shift, uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+                           uint32_t shift, uint64_t* __restrict__ keys, uint32_t* __restrict__ idx,
+                           uint32_t* __restrict__ hist, uint32_t passes) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t chunk = i >> 5, lane = i & 31;
-    const uint32_t s = chunkScene[chunk];
-    const BatchSceneDev& d = sc[s];
-    uint64_t k = d.emptyKey;
-    if (lane < (uint32_t)chunkLen[chunk]) {
-        const float4 p = pos[i];
-        const uint64_t c = CellIdOf(p.x, p.y, p.z, d.fr);
-        k = c < d.emptyKey ? c : d.emptyKey;
+    uint64_t key = 0;
+    if (i < n) {
+        const uint32_t chunk = i >> 5, lane = i & 31;
+        const uint32_t s = chunkScene[chunk];
+        const BatchSceneDev& d = sc[s];
+        uint64_t k = d.emptyKey;
+        if (lane < (uint32_t)chunkLen[chunk]) {
+            const float4 p = pos[i];
+            const uint64_t c = CellIdOf(p.x, p.y, p.z, d.fr);
+            k = c < d.emptyKey ? c : d.emptyKey;
+        }
+        key = ((uint64_t)s << shift) | k;
+        keys[i] = key;
+        idx[i] = i;
     }
-    keys[i] = ((uint64_t)s << shift) | k;
-    idx[i] = i;
+    // every pass's digit histogram for the one-pass sort
+    __shared__ uint32_t sh[OS_MAX_PASSES * 256];
+    for (uint32_t b = threadIdx.x; b < passes * 256u; b += blockDim.x) sh[b] = 0;
+    __syncthreads();
+    OnesweepCountKey(key, i < n, passes, sh);
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < passes * 256u; b += blockDim.x)
+        if (sh[b]) atomicAdd(hist + b, sh[b]);
 }
 
 __global__ void KBatchKeysToCellIds(const uint64_t* __restrict__ keys, uint32_t n, const BatchSceneDev* __restrict__ sc,
@@ -381,6 +393,7 @@ public:
     // neighbor build
     DBuf<uint64_t> keysA, keysB, cidF, uniqF, nCellsDev;
     DBuf<uint32_t> valsA, valsB, tileHist, digitTotals, startF, gridF, err;
+    DBuf<uint32_t> osAux, cellAux;  // one-pass sort and single-pass cell table (look-back words)
     DBuf<uint64_t> scanScratch;
     DBuf<U64x2> scanScratch2, sellTot;
     DBuf<unsigned long long> nbrTot;
@@ -715,6 +728,8 @@ public:
         uniqF.ensure(n); startF.ensure(n + 1ull);
         tileHist.ensure(RadixTileHistItems(nSort));
         digitTotals.ensure(256);
+        osAux.ensure(OnesweepAuxWords(std::max<uint32_t>(nSort, 2), OS_MAX_PASSES));
+        cellAux.ensure(CellTableGridAuxWords(std::max<uint32_t>(nSort, 1)));
         scanScratch.ensure(ScanScratchItems(nSort + 1ull));
         scanScratch2.ensure(ScanScratchItems(n + 1ull));
         for (auto& m : sell) {
@@ -859,6 +874,8 @@ public:
         if (!e) return;
         CK(cudaMemset(err.p, 0, 4));
         if (e & ERR_COUNT_U16) throw Error(TSP_ERR_OVERFLOW, "a neighbor count exceeds uint16 storage");
+        if (e & ERR_SORT_LOOKBACK)
+            throw Error(TSP_ERR_CUDA, "cell sort / cell table: a tile's look-back gave up waiting for its predecessors");
         throw Error(TSP_ERR_NEIGHBOR_LIST, "SELL32 neighbor-list fill overflow / delta range error");
     }
 
@@ -994,19 +1011,26 @@ public:
         // ---- fluid: composite keys, one stable sort, reorder, cell table, grids
         const uint32_t n = nFtot;
         const unsigned g = (unsigned)((n + 255) / 256);
-        KBatchKeys<<<g, 256, 0, s>>>(posP.p, n, chunkLen.p, chunkScene.p, dSc.p, shift, keysA.p, valsA.p);
-        const bool alt = RadixSortPairs<uint64_t, uint32_t>(keysA.p, valsA.p, keysB.p, valsB.p, n, shift + rankBits,
-                                                            tileHist.p, digitTotals.p, s);
+        // one-pass sort of the composite keys (histograms counted by the key kernel)
+        const uint32_t sortBits = shift + rankBits;
+        const uint32_t passes = (sortBits + 7u) / 8u;
+        CK(cudaMemsetAsync(osAux.p, 0, OnesweepAuxWords(n, passes) * sizeof(uint32_t), s));
+        const OnesweepAux oa = OnesweepLayout(osAux.p, err.p, ERR_SORT_LOOKBACK);
+        KBatchKeys<<<g, 256, 0, s>>>(posP.p, n, chunkLen.p, chunkScene.p, dSc.p, shift, keysA.p, valsA.p, oa.hist,
+                                     passes);
+        const bool alt = n >= 2 ? OnesweepSortPairsPingPong<uint64_t, uint32_t>(keysA.p, valsA.p, keysB.p, valsB.p, n,
+                                                                                sortBits, oa, s)
+                                : false;
         const uint64_t* sk = alt ? keysB.p : keysA.p;
         const uint32_t* perm = alt ? valsB.p : valsA.p;
         KBatchKeysToCellIds<<<g, 256, 0, s>>>(sk, n, dSc.p, shift, cidF.p);
         LaunchReorderFluidStep(perm, posP.p, velRho.p, idF.p, posP2.p, velRho2.p, idF2.p, n, s);
         Swap(posP, posP2); Swap(velRho, velRho2); Swap(idF, idF2);
-        BuildCellTable(sk, n, uniqF.p, startF.p, nCellsDev.p, scanScratch.p, s);
+        BuildCellTableGrid(sk, n, uniqF.p, startF.p, nCellsDev.p, nullptr, EmptyFrame(), 0, cellAux.p, err.p, s);
         CK(cudaMemsetAsync(gridF.p, 0xff, gridCellsF * sizeof(uint32_t), s));
         KBatchGridScatterF<<<std::min<uint32_t>(g, 148u * 16u), 256, 0, s>>>(uniqF.p, nCellsDev.p, dSc.p, dGeom.p, shift,
                                                                              gridF.p, n);
-        launches += 4 + 3 * ((shift + rankBits + 7) / 8) + 3 + 1;
+        launches += 4 + (n >= 2 ? passes : 0u) + 1 + 1;
         // ---- query count, sizes, fill
         QueryArgs qa{};
         qa.posF = posP.p; qa.cidF = cidF.p; qa.nF = n;

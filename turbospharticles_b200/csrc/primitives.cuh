@@ -502,6 +502,24 @@ __global__ void __launch_bounds__(RS_THREADS) KOnesweepPass(const K* __restrict_
     }
 }
 
+// the passes of a one-pass sort, keys and values ping-ponging between the given buffers (like
+// RadixSortPairs); returns true when the result ended up in the alternate buffers
+template <typename K, typename V>
+bool OnesweepSortPairsPingPong(K* keys, V* vals, K* kAlt, V* vAlt, uint32_t n, uint32_t bits, const OnesweepAux& a,
+                               cudaStream_t s) {
+    const uint32_t nTiles = (n + RS_TILE - 1) / RS_TILE;
+    const uint32_t passes = (bits + 7u) / 8u;
+    K* ks = keys; V* vs = vals; K* kd = kAlt; V* vd = vAlt;
+    bool alt = false;
+    for (uint32_t p = 0; p < passes; p++) {
+        KOnesweepPass<K, V><<<nTiles, RS_THREADS, 0, s>>>(ks, vs, kd, vd, n, p, nTiles, a, nullptr, 0ull);
+        K* tk = ks; ks = kd; kd = tk;
+        V* tv = vs; vs = vd; vd = tv;
+        alt = !alt;
+    }
+    return alt;
+}
+
 // the passes of a one-pass sort over keys whose histograms the key kernel has counted into
 // `a`; the last pass writes the sorted values to vFinal and the sorted keys, as cell IDs
 // (emptyKey -> 0xFF..FF), to cidFinal. Keys and values ping-pong between the given buffers.

@@ -13,11 +13,11 @@ its iteration limit; the run reports the largest error seen, the count of scene-
 limit and `accuracy_ok`.
 
 The comparison path runs the same scenes one at a time on the one-scene backend
-(`SimBackendB200`), the plain path; to bound its run time it times a sample of steps of every
-scene (steps 3-12) and charges each scene its full step count at the sampled per-step time. A
-calibration subset of scenes is also run for the full step count, and the ratio of its full-run
-mean step time to its sampled mean is reported (`full_over_sampled`): the flow develops and
-later steps need more Jacobi sweeps, so the sample makes the plain path look faster than it is.
+(`SimBackendB200`), the plain path, each for the same number of steps as in the served run;
+its device time is the sum of its steps' CUDA-event times. (`--plain-sample K` instead times
+steps 3..K+2 of every scene, charges the full step count at that rate and reports the bias of
+that sampling from 16 scenes run in full: the flow develops and later steps need more Jacobi
+sweeps, so a sample of early steps makes the plain path look faster than it is.)
 
     python -m turbospharticles_b200.serve --scenes 256 --steps 500        # the full stream
 """
@@ -130,16 +130,31 @@ def run_served(prepared, steps, budget_bytes, max_substeps=None):
                          "accuracy_ok": over_target == 0}}
 
 
-def run_plain(prepared, steps, sample_steps=10, warmup=2, calibrate=16):
-    """The same scenes one at a time on the one-scene backend (device time per step): steps
-    warmup+1 .. warmup+sample_steps of every scene timed and charged for `steps` steps; the
-    first `calibrate` scenes (in stream order) also run all `steps` steps for the sampling's bias."""
+def run_plain(prepared, steps, sample_steps=10, warmup=2, calibrate=16, full=True):
+    """The same scenes one at a time on the one-scene backend, device time per step (the
+    backend's CUDA events around each step, summed). full: every scene runs all `steps` steps
+    (the same steps the served run makes), its device time the sum of its steps; the first
+    `calibrate` scenes are stepped one call per step for the per-step percentiles. Otherwise
+    steps warmup+1 .. warmup+sample_steps of every scene are timed and charged for `steps` steps,
+    and the calibration scenes also run in full to show the sampling's bias."""
     total_updates, total_s, step_ms = 0, 0.0, []
     cal_full, cal_sampled = [], []
     for idx, (sp, st, dmin, dmax, p) in enumerate(prepared):
         be = SimBackendB200(p)
         be.set_sim_domain_bounds(dmin, dmax)
         be.pull(st, p)
+        if full:
+            if idx < calibrate:
+                for _ in range(steps):
+                    be.step(p)
+                    step_ms.append(be.stats().lastStepMs)
+            else:
+                be.step(p, steps)
+            ms_total, n = be.step_time_total()
+            be.close()
+            total_updates += sp.n_fluid * steps
+            total_s += ms_total / 1e3
+            continue
         for _ in range(warmup):
             be.step(p)
         ms = []
@@ -147,11 +162,11 @@ def run_plain(prepared, steps, sample_steps=10, warmup=2, calibrate=16):
             be.step(p)
             ms.append(be.stats().lastStepMs)
         if idx < calibrate:
-            full = list(ms)
+            fl = list(ms)
             for _ in range(steps - warmup - sample_steps):
                 be.step(p)
-                full.append(be.stats().lastStepMs)
-            cal_full.append(float(np.mean(full)))
+                fl.append(be.stats().lastStepMs)
+            cal_full.append(float(np.mean(fl)))
             cal_sampled.append(float(np.mean(ms)))
         be.close()
         per = float(np.mean(ms))
@@ -159,12 +174,17 @@ def run_plain(prepared, steps, sample_steps=10, warmup=2, calibrate=16):
         total_updates += sp.n_fluid * steps
         total_s += per * steps / 1e3
     q = np.percentile(step_ms, [50, 99])
-    return {"particle_updates": int(total_updates), "device_s": round(total_s, 4),
-            "value": round(total_updates / total_s, 1), "p50_step_ms": round(float(q[0]), 4),
-            "p99_step_ms": round(float(q[1]), 4), "sampled_steps_per_scene": sample_steps,
-            "sampling": f"steps {warmup + 1}-{warmup + sample_steps} of each scene timed, charged for {steps} steps",
-            "calibration_scenes": len(cal_full),
-            "full_over_sampled": round(float(np.sum(cal_full) / np.sum(cal_sampled)), 3) if cal_full else None}
+    out = {"particle_updates": int(total_updates), "device_s": round(total_s, 4),
+           "value": round(total_updates / total_s, 1), "p50_step_ms": round(float(q[0]), 4),
+           "p99_step_ms": round(float(q[1]), 4)}
+    if full:
+        out["sampling"] = (f"every scene all {steps} steps (device time = sum of the per-step CUDA-event times); "
+                           f"percentiles from the first {min(calibrate, len(prepared))} scenes' steps")
+    else:
+        out["sampling"] = f"steps {warmup + 1}-{warmup + sample_steps} of each scene timed, charged for {steps} steps"
+        out["calibration_scenes"] = len(cal_full)
+        out["full_over_sampled"] = round(float(np.sum(cal_full) / np.sum(cal_sampled)), 3) if cal_full else None
+    return out
 
 
 def main():
@@ -173,13 +193,13 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--rate", type=float, default=64.0, help="Poisson arrival rate, scenes per second")
     ap.add_argument("--budget-gb", type=float, default=16.0)
-    ap.add_argument("--plain-sample", type=int, default=10)
+    ap.add_argument("--plain-sample", type=int, default=0, help="time a sample of K steps per scene (0: all steps)")
     ap.add_argument("--seed", type=int, default=2024)
     args = ap.parse_args()
     specs = S.served_stream(args.scenes, rate_hz=args.rate, seed=args.seed)
     prepared = prepare(specs)
     served = run_served(prepared, args.steps, int(args.budget_gb * (1 << 30)))
-    plain = run_plain(prepared, args.steps, args.plain_sample)
+    plain = run_plain(prepared, args.steps, args.plain_sample or 10, full=args.plain_sample == 0)
     print(json.dumps({"workload": "served_stream", "scenes": args.scenes, "steps_per_scene": args.steps,
                       "rate_hz": args.rate, "n_fluid_total": int(sum(s.n_fluid for s in specs)),
                       "served": served, "plain": plain,
