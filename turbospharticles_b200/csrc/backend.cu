@@ -869,6 +869,7 @@ public:
         EnsureTuned(TUNE_QUERY_COUNT, nF, [&](int v) {
             QueryArgs t = qa;
             t.nbrTotals = nullptr;  // tuning runs leave the neighbor totals alone
+            t.nF = std::min(nF, TUNE_MAX_N);
             LaunchQueryFluid(false, t, m0, m1, m2, s, v);
         });
         CK(cudaMemsetAsync(nbrTot.p, 0, 3 * sizeof(unsigned long long), s));
@@ -893,7 +894,11 @@ public:
         }
         m0 = Meta(0); m1 = Meta(1); m2 = Meta(2);
         rl = RLists();
-        EnsureTuned(TUNE_QUERY_FILL, nF, [&](int v) { LaunchQueryFluid(true, qa, m0, m1, m2, s, v); });
+        EnsureTuned(TUNE_QUERY_FILL, nF, [&](int v) {
+            QueryArgs t = qa;
+            t.nF = std::min(nF, TUNE_MAX_N);
+            LaunchQueryFluid(true, t, m0, m1, m2, s, v);
+        });
         LaunchQueryFluid(true, qa, m0, m1, m2, s);
         LaunchQueryRigid(true, qa, rl, s);
         CK(cudaEventRecord(pev[5], s));
@@ -1236,11 +1241,12 @@ public:
         CK(cudaEventRecord(ev[1], s));
         FluidDev f = FluidView(); BoundaryDev b = BoundaryView(); RigidDev r = RigidDevView(); NeighborView nv = NView();
         RigidParticlesDev rp = RigidView(); BodyDev bd = BodyView();
-        EnsureTuned(TUNE_DENSITY, nF, [&](int v) { LaunchDensity(c, f, b, r, nv, s, v); });
+        const FluidDev ft = TuneView(f, nF);
+        EnsureTuned(TUNE_DENSITY, nF, [&](int v) { LaunchDensity(c, ft, b, r, nv, s, v); });
         LaunchDensity(c, f, b, r, nv, s);
         if (nRB) LaunchRigidClearAddGravity(bd, prm.gravity[0], prm.gravity[1], prm.gravity[2], s);
         CK(cudaEventRecord(pev[6], s));
-        EnsureTuned(TUNE_NON_PRESSURE, nF, [&](int v) { LaunchNonPressure(c, f, b, r, nv, s, v); });
+        EnsureTuned(TUNE_NON_PRESSURE, nF, [&](int v) { LaunchNonPressure(c, ft, b, r, nv, s, v); });
         LaunchNonPressure(c, f, b, r, nv, s);
         if (nRB) {
             LaunchRigidViscousForces(c, rp, f, offR[0].p, listR[0].p, s);
@@ -1249,16 +1255,16 @@ public:
             LaunchRigidUpdateParticles(rp, bd, true, err.p, s);
         }
         CK(cudaEventRecord(pev[7], s));
-        EnsureTuned(TUNE_SOURCE_DIAG, nF, [&](int v) { LaunchSourceDiagInit(c, f, b, r, nv, nullptr, s, v); }, true);
+        EnsureTuned(TUNE_SOURCE_DIAG, nF, [&](int v) { LaunchSourceDiagInit(c, ft, b, r, nv, nullptr, s, v); }, true);
         LaunchSourceDiagInit(c, f, b, r, nv, st.p, s);
         CK(cudaEventRecord(ev[2], s));
         CK(cudaEventRecord(pev[8], s));
         if (nF) {
             partials.ensure(3ull * JacobiBlocks(nF) + 3);
             const SolverControl ctl = Control();
-            EnsureTuned(TUNE_PRESSURE_ACC, nF, [&](int v) { LaunchPressureAcc(c, f, b, r, nv, s, v); });
+            EnsureTuned(TUNE_PRESSURE_ACC, nF, [&](int v) { LaunchPressureAcc(c, ft, b, r, nv, s, v); });
             EnsureTuned(TUNE_JACOBI, nF, [&](int v) {
-                LaunchJacobi(c, f, b, r, nv, ctl, st.p, partials.p, 0ull, false, s, v);
+                LaunchJacobi(c, ft, b, r, nv, ctl, st.p, partials.p, 0ull, false, s, v);
             }, true, true);
             cudaGraphExec_t ex = JacobiGraphFor(c, ctl);
             CK(cudaGraphLaunch(ex, s));

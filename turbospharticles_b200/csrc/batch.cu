@@ -1044,6 +1044,7 @@ public:
         EnsureTuned(TUNE_QUERY_COUNT, n, [&](int v) {
             QueryArgs t = qa;
             t.nbrTotals = nullptr;
+            t.nF = std::min(n, TUNE_MAX_N);
             LaunchQueryFluid(false, t, Meta(0), Meta(1), Meta(2), s, v);
         });
         CK(cudaMemsetAsync(nbrTot.p, 0, 3 * sizeof(unsigned long long), s));
@@ -1056,7 +1057,11 @@ public:
             sell[k].n16 = tot[k].a; sell[k].n32 = tot[k].b;
             sell[k].l16.grow(tot[k].a, BATCH_LIST_GROWTH); sell[k].l32.grow(tot[k].b, BATCH_LIST_GROWTH);
         }
-        EnsureTuned(TUNE_QUERY_FILL, n, [&](int v) { LaunchQueryFluid(true, qa, Meta(0), Meta(1), Meta(2), s, v); });
+        EnsureTuned(TUNE_QUERY_FILL, n, [&](int v) {
+            QueryArgs t = qa;
+            t.nF = std::min(n, TUNE_MAX_N);
+            LaunchQueryFluid(true, t, Meta(0), Meta(1), Meta(2), s, v);
+        });
         LaunchQueryFluid(true, qa, Meta(0), Meta(1), Meta(2), s);
         launches += 2 + FinalizeSell3Launches(nChunks);
         // ---- solver stages; the Jacobi loop skips converged scenes
@@ -1065,11 +1070,12 @@ public:
         const BoundaryDev b{posB.p, volB.p, (uint32_t)allocB.cap};
         const RigidDev rd{nullptr, nullptr, nullptr, 0};
         const NeighborView nv{View(0), View(1), View(2)};
-        EnsureTuned(TUNE_DENSITY, f.n, [&](int v) { LaunchDensity(c, f, b, rd, nv, s, v); });
+        const FluidDev ft = TuneView(f, nFtot);
+        EnsureTuned(TUNE_DENSITY, f.n, [&](int v) { LaunchDensity(c, ft, b, rd, nv, s, v); });
         LaunchDensity(c, f, b, rd, nv, s);
-        EnsureTuned(TUNE_NON_PRESSURE, f.n, [&](int v) { LaunchNonPressure(c, f, b, rd, nv, s, v); });
+        EnsureTuned(TUNE_NON_PRESSURE, f.n, [&](int v) { LaunchNonPressure(c, ft, b, rd, nv, s, v); });
         LaunchNonPressure(c, f, b, rd, nv, s);
-        EnsureTuned(TUNE_SOURCE_DIAG, f.n, [&](int v) { LaunchSourceDiagInit(c, f, b, rd, nv, nullptr, s, v); }, true);
+        EnsureTuned(TUNE_SOURCE_DIAG, f.n, [&](int v) { LaunchSourceDiagInit(c, ft, b, rd, nv, nullptr, s, v); }, true);
         LaunchSourceDiagInit(c, f, b, rd, nv, nullptr, s);
         KBatchSolverReset<<<(sceneCap + 1 + 127) / 128, 128, 0, s>>>(dSolver.p, dActive.p, dSc.p, sceneCap + 1);
         const SolverControl ctl{prm.minSolverIters, prm.maxSolverIters, prm.fixedIters, prm.solverTerminationCond,
@@ -1078,12 +1084,13 @@ public:
             // the loop's kernels are tuned as the loop graph launches them: masked view (live count
             // on the device, per-chunk FP64 partials, every scene active after the reset above)
             const FluidDev fm = Fluid(true);
-            EnsureTuned(TUNE_PRESSURE_ACC, fm.n, [&](int v) { LaunchPressureAcc(c, fm, b, rd, nv, s, v); });
+            const FluidDev fmt = TuneView(fm, nFtot);  // live chunks only, per-chunk partials kept
+            EnsureTuned(TUNE_PRESSURE_ACC, fm.n, [&](int v) { LaunchPressureAcc(c, fmt, b, rd, nv, s, v); });
             EnsureTuned(TUNE_JACOBI, fm.n, [&](int v) {
-                LaunchJacobi(c, fm, b, rd, nv, ctl, nullptr, nullptr, 0ull, false, s, v);
+                LaunchJacobi(c, fmt, b, rd, nv, ctl, nullptr, nullptr, 0ull, false, s, v);
             }, true);
         }
-        EnsureTuned(TUNE_PRESSURE_ACC, f.n, [&](int v) { LaunchPressureAcc(c, f, b, rd, nv, s, v); });
+        EnsureTuned(TUNE_PRESSURE_ACC, f.n, [&](int v) { LaunchPressureAcc(c, ft, b, rd, nv, s, v); });
         CK(cudaGraphLaunch(LoopGraphFor(c, ctl), s));
         LaunchPressureAcc(c, f, b, rd, nv, s);
         LaunchIntegration(c, f, s);

@@ -236,6 +236,18 @@ std::string TuneReport();  // JSON object of every recorded choice on the curren
 // false if the kernel or the configuration is not one of the candidates
 bool TuneSet(const char* kernel, uint32_t n, uint32_t slots, uint32_t minBlocks);
 
+// Tuning launches cover at most the first TUNE_MAX_N particles (a multiple of the SELL32 chunk):
+// every size class at or above it shares one choice, timed on that many particles, so tuning a
+// large scene or batch costs no more than tuning a 2^20-particle one.
+constexpr uint32_t TUNE_MAX_N = 1u << 20;
+// the view a tuning launch sweeps: the first min(live, TUNE_MAX_N) particles, all their chunks
+__host__ __device__ inline FluidDev TuneView(FluidDev f, uint32_t live) {
+    f.n = live < TUNE_MAX_N ? live : TUNE_MAX_N;
+    f.liveN = nullptr;
+    f.sceneActive = nullptr;
+    return f;
+}
+
 // ---- sph_kernels.cu (variant < 0: the autotuner's choice for the size class, else that candidate)
 const TuneCandidate* SweepCandidates(int* n);
 void LaunchDensity(const Consts& c, const FluidDev& f, const BoundaryDev& b, const RigidDev& r, const NeighborView& nv,

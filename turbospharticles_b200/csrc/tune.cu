@@ -5,8 +5,9 @@
 // pipelined group (the sweeps' loads in flight) and the minimum resident blocks per SM of
 // __launch_bounds__ (which sets the register budget and so the occupancy). Which one is fastest
 // depends on the scene (neighbor counts, list formats) and the GPU, so it is measured, not set:
-// the first time a kernel runs for a size class (particle count rounded to a power of two) on a
-// device, the caller hands TuneRun a launcher and every candidate is timed on the live state --
+// the first time a kernel runs for a size class (particle count rounded to a power of two, all
+// counts from 2^20 up in one class) on a device, the caller hands TuneRun a launcher and every
+// candidate is timed on the live state (its first 2^20 particles at most) --
 // one warm-up launch, then three launches between CUDA events on the caller's stream -- and the
 // fastest is kept for that class. Candidates change register allocation and load grouping, never
 // the order of a sum, so the choice does not change any result bit.
@@ -47,7 +48,8 @@ int CurrentDevice() {
     cudaGetDevice(&d);
     return d;
 }
-int SizeClass(uint32_t n) {
+int SizeClass(uint32_t n) {  // bit length of n, sizes from TUNE_MAX_N up share one class
+    if (n > TUNE_MAX_N) n = TUNE_MAX_N;
     int b = 0;
     while (n) { b++; n >>= 1; }
     return b;

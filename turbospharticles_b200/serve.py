@@ -123,6 +123,8 @@ def run_served(prepared, steps, budget_bytes, max_substeps=None):
             "value": round(done_updates / dev_s, 1), "value_wall": round(done_updates / wall_s, 1),
             "substeps": it, "p50_step_ms": round(float(q[0]), 4), "p99_step_ms": round(float(q[1]), 4),
             "latency_split": split,
+            "longest_substeps_ms": [round(float(x), 2) for x in np.sort(ms_a)[-8:][::-1]],
+            "substeps_over_20ms_s": round(float(ms_a[ms_a > 20.0].sum()) / 1e3, 3),
             "mean_active_scenes": round(float(np.mean(n_active)), 1), "max_active_scenes": int(np.max(n_active)),
             "admissions_deferred": refused, "budget_bytes": int(budget_bytes),
             "accuracy": {"target": target, "max_avg_density_error": max_err, "scene_steps_checked": checked,
