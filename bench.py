@@ -442,7 +442,8 @@ def served_stream_measure(n_scenes, steps):
             "n_fluid_total": int(sum(sp.n_fluid for sp in specs)), "unit": UNIT,
             "value": sv["value"], "value_wall": sv["value_wall"], "p50_step_ms": sv["p50_step_ms"],
             "p99_step_ms": sv["p99_step_ms"], "mean_active_scenes": sv["mean_active_scenes"],
-            "latency_split": sv["latency_split"], "accuracy": sv["accuracy"],
+            "latency_split": sv["latency_split"], "longest_substeps_ms": sv["longest_substeps_ms"],
+            "substeps_over_20ms_s": sv["substeps_over_20ms_s"], "accuracy": sv["accuracy"],
             "plain_value": pl["value"], "plain_p50_step_ms": pl["p50_step_ms"],
             "plain_p99_step_ms": pl["p99_step_ms"], "plain_sampling": pl["sampling"],
             "served_over_plain": round(sv["value"] / pl["value"], 3)}

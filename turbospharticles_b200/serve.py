@@ -119,6 +119,13 @@ def run_served(prepared, steps, budget_bytes, max_substeps=None):
              "relayout_p50_ms": round(float(np.percentile(ms_a[ch], 50)), 4) if ch.any() else None,
              "steady_p50_ms": round(float(np.percentile(ms_a[~ch], 50)), 4) if (~ch).any() else None,
              "steady_p99_ms": round(float(np.percentile(ms_a[~ch], 99)), 4) if (~ch).any() else None}
+    # what the slowest 1 % of substeps have in common: fluid particles in flight and relayouts
+    pp = np.asarray(particles_per_sub, np.float64)
+    tail = ms_a >= q[1]
+    split.update({"tail_substeps": int(tail.sum()), "tail_after_relayout": int((tail & ch).sum()),
+                  "tail_mean_fluid": int(pp[tail].mean()), "all_mean_fluid": int(pp.mean()),
+                  "tail_us_per_1k_fluid": round(float((ms_a[tail] / pp[tail]).mean()) * 1e6, 3),
+                  "all_us_per_1k_fluid": round(float((ms_a / pp).mean()) * 1e6, 3)})
     return {"particle_updates": int(done_updates), "device_s": round(dev_s, 4), "wall_s": round(wall_s, 3),
             "value": round(done_updates / dev_s, 1), "value_wall": round(done_updates / wall_s, 1),
             "substeps": it, "p50_step_ms": round(float(q[0]), 4), "p99_step_ms": round(float(q[1]), 4),
