@@ -211,6 +211,9 @@ def run_b200(args):
     if args.tuning:
         with open(args.tuning) as f:
             abi.pin_tuning(json.load(f), local)
+    for spec in args.pin or []:  # KERNEL:SLOTS:MINBLOCKS at every particle count
+        kernel, slots, mb = spec.split(":")
+        abi.pin_tuning({f"{kernel}/n{1 << k}": {"slots": int(slots), "min_blocks": int(mb)} for k in range(22)}, local)
     dev = torch.device("cuda", local)
     st, dmin, dmax, p = build_workload(rank)
     be = SimBackendB200(p, device=local)
@@ -528,6 +531,9 @@ def main():
     ap.add_argument("--no-configs", action="store_true", help="skip the other configurations' sub-measure")
     ap.add_argument("--tuning", default=None,
                     help="JSON file of launch configurations (a bench line's `tuned` object) to pin instead of tuning")
+    ap.add_argument("--pin", action="append", default=None, metavar="KERNEL:SLOTS:MINBLOCKS",
+                    help="pin one kernel's configuration at every particle count (repeatable), "
+                         "e.g. KQueryFluidCount:1:5 for the staged count pass")
     ap.add_argument("--served-scenes", type=int, default=256,
                     help="scenes of the served-stream sub-measure (0: skip; 256 = the full stream)")
     ap.add_argument("--served-steps", type=int, default=500)

@@ -410,12 +410,14 @@ uint64_t tsp_b200_batch_scene_bytes(uint32_t n_fluid, uint32_t n_boundary, uint6
 /* ---- autotuner (no counterpart in the reference: its CUDA kernels use one fixed block size,
  * source/simulation/GPU/backend/common.cuh:13-14) ---------------------------------------------
  * The neighbor sweeps and the fluid-query passes exist in several launch configurations (FF
- * slots per pipelined group, minimum resident blocks per SM). The first step of a backend times
- * every configuration of each kernel on its live state, once per size class (particle count
- * rounded to a power of two) and device, and keeps the fastest for all later launches of that
+ * slots per pipelined group, minimum resident blocks per SM; for KQueryFluidCount, slots = 1
+ * selects the variant that stages the neighboring cell blocks in shared memory). The first step
+ * of a backend times every configuration of each kernel on its live state (its first 2^20
+ * particles at most), once per size class (particle count rounded to a power of two, all counts
+ * from 2^20 up in one class) and device, and keeps the fastest for all later launches of that
  * class in the process; the served batch launches the same kernels with the same choices. The
- * configurations differ in registers and load grouping only, so results are identical whichever
- * is chosen. tsp_b200_set_autotune(0) makes every launch use the untuned configuration;
+ * configurations differ in registers, load grouping and staging only, never in the candidates
+ * or the order of a sum, so results are identical whichever is chosen. tsp_b200_set_autotune(0) makes every launch use the untuned configuration;
  * tsp_b200_reset_tuning() forgets all choices; tsp_b200_get_tuning writes the choices of a device
  * as a JSON object ("kernel/nN": {slots, min_blocks, ms, untuned_ms, worst_ms, candidates}) and
  * its length (without the terminating zero) to *len; out may be NULL to query the length.

@@ -367,6 +367,8 @@ public:
         if (e & ERR_COUNT_U16) throw Error(TSP_ERR_OVERFLOW, "a neighbor count exceeds uint16 storage");
         if (e & ERR_SORT_LOOKBACK)
             throw Error(TSP_ERR_CUDA, "cell sort / cell table: a tile's look-back gave up waiting for its predecessors");
+        if (e & ERR_STAGE_WAIT)
+            throw Error(TSP_ERR_CUDA, "neighbor query: a block's staging copies did not complete");
         throw Error(TSP_ERR_NEIGHBOR_LIST, "SELL32 neighbor-list fill overflow / delta range error");
     }
 

@@ -27,6 +27,7 @@ constexpr uint32_t ERR_CONTACT_BODIES = 1u << 7;   // a contact element touches 
 constexpr uint32_t ERR_CONTACT_INVALID = 1u << 8;  // invalid contact diagonal / non-finite error or pressure
                                                    // (rigid_solver.cpp:332-336, 567, 595)
 constexpr uint32_t ERR_SORT_LOOKBACK = 1u << 9;    // a sort pass's look-back gave up waiting (bounded spin)
+constexpr uint32_t ERR_STAGE_WAIT = 1u << 10;      // a staged query block's bulk copies did not complete (bounded wait)
 
 // cell frame of the compact cell-linked list (source/simulation/core/cell_frame.h:18-26)
 struct Frame {

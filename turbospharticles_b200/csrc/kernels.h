@@ -22,7 +22,7 @@ enum TuneKernel : int {
     TUNE_QUERY_FILL, TUNE_KERNELS
 };
 struct TuneCandidate {
-    uint16_t slots;      // FF list slots per pipelined group (sweeps); 0 where not a parameter
+    uint16_t slots;      // FF list slots per pipelined group (sweeps); count pass: 1 = cell blocks staged in shared memory
     uint16_t minBlocks;  // __launch_bounds__ minimum resident blocks per SM
 };
 

@@ -7,17 +7,21 @@
 // Pipeline of one build (reference: ReOrderParticleData + Construct + Query_Count +
 // Finalize_Count + Query_Fill, source/simulation/CPU/backend/neighbor_search.cpp:613-1848):
 //   KProbe          AABB of positions + "left the inner frame" flag -> host frame rule
-//   KKeys           clamped Morton key per particle (min(cellId, emptyKey))
-//   RadixSortPairs  stable LSD sort (primitives.cuh)
-//   KReorder*       gather the SoA fields through the permutation, sorted cell IDs
-//   cell table      run starts of the sorted cell IDs (device scan), count stays on device
-//   KGridScatter    dense frame grid: linear cell coordinate -> compact cell index
+//   KKeys           clamped Morton key per particle (min(cellId, emptyKey)) + the digit
+//                   histograms of every sort pass
+//   KOnesweepPass   stable LSD sort, one kernel per 8-bit digit (primitives.cuh); the last
+//                   pass writes the permutation and the sorted cell IDs
+//   KReorder*       gather the SoA fields through the permutation
+//   KCellTableGrid  run starts of the sorted cell IDs (single-pass scan), each writing the
+//                   compact cell table and the dense frame grid entry; count stays on device
 //   KQueryFluid*    one warp per SELL32 chunk (32 consecutive sorted fluid particles):
 //                   each lane walks only its own strict stencil, whose non-empty cell
 //                   ranges are looked up once per distinct cell of the chunk and ranked by
 //                   first index (= Morton order), so rows arrive in ascending index order.
 //                   The count pass keeps each row in a [slot][lane] scratch; the fill pass
-//                   encodes the scratch into the SELL32 slices (same layout, coalesced)
+//                   encodes the scratch into the SELL32 slices (same layout, coalesced). A
+//                   variant of the count pass first copies the block's neighboring cell
+//                   blocks into shared memory (TMA bulk copies) and walks them there
 //   KQueryRigid     one thread per rigid particle, CSR rows (RF, RB, RR)
 #include "kernels.h"
 #include "primitives.cuh"
@@ -698,31 +702,19 @@ __device__ __forceinline__ void HomeStatsFromScratch(const uint32_t* scr, LaneRe
     }
 }
 
-// count pass: neighbor counts, chunk compression meta, rows into the per-chunk scratch.
-// Instantiated per minimum resident blocks per SM (QUERY_COUNT_CANDIDATES), chosen by the
-// autotuner; an earlier hand sweep on the 1M dam (ms per count pass): 1 block (78 registers)
-// 0.393, none given (64 registers) 0.350, 9 (56) 0.332, 10 (48) 0.348, 12 (40, spills) 0.338
-#define QUERY_COUNT_CANDIDATES(X) X(6) X(8) X(9) X(10) X(12)
-#define QUERY_FILL_CANDIDATES(X) X(8) X(10) X(12) X(16)
-template <int MB>
-__global__ void __launch_bounds__(QUERY_THREADS, MB) KQueryFluidCount(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
-    extern __shared__ uint2 qsm[];
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t chunk = blockIdx.x * (QUERY_THREADS / 32) + warp;
-    const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
-    if (chunk >= nChunks) return;  // uniform per warp
-    const QueryScene sc = ResolveScene(a, chunk);
-    const QueryWarp w = QueryWarpSmem(qsm, warp, a.fr.reach);
-    const QueryLaneInfo q = QuerySetup(a, chunk, lane, w);
+// rest of the count pass after the FF walk (shared by both variants): FB and FR walks, the FF
+// home-window statistics where needed, counts, neighbor totals and the chunk meta
+__device__ __forceinline__ void QueryCountRest(const QueryArgs& a, const QueryScene& sc, const QueryWarp& w,
+                                               const QueryLaneInfo& q, uint32_t chunk, uint32_t lane, LaneRefs& rFF,
+                                               const uint32_t* sF, const SellMeta& mFF, const SellMeta& mFB,
+                                               const SellMeta& mFR) {
     uint32_t homeLo, homeHi;
     HomeWindow(chunk, homeLo, homeHi);
-    LaneRefs rFF, rFB, rFR;
-    rFF.init(); rFB.init(); rFR.init();
+    LaneRefs rFB, rFR;
+    rFB.init(); rFR.init();
     LaneWriter none;
-    uint32_t* sF = a.scrF + (uint64_t)chunk * a.ksF * SELL_W + lane;
     uint32_t* sB = a.scrB + (uint64_t)chunk * a.ksB * SELL_W + lane;
     uint32_t* sR = a.scrR + (uint64_t)chunk * a.ksR * SELL_W + lane;
-    QuerySpecies<0, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFF, sF, a.ksF, none, mFF);
     QuerySpecies<1, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFB, sB, a.ksB, none, mFB);
     QuerySpecies<2, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFR, sR, a.ksR, none, mFR);
     // F and B rows are ascending: the minimum is the first stored entry
@@ -773,6 +765,298 @@ __global__ void __launch_bounds__(QUERY_THREADS, MB) KQueryFluidCount(QueryArgs 
     CommitChunkMeta(chunk, owner, rFF, true, mFF);
     CommitChunkMeta(chunk, owner, rFB, false, mFB);
     CommitChunkMeta(chunk, owner, rFR, false, mFR);
+}
+
+// count pass: neighbor counts, chunk compression meta, rows into the per-chunk scratch.
+// Instantiated per minimum resident blocks per SM (QUERY_COUNT_CANDIDATES: X plain, XS with the
+// neighboring cell blocks staged in shared memory, below), chosen by the autotuner; an earlier
+// hand sweep on the 1M dam (ms per count pass): 1 block (78 registers) 0.393, none given (64
+// registers) 0.350, 9 (56) 0.332, 10 (48) 0.348, 12 (40, spills) 0.338
+#define QUERY_COUNT_CANDIDATES(X, XS) X(6) X(8) X(9) X(10) X(12) XS(4) XS(5)
+#define QUERY_FILL_CANDIDATES(X) X(8) X(10) X(12) X(16)
+template <int MB>
+__global__ void __launch_bounds__(QUERY_THREADS, MB) KQueryFluidCount(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
+    extern __shared__ uint2 qsm[];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t chunk = blockIdx.x * (QUERY_THREADS / 32) + warp;
+    const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
+    if (chunk >= nChunks) return;  // uniform per warp
+    const QueryScene sc = ResolveScene(a, chunk);
+    const QueryWarp w = QueryWarpSmem(qsm, warp, a.fr.reach);
+    const QueryLaneInfo q = QuerySetup(a, chunk, lane, w);
+    uint32_t homeLo, homeHi;
+    HomeWindow(chunk, homeLo, homeHi);
+    LaneRefs rFF;
+    rFF.init();
+    LaneWriter none;
+    uint32_t* sF = a.scrF + (uint64_t)chunk * a.ksF * SELL_W + lane;
+    QuerySpecies<0, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFF, sF, a.ksF, none, mFF);
+    QueryCountRest(a, sc, w, q, chunk, lane, rFF, sF, mFF, mFB, mFR);
+}
+
+// ---- count pass with the neighboring cell blocks staged in shared memory
+//
+// A block's four chunks are 128 consecutive particles in Morton order, so their cells and the
+// strict stencils of those cells lie in a small box of the frame (at 8 particles per cell about
+// 6 x 4 x 4 cells). This variant looks up every cell of that box once (range from the dense grid
+// and the cell table), copies the particles of each non-empty cell into shared memory with one
+// TMA bulk copy per cell (cp.async.bulk global -> shared, completion counted in bytes on one
+// mbarrier, wait bounded), takes the FF stencil ranges from the box table and walks candidate
+// positions in shared memory instead of through L1. Same candidates in the same order, so the
+// same rows. A block whose box exceeds STAGE_BOX_CAP cells or STAGE_CAP particles, or whose
+// chunks belong to different scenes of a served batch, reads global memory like the plain
+// variant. FB and FR walks are unchanged (boundary cells are mostly empty inside the fluid).
+constexpr uint32_t STAGE_BOX_CAP = 256, STAGE_CAP = 1024;
+constexpr uint32_t STAGE_WAIT_LIMIT = 1u << 20;
+
+__device__ __forceinline__ uint32_t SmemAddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void MbarInit(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void MbarArriveExpectTx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(SmemAddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool MbarTryWait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(SmemAddr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+// bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global memory
+// into this CTA's shared memory, completion signalled on `bar`
+__device__ __forceinline__ void BulkCopyG2S(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     SmemAddr(dst)),
+                 "l"(src), "r"(bytes), "r"(SmemAddr(bar))
+                 : "memory");
+}
+
+__host__ __device__ __forceinline__ size_t StageOffBytes(uint32_t reach) {
+    return ((size_t)QueryRangeCap(reach) * 2u * sizeof(uint16_t) + 15u) & ~(size_t)15u;
+}
+__host__ __device__ __forceinline__ size_t QueryStagedSmemBytes(uint32_t reach) {
+    return (QueryWarpSmemBytes(reach) + StageOffBytes(reach)) * (QUERY_THREADS / 32) + (size_t)STAGE_CAP * sizeof(float4) +
+           (size_t)STAGE_BOX_CAP * 3u * sizeof(uint32_t);
+}
+
+struct StageBox {
+    const float4* stage;                      // staged particles, cell after cell in box order
+    const uint32_t *beg, *len, *off;          // per box cell: first particle, count, stage offset
+    int x0, y0, z0;
+    uint32_t bx, by, vol;
+    uint16_t *offU, *offS;                    // this warp's stage offsets of its stencil slots
+};
+
+// FF stencil ranges of groups [g0, g0 + nb) from the box table, ranked by first index, with the
+// stage offset of each ranked range (QueryRanges for staged particles)
+__device__ __forceinline__ void QueryRangesStaged(const QueryArgs& a, const QueryScene& sc, const QueryWarp& w,
+                                                  const StageBox& bx, uint32_t g0, uint32_t nb, uint32_t lane) {
+    const int r = (int)sc.fr.reach, D = 2 * r + 1;
+    const uint32_t sv = (uint32_t)(D * D * D), total = nb * sv;
+    if (lane < nb) w.nne[lane] = 0;
+    __syncwarp();
+    for (uint32_t t = lane; t < total; t += 32) {
+        const uint32_t gl = t / sv, s = t - gl * sv;
+        const int x = w.gc[g0 + gl] + (int)(s % D) - r;
+        const int y = w.gc[32 + g0 + gl] + (int)((s / D) % D) - r;
+        const int z = w.gc[64 + g0 + gl] + (int)(s / (D * D)) - r;
+        uint2 v = make_uint2(0u, 0u);
+        uint32_t o = 0u;
+        if (x >= 0 && x < (int)sc.fr.nx && y >= 0 && y < (int)sc.fr.ny && z >= 0 && z < (int)sc.fr.nz) {
+            // inside the box by construction (box = the groups' cells widened by the reach)
+            const uint32_t b = (uint32_t)(x - bx.x0) + bx.bx * ((uint32_t)(y - bx.y0) + bx.by * (uint32_t)(z - bx.z0));
+            if (b < bx.vol) {
+                v = make_uint2(bx.beg[b], bx.beg[b] + bx.len[b]);
+                o = bx.off[b];
+            } else {
+                atomicOr(a.err, ERR_QUERY_CAP);
+            }
+        }
+        w.rng[t] = v;
+        bx.offU[t] = (uint16_t)o;
+        if (v.x < v.y) atomicAdd(&w.nne[gl], 1u);
+    }
+    __syncwarp();
+    for (uint32_t t = lane; t < total; t += 32) {
+        const uint32_t gl = t / sv;
+        const uint2 v = w.rng[t];
+        if (v.x < v.y) {
+            uint32_t rank = 0;
+            const uint2* row = w.rng + gl * sv;
+            for (uint32_t u = 0; u < sv; u++) {
+                const uint2 o = row[u];
+                rank += (o.x < o.y && o.x < v.x) ? 1u : 0u;
+            }
+            w.srt[gl * sv + rank] = v;
+            bx.offS[gl * sv + rank] = bx.offU[t];
+        }
+    }
+    __syncwarp();
+}
+
+// QueryWalkCountU over staged FF candidates: the position of candidate j of a ranked range
+// (begin, end) with stage offset o is stage[o + (j - begin)]
+__device__ __forceinline__ void QueryWalkCountStaged(const QueryArgs& a, const QueryScene& sc, const QueryWarp& w,
+                                                     const StageBox& bx, const QueryLaneInfo& q, uint32_t g0,
+                                                     uint32_t nb, LaneRefs& ref, uint32_t* scr, uint32_t ks) {
+    constexpr uint32_t U = QUERY_WALK_U;
+    const uint32_t sv = StencilVolume(sc.fr.reach);
+    const bool mine = q.g != EMPTY_32 && q.g >= g0 && q.g < g0 + nb;
+    const uint32_t gl = mine ? q.g - g0 : 0u;
+    const uint32_t n = mine ? w.nne[gl] : 0u;
+    const uint2* rows = w.srt + gl * sv;
+    const uint16_t* offs = bx.offS + gl * sv;
+    const float xi = q.pi.x, yi = q.pi.y, zi = q.pi.z, r2 = a.r2;
+    uint32_t k = 0, j = 0, e = 0, so = 0;
+    if (n > 0) { const uint2 v = rows[0]; j = v.x; e = v.y; so = offs[0]; }
+    uint32_t cnt = ref.cnt, mx = ref.mx;
+    while (k < n) {
+        const uint32_t m = min(U, e - j);
+        const float4* pp = bx.stage + so;
+        float4 p[U];
+#pragma unroll
+        for (uint32_t u = 0; u < U; u++) p[u] = (u < m) ? pp[u] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (uint32_t u = 0; u < U; u++) {
+            const bool h = (u < m) && IsNeighbor(xi, yi, zi, p[u].x, p[u].y, p[u].z, r2);
+            if (h && cnt < ks) scr[(size_t)cnt * SELL_W] = j + u;
+            cnt += h ? 1u : 0u;
+            mx = h ? j + u : mx;
+        }
+        j += m;
+        so += m;
+        if (j == e) {
+            if (++k < n) { const uint2 v = rows[k]; j = v.x; e = v.y; so = offs[k]; }
+        }
+    }
+    ref.cnt = cnt;
+    ref.mx = mx;
+}
+
+template <int MB>
+__global__ void __launch_bounds__(QUERY_THREADS, MB)
+    KQueryFluidCountStaged(QueryArgs a, SellMeta mFF, SellMeta mFB, SellMeta mFR) {
+    extern __shared__ float4 qsmS[];
+    constexpr uint32_t W = QUERY_THREADS / 32;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t chunk0 = blockIdx.x * W, chunk = chunk0 + warp;
+    const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
+    const bool active = chunk < nChunks;  // chunk0 < nChunks for every launched block
+    const uint32_t reach = a.fr.reach;
+    char* base = reinterpret_cast<char*>(qsmS);
+    const size_t wsz = QueryWarpSmemBytes(reach), osz = StageOffBytes(reach);
+    const QueryWarp w = QueryWarpSmem(base, warp, reach);
+    float4* stage = reinterpret_cast<float4*>(base + W * (wsz + osz));
+    uint32_t* boxBeg = reinterpret_cast<uint32_t*>(stage + STAGE_CAP);
+    uint32_t* boxLen = boxBeg + STAGE_BOX_CAP;
+    uint32_t* boxOff = boxLen + STAGE_BOX_CAP;
+    __shared__ int sLo[3], sHi[3];
+    __shared__ uint32_t sScene[2], sWarpTot[W], sTot;
+    __shared__ __align__(8) uint64_t sBar;
+    if (tid < 3) { sLo[tid] = INT_MAX; sHi[tid] = INT_MIN; }
+    if (tid == 0) {
+        sScene[0] = 0xffffffffu; sScene[1] = 0u;
+        MbarInit(&sBar, 1u);
+    }
+    __syncthreads();
+    // the block's FF cell box: bounds of its chunks' cells (one entry per distinct cell)
+    QueryLaneInfo q{};
+    if (active) {
+        q = QuerySetup(a, chunk, lane, w);
+        if (lane < q.nGroups) {
+            atomicMin(&sLo[0], w.gc[lane]); atomicMax(&sHi[0], w.gc[lane]);
+            atomicMin(&sLo[1], w.gc[32 + lane]); atomicMax(&sHi[1], w.gc[32 + lane]);
+            atomicMin(&sLo[2], w.gc[64 + lane]); atomicMax(&sHi[2], w.gc[64 + lane]);
+        }
+        if (lane == 0 && a.scenes) {
+            atomicMin(&sScene[0], a.chunkScene[chunk]);
+            atomicMax(&sScene[1], a.chunkScene[chunk]);
+        }
+    }
+    __syncthreads();
+    const QueryScene s0 = ResolveScene(a, chunk0);
+    StageBox bx{};
+    bx.offU = reinterpret_cast<uint16_t*>(base + W * wsz + warp * osz);
+    bx.offS = bx.offU + QueryRangeCap(reach);
+    bool ok = s0.gridF != nullptr && sLo[0] <= sHi[0] && (a.scenes == nullptr || sScene[0] == sScene[1]);
+    if (ok) {
+        const int r = (int)s0.fr.reach;
+        bx.x0 = max(sLo[0] - r, 0); bx.y0 = max(sLo[1] - r, 0); bx.z0 = max(sLo[2] - r, 0);
+        const int x1 = min(sHi[0] + r, (int)s0.fr.nx - 1), y1 = min(sHi[1] + r, (int)s0.fr.ny - 1),
+                  z1 = min(sHi[2] + r, (int)s0.fr.nz - 1);
+        const uint64_t vol = (uint64_t)(x1 - bx.x0 + 1) * (uint64_t)(y1 - bx.y0 + 1) * (uint64_t)(z1 - bx.z0 + 1);
+        ok = x1 >= bx.x0 && y1 >= bx.y0 && z1 >= bx.z0 && vol <= STAGE_BOX_CAP;
+        bx.bx = (uint32_t)(x1 - bx.x0 + 1); bx.by = (uint32_t)(y1 - bx.y0 + 1); bx.vol = ok ? (uint32_t)vol : 0u;
+    }
+    // ok is the same in every thread of the block (computed from shared values)
+    if (ok) {
+        for (uint32_t b = tid; b < bx.vol; b += QUERY_THREADS) {
+            const uint32_t xx = b % bx.bx, yy = (b / bx.bx) % bx.by, zz = b / (bx.bx * bx.by);
+            const uint32_t c = s0.gridF[(uint64_t)(bx.x0 + (int)xx) +
+                                        (uint64_t)s0.fr.nx * ((uint64_t)(bx.y0 + (int)yy) +
+                                                              (uint64_t)s0.fr.ny * (uint64_t)(bx.z0 + (int)zz))];
+            uint32_t bg = 0u, ln = 0u;
+            if (c != EMPTY_32) { bg = a.startF[c]; ln = a.startF[c + 1] - bg; }
+            boxBeg[b] = bg;
+            boxLen[b] = ln;
+        }
+        __syncthreads();
+        // exclusive scan of the cell counts, two box cells per thread (STAGE_BOX_CAP = 2 x threads)
+        const uint32_t b0 = 2u * tid;
+        const uint32_t l0 = b0 < bx.vol ? boxLen[b0] : 0u, l1 = b0 + 1u < bx.vol ? boxLen[b0 + 1u] : 0u;
+        uint32_t incl = l0 + l1;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+            if ((int)lane >= d) incl += v;
+        }
+        if (lane == 31) sWarpTot[warp] = incl;
+        __syncthreads();
+        uint32_t pre = 0u;
+        for (uint32_t v = 0; v < warp; v++) pre += sWarpTot[v];
+        const uint32_t ex = pre + incl - (l0 + l1);
+        if (b0 < bx.vol) boxOff[b0] = ex;
+        if (b0 + 1u < bx.vol) boxOff[b0 + 1u] = ex + l0;
+        if (tid == QUERY_THREADS - 1u) sTot = pre + incl;
+    }
+    __syncthreads();
+    const uint32_t T = ok ? sTot : 0u;
+    bool staged = ok && T <= STAGE_CAP;
+    if (staged) {
+        if (tid == 0) MbarArriveExpectTx(&sBar, T * (uint32_t)sizeof(float4));
+        __syncthreads();  // the expected byte count is posted before any copy can complete
+        for (uint32_t b = tid; b < bx.vol; b += QUERY_THREADS)
+            if (boxLen[b]) BulkCopyG2S(stage + boxOff[b], a.posF + boxBeg[b], boxLen[b] * (uint32_t)sizeof(float4), &sBar);
+        bool done = false;
+        for (uint32_t spin = 0; spin < STAGE_WAIT_LIMIT && !done; spin++) done = MbarTryWait(&sBar, 0u);
+        if (!done) atomicOr(a.err, ERR_STAGE_WAIT);
+        staged = __syncthreads_and(done ? 1 : 0) != 0;
+    }
+    if (!active) return;  // no block-wide barrier below
+    bx.stage = stage; bx.beg = boxBeg; bx.len = boxLen; bx.off = boxOff;
+    const QueryScene sc = ResolveScene(a, chunk);
+    uint32_t homeLo, homeHi;
+    HomeWindow(chunk, homeLo, homeHi);
+    LaneRefs rFF;
+    rFF.init();
+    LaneWriter none;
+    uint32_t* sF = a.scrF + (uint64_t)chunk * a.ksF * SELL_W + lane;
+    if (staged) {
+        const uint32_t gb = QueryGroupsPerBatch(sc.fr.reach);
+        for (uint32_t g0 = 0; g0 < q.nGroups; g0 += gb) {
+            const uint32_t nb = min(gb, q.nGroups - g0);
+            QueryRangesStaged(a, sc, w, bx, g0, nb, lane);
+            QueryWalkCountStaged(a, sc, w, bx, q, g0, nb, rFF, sF, a.ksF);
+            __syncwarp();
+        }
+    } else {
+        QuerySpecies<0, WALK_COUNT>(a, sc, w, q, lane, homeLo, homeHi, rFF, sF, a.ksF, none, mFF);
+    }
+    QueryCountRest(a, sc, w, q, chunk, lane, rFF, sF, mFF, mFB, mFR);
 }
 
 // encode one species' scratch rows of a chunk into its SELL32 slice (coalesced: the scratch
@@ -828,16 +1112,21 @@ uint32_t QueryCap(uint32_t reach) { return QueryRangeCap(reach); }
 size_t QuerySmemBytes(uint32_t reach) { return QueryWarpSmemBytes(reach) * (QUERY_THREADS / 32); }
 size_t QueryScratchWords(uint32_t nChunks, uint32_t ks) { return (size_t)nChunks * ks * SELL_W; }
 
+// `slots` of a count-pass candidate: 1 = neighboring cell blocks staged in shared memory
 #define TSP_QC_ENTRY(mb) TuneCandidate{0, mb},
-static const TuneCandidate kCountCandidates[] = {QUERY_COUNT_CANDIDATES(TSP_QC_ENTRY)};
+#define TSP_QS_ENTRY(mb) TuneCandidate{1, mb},
+static const TuneCandidate kCountCandidates[] = {QUERY_COUNT_CANDIDATES(TSP_QC_ENTRY, TSP_QS_ENTRY)};
 static const TuneCandidate kFillCandidates[] = {QUERY_FILL_CANDIDATES(TSP_QC_ENTRY)};
 #undef TSP_QC_ENTRY
+#undef TSP_QS_ENTRY
 using QueryKernel = void (*)(QueryArgs, SellMeta, SellMeta, SellMeta);
 #define TSP_QC_FN(mb) &KQueryFluidCount<mb>,
+#define TSP_QS_FN(mb) &KQueryFluidCountStaged<mb>,
 #define TSP_QF_FN(mb) &KQueryFluidFill<mb>,
-static const QueryKernel kCountFns[] = {QUERY_COUNT_CANDIDATES(TSP_QC_FN)};
+static const QueryKernel kCountFns[] = {QUERY_COUNT_CANDIDATES(TSP_QC_FN, TSP_QS_FN)};
 static const QueryKernel kFillFns[] = {QUERY_FILL_CANDIDATES(TSP_QF_FN)};
 #undef TSP_QC_FN
+#undef TSP_QS_FN
 #undef TSP_QF_FN
 const TuneCandidate* QueryCandidates(bool fill, int* n) {
     *n = fill ? (int)(sizeof(kFillCandidates) / sizeof(kFillCandidates[0]))
@@ -850,16 +1139,21 @@ void LaunchQueryFluid(bool fill, const QueryArgs& a, const SellMeta& ff, const S
     const uint32_t nChunks = (a.nF + SELL_W - 1) / SELL_W;
     if (nChunks == 0) return;
     const uint32_t warps = QUERY_THREADS / 32;
-    const size_t smem = QueryWarpSmemBytes(a.fr.reach) * warps;
     const uint32_t blocks = (nChunks + warps - 1) / warps;
     int nc = 0;
-    QueryCandidates(fill, &nc);
+    const TuneCandidate* cand = QueryCandidates(fill, &nc);
     const TuneKernel k = fill ? TUNE_QUERY_FILL : TUNE_QUERY_COUNT;
     int v = variant;
     if (v < 0 || v >= nc) {
         v = TuneChoice(k, a.nF);
         if (v < 0) v = TuneDefault(k);
     }
+    bool staged = !fill && cand[v].slots == 1u;
+    if (staged && QueryStagedSmemBytes(a.fr.reach) > 227u * 1024u) {  // large reach: plain variant
+        v = TuneDefault(k);
+        staged = false;
+    }
+    const size_t smem = staged ? QueryStagedSmemBytes(a.fr.reach) : QueryWarpSmemBytes(a.fr.reach) * warps;
     const QueryKernel fn = fill ? kFillFns[v] : kCountFns[v];
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     fn<<<blocks, QUERY_THREADS, smem, s>>>(a, ff, fb, fr);
