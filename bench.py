@@ -9,8 +9,10 @@ relaxed-Jacobi loop to the density-error target, pressure acceleration, integrat
 working set (~0.3 GB) is larger than L2, so no flush is needed between steps.
 
 value: fluid particles x steps / device time (CUDA events on the backend stream, timed region
-bracketed by a barrier and device synchronisation, max over ranks). Multi-GPU: independent
-replicas (one scene per GPU, no inter-GPU traffic) -> weak scaling.
+bracketed by a barrier and device synchronisation, max over ranks). The K timed steps run as one
+tsp_b200_step(h, p, K) call (the interface's N_steps); p50/p99 come from the backend's per-step
+history (tsp_b200_get_step_history), the phase split from 20 further steps. Multi-GPU:
+independent replicas (one scene per GPU, no inter-GPU traffic) -> weak scaling.
 developed: the same run continued to step 1,000 (the collapse under way, more Jacobi sweeps per
 step), then 20 steps timed the same way.
 tuned: the autotuner's launch configurations (tune.cu), chosen during the first warm-up step.
@@ -178,6 +180,7 @@ def cpu_description():
 
 DEVELOPED_AT = 1000
 DEVELOPED_STEPS = 20
+PHASE_SAMPLE = 20  # steps after the timed region whose per-phase device times give phase_ms_p50
 
 
 def build_workload(rank=0):
@@ -225,7 +228,8 @@ def run_b200(args):
         be.step(p)  # the first step also runs the autotuner (tune.cu) for this size class
     tuned = abi.tuning(local)
     # ---- device-timed region (clock sampling already running when it starts)
-    step_ms, iters, phases = [], [], []
+    # K steps in one tsp_b200_step call (the interface's N_steps); each step's device time and
+    # iteration count come from the backend's step history after the region
     with ClockSampler(local) as clk:
         barrier(dist, dev)
         torch.cuda.synchronize(dev)
@@ -234,18 +238,21 @@ def run_b200(args):
         e1 = torch.cuda.Event(enable_timing=True)
         clk.mark_start()
         e0.record(stream)
-        for _ in range(args.steps):
-            be.step(p)
-            s = be.stats()
-            step_ms.append(s.lastStepMs)
-            iters.append(s.solverIters - 1)
-            phases.append(be.phase_times())
+        be.step(p, args.steps)
         e1.record(stream)
         torch.cuda.synchronize(dev)
         clk.mark_end()
     barrier(dist, dev)
     elapsed_ms = max_over_ranks(dist, e0.elapsed_time(e1), dev)
     launches = be.launch_count() - l0
+    hist = be.step_history(args.steps)
+    step_ms = [r["ms"] for r in hist]
+    iters = [r["solverIters"] - 1 for r in hist]
+    # phase split: PHASE_SAMPLE further steps, one call each, phase times read after each
+    phases = []
+    for _ in range(PHASE_SAMPLE):
+        be.step(p)
+        phases.append(be.phase_times())
     nF = st.N_F
     value = aggregate_rate(nF * args.steps, ws, elapsed_ms)
     sweeps = int(np.sum(iters))
@@ -272,23 +279,21 @@ def run_b200(args):
     # more Jacobi sweeps per step), then DEVELOPED_STEPS steps timed the same way
     developed = None
     if not args.no_developed:
-        done = args.warmup + args.steps
+        done = args.warmup + args.steps + PHASE_SAMPLE
         if DEVELOPED_AT > done:
             be.step(p, DEVELOPED_AT - done)
         barrier(dist, dev)
         torch.cuda.synchronize(dev)
-        d_ms, d_it = [], []
         e4 = torch.cuda.Event(enable_timing=True)
         e5 = torch.cuda.Event(enable_timing=True)
         e4.record(stream)
-        for _ in range(DEVELOPED_STEPS):
-            be.step(p)
-            sd = be.stats()
-            d_ms.append(sd.lastStepMs)
-            d_it.append(sd.solverIters - 1)
+        be.step(p, DEVELOPED_STEPS)
         e5.record(stream)
         torch.cuda.synchronize(dev)
         dev_ms = max_over_ranks(dist, e4.elapsed_time(e5), dev)
+        dh = be.step_history(DEVELOPED_STEPS)
+        d_ms = [r["ms"] for r in dh]
+        d_it = [r["solverIters"] - 1 for r in dh]
         dq = np.percentile(d_ms, [50, 99])
         developed = {"from_step": max(DEVELOPED_AT, done), "steps": DEVELOPED_STEPS, "unit": UNIT,
                      "value": round(aggregate_rate(nF * DEVELOPED_STEPS, ws, dev_ms), 1),
@@ -353,6 +358,7 @@ def run_b200(args):
         "jacobi_sweeps": sweeps, "jacobi_iters_per_s": round(sweeps * ws / (elapsed_ms / 1e3), 1),
         "neighbor_ms_last": round(s.lastNeighborMs, 4), "jacobi_ms_last": round(s.lastJacobiMs, 4),
         "phase_ms_p50": {k: round(v, 4) for k, v in phase_p50.items()},
+        "phase_sample": f"{PHASE_SAMPLE} steps after the timed region",
         "roofline": roof, "developed": developed, "tuned": tuned, "e2e": e2e, "cpu_baseline": cpu,
         "gpu_launches": int(launches), "clocks": clk.summary(), "other_configs": others, "served": served,
         "impl": "b200",
@@ -364,16 +370,12 @@ def _timed_steps(torch, dev, be, p, steps):
     stream = torch.cuda.ExternalStream(be.stream_handle(), device=dev)
     torch.cuda.synchronize(dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ms, sweeps = [], 0
     e0.record(stream)
-    for _ in range(steps):
-        be.step(p)
-        s = be.stats()
-        ms.append(s.lastStepMs)
-        sweeps += s.solverIters - 1
+    be.step(p, steps)
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    return e0.elapsed_time(e1), ms, sweeps
+    h = be.step_history(steps)
+    return e0.elapsed_time(e1), [r["ms"] for r in h], sum(r["solverIters"] - 1 for r in h)
 
 
 def other_configs_measure(torch, dev):

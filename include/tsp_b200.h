@@ -316,6 +316,17 @@ int tsp_b200_get_launch_count(const tsp_backend* h, uint64_t* count);
 /* device milliseconds of all steps this backend ran since creation (the sum of the per-step
  * times of tsp_step_stats.lastStepMs, GetBenchOps analogue, backend_sim.h:255) and their count */
 int tsp_b200_get_step_time_total(const tsp_backend* h, double* ms, uint64_t* steps);
+/* per-step record of the last 65,536 steps (GetBenchOps analogue, backend_sim.h:255): lets a
+ * caller run many steps in one tsp_b200_step call and still read each step's time */
+typedef struct tsp_step_record {
+    uint64_t step;              /* simulation step counter after the step */
+    float ms;                   /* device milliseconds of the step (as tsp_step_stats.lastStepMs) */
+    uint32_t solverIters;       /* relaxed-Jacobi iterations of the step */
+    double avgRelDensityErrPos; /* average positive density error at the end of its solve */
+} tsp_step_record;
+/* writes the records of the most recent min(cap, kept) steps, oldest first, and their number to
+ * *n; with out NULL (cap ignored) *n receives the number of records kept */
+int tsp_b200_get_step_history(const tsp_backend* h, tsp_step_record* out, uint32_t cap, uint32_t* n);
 
 /*
  * Host view of Sync::ExportSnapshot (source/simulation/sync/snapshots.h:37-66): the particles

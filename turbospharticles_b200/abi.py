@@ -92,6 +92,11 @@ class TspStateView(C.Structure):
 STATE_ARRAY_FIELDS = [name for name, _ in _STATE_FIELDS[6:]]
 
 
+class TspStepRecord(C.Structure):
+    _fields_ = [("step", C.c_uint64), ("ms", C.c_float), ("solverIters", C.c_uint32),
+                ("avgRelDensityErrPos", C.c_double)]
+
+
 class TspStepStats(C.Structure):
     _fields_ = [
         ("step", C.c_uint64), ("time", C.c_double), ("solverIters", _u32), ("reserved0", _u32),
@@ -165,6 +170,7 @@ EXPORTS = {
     "tsp_b200_time_stage": (C.c_int, [_VP, C.POINTER(TspParams), _u32, _u32, _pf]),
     "tsp_b200_get_launch_count": (C.c_int, [_VP, C.POINTER(C.c_uint64)]),
     "tsp_b200_get_step_time_total": (C.c_int, [_VP, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    "tsp_b200_get_step_history": (C.c_int, [_VP, C.POINTER(TspStepRecord), _u32, C.POINTER(_u32)]),
     "tsp_b200_get_stream": (C.c_int, [_VP, C.POINTER(_VP)]),
     "tsp_b200_fill_statistics": (C.c_int, [_VP, C.POINTER(TspParams), C.POINTER(C.c_double), C.c_uint32]),
     "tsp_b200_get_contact_report": (C.c_int, [_VP, C.POINTER(TspContactReport)]),

@@ -227,6 +227,17 @@ class SimBackendB200:
         self._chk(self.L.tsp_b200_get_step_time_total(self.h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
+    def step_history(self, last: int | None = None) -> list:
+        """Records of the most recent `last` steps (all kept ones if None), oldest first: dicts of
+        step, ms (device milliseconds), solverIters, avgRelDensityErrPos."""
+        n = C.c_uint32()
+        self._chk(self.L.tsp_b200_get_step_history(self.h, None, 0, C.byref(n)))
+        k = n.value if last is None else min(int(last), n.value)
+        buf = (abi.TspStepRecord * max(k, 1))()
+        self._chk(self.L.tsp_b200_get_step_history(self.h, buf, k, C.byref(n)))
+        return [{"step": r.step, "ms": r.ms, "solverIters": r.solverIters,
+                 "avgRelDensityErrPos": r.avgRelDensityErrPos} for r in buf[:n.value]]
+
     def stream_handle(self) -> int:
         s = C.c_void_p()
         self._chk(self.L.tsp_b200_get_stream(self.h, C.byref(s)))

@@ -291,6 +291,10 @@ public:
     float lastStepMs = 0.f, lastNbrMs = 0.f, lastJacMs = 0.f;
     double stepMsTotal = 0.0;   // device milliseconds of all steps since creation
     uint64_t stepsTimed = 0;
+    // records of the last HIST_CAP steps (a ring, allocated at the first step)
+    static constexpr uint32_t HIST_CAP = 1u << 16;
+    std::vector<tsp_step_record> hist;
+    uint64_t histCount = 0;
     std::string lastErr;
     uint64_t launches = 0;  // kernels launched by this backend (graph nodes included)
     // one-pass sort: the key kernel (with the histograms) and one kernel per 8-bit pass
@@ -1309,6 +1313,22 @@ public:
         if (nF && hm->st.iters > 0) launches += 2ull * (hm->st.iters - 1u);
     }
 
+    void RecordStep() {
+        if (hist.empty()) hist.resize(HIST_CAP);
+        tsp_step_record& r = hist[histCount % HIST_CAP];
+        r.step = stepCount;
+        r.ms = lastStepMs;
+        r.solverIters = hm->st.iters;
+        r.avgRelDensityErrPos = hm->st.avg[1];
+        histCount++;
+    }
+    uint32_t History(tsp_step_record* out, uint32_t cap) const {
+        const uint64_t kept = std::min<uint64_t>(histCount, HIST_CAP);
+        const uint64_t m = std::min<uint64_t>(kept, cap);
+        for (uint64_t k = 0; k < m; k++) out[k] = hist[(histCount - m + k) % HIST_CAP];
+        return (uint32_t)m;
+    }
+
     // device milliseconds between consecutive phase events of the last completed step
     uint32_t PhaseTimes(float* ms, uint32_t cap) {
         if (!phaseValid) return 0;
@@ -1715,9 +1735,11 @@ int tsp_b200_step(tsp_backend* h, const tsp_params* p, uint32_t n) {
     if (!p) return TSP_ERR_INVALID;
     TSP_GUARD(h, {
         for (uint32_t k = 0; k < n; k++) {
+            const uint64_t timed = h->b->stepsTimed;
             h->b->Step(*p);
             h->b->stepCount += 1;
             h->b->simTime += (double)p->timeStep;
+            if (h->b->stepsTimed != timed) h->b->RecordStep();
         }
     });
 }
@@ -1950,6 +1972,12 @@ int tsp_b200_get_step_time_total(const tsp_backend* h, double* ms, uint64_t* ste
     if (!ms || !steps) return TSP_ERR_INVALID;
     *ms = h->b->stepMsTotal;
     *steps = h->b->stepsTimed;
+    return TSP_OK;
+}
+int tsp_b200_get_step_history(const tsp_backend* h, tsp_step_record* out, uint32_t cap, uint32_t* n) {
+    TSP_NEED(h);
+    if (!n) return TSP_ERR_INVALID;
+    *n = out ? h->b->History(out, cap) : (uint32_t)std::min<uint64_t>(h->b->histCount, Backend::HIST_CAP);
     return TSP_OK;
 }
 
