@@ -73,10 +73,6 @@ __global__ void KBoundaryDiff(const float4* __restrict__ a, const float* __restr
                    ia[i] != ib[i];
     if (d) *diff = 1u;
 }
-__global__ void KIota(uint32_t* v, uint32_t n) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) v[i] = i;
-}
 void LaunchPack4(const float* a, const float* b, const float* c, const float* d, float dDefault, float4* out,
                  uint32_t n, cudaStream_t s) {
     if (n) KPack4<<<G(n), 256, 0, s>>>(a, b, c, d, dDefault, out, n);
@@ -201,6 +197,7 @@ public:
     DBuf<uint32_t> osAux;     // one-pass sort: histograms, tickets, look-back status
     DBuf<uint32_t> cellAux;   // single-pass cell table: ticket and look-back status
     DBuf<uint32_t> permF, permB, permR;
+    bool permBIdentity = false;  // the last build's boundary permutation is the identity (not written)
     DBuf<uint64_t> cidF, cidB, cidR, cidRs;
     DBuf<uint64_t> uniqF, uniqB, uniqR;
     DBuf<uint32_t> startF, startB, startR;
@@ -842,12 +839,11 @@ public:
         if (gridCells > gridB.cap) bSortedValid = false;
         gridF.ensure(gridCells); gridB.ensure(gridCells); gridR.ensure(gridCells);
         const int bs = EnsureBoundarySorted(sc);
-        if (nB && bs == B_KEPT_FROM_PULL) {
+        // an already sorted boundary's permutation is the identity: nothing reads it on the
+        // device, so it is only materialised when read (tsp_b200_read_permutation)
+        permBIdentity = nB && bs == B_ALREADY_SORTED;
+        if (nB && bs == B_KEPT_FROM_PULL)
             CK(cudaMemcpyAsync(permB.p, rawPermB.p, nB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-        } else if (nB && bs == B_ALREADY_SORTED) {
-            KIota<<<G(nB), 256, 0, s>>>(permB.p, nB);
-            launches += 1;
-        }
         // fluid: IDs, pos (+pressure), vel (+density) always; all fields for a standalone search
         if (nF) {
             SortByCell(posP.p, nF, fr, sc, permF.p, cidF.p, s);
@@ -1770,7 +1766,11 @@ int tsp_b200_read_permutation(const tsp_backend* h, uint32_t species, uint32_t* 
         const uint32_t cnt = species == 0 ? b.nF : species == 1 ? b.nB : b.nR;
         if (n != cnt || !out) throw Error(TSP_ERR_INVALID, "size mismatch");
         const uint32_t* src = species == 0 ? b.permF.p : species == 1 ? b.permB.p : b.permR.p;
-        if (cnt) CK(cudaMemcpy(out, src, cnt * 4ull, cudaMemcpyDeviceToHost));
+        if (species == 1 && b.permBIdentity) {
+            for (uint32_t i = 0; i < cnt; i++) out[i] = i;
+        } else if (cnt) {
+            CK(cudaMemcpy(out, src, cnt * 4ull, cudaMemcpyDeviceToHost));
+        }
     });
 }
 int tsp_b200_read_cell_table(const tsp_backend* h, uint32_t species, uint64_t* uniq, uint32_t* start, uint32_t cap,

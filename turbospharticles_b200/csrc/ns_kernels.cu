@@ -1059,19 +1059,60 @@ __global__ void __launch_bounds__(QUERY_THREADS, MB)
     QueryCountRest(a, sc, w, q, chunk, lane, rFF, sF, mFF, mFB, mFR);
 }
 
-// encode one species' scratch rows of a chunk into its SELL32 slice (coalesced: the scratch
-// and the slice share the [slot][lane] layout)
-__device__ __forceinline__ void EncodeFromScratch(const SellMeta& m, LaneWriter& wr, const uint32_t* scr, uint32_t cnt,
-                                                  uint32_t lane, uint32_t* err) {
-    constexpr uint32_t U = 8;  // loads of U slots in flight before their stores
-    for (uint32_t k0 = 0; k0 < wr.pitch; k0 += U) {
-        uint32_t v[U];
+// encode one species' scratch rows of a chunk into its SELL32 slice. The scratch and the slice
+// share the [slot][lane] layout, so each thread takes four adjacent lanes of one slot: one
+// 16-byte scratch load, four codes (StoreNeighbor_CompressedSell32,
+// neighbor_search_kernels.cu:193-247), one 8-byte (Delta16x2) or 16-byte (Abs32) store; the
+// warp's eight quarter-rows cover four slots per round. Slots past a lane's count (padding up
+// to the chunk's pitch, never read by the sweeps) are written as zero. Every slot of the slice
+// lies inside the scratch (pitch <= slots per lane when the chunk did not overflow), and the
+// offsets of chunks are multiples of 32 entries, so the vector accesses are aligned.
+__device__ __forceinline__ void EncodeFromScratch(const SellMeta& m, LaneWriter& wr, const uint32_t* scrChunk,
+                                                  uint32_t cnt, uint32_t lane, uint32_t* err) {
+    const uint32_t sub = lane & 7u, kFirst = lane >> 3;
+    uint32_t c[4];
 #pragma unroll
-        for (uint32_t u = 0; u < U; u++) v[u] = (k0 + u < cnt) ? __ldcs(scr + (uint64_t)(k0 + u) * SELL_W) : 0u;
+    for (uint32_t q = 0; q < 4; q++) c[q] = __shfl_sync(0xffffffffu, cnt, 4u * sub + q);
+    const bool d16 = wr.fmt == FMT_DELTA16X2;
+    const uint64_t cap = d16 ? m.cap16 : m.cap32;
+    uint32_t errBits = 0u;
+    constexpr uint32_t B = 4;  // rounds whose loads are in flight together
+    for (uint32_t kb = kFirst; kb < wr.pitch; kb += 4u * B) {
+        uint4 v[B];
 #pragma unroll
-        for (uint32_t u = 0; u < U; u++)
-            if (k0 + u < cnt) wr.store(m, lane, v[u], err);
+        for (uint32_t b = 0; b < B; b++) {
+            const uint32_t k = kb + 4u * b;
+            v[b] = k < wr.pitch ? __ldcs(reinterpret_cast<const uint4*>(scrChunk + (size_t)k * SELL_W + 4u * sub))
+                                : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (uint32_t b = 0; b < B; b++) {
+            const uint32_t k = kb + 4u * b;
+            if (k >= wr.pitch) break;
+            const uint64_t lin = wr.off + (uint64_t)k * SELL_W + 4u * sub;
+            if (lin + 4u > cap) { errBits |= ERR_FILL_OVERFLOW; continue; }
+            const uint32_t j[4] = {v[b].x, v[b].y, v[b].z, v[b].w};
+            uint32_t code[4];
+#pragma unroll
+            for (uint32_t q = 0; q < 4; q++) {
+                const bool valid = k < c[q];
+                if (d16) {
+                    const bool first = j[q] >= wr.base && j[q] - wr.base <= 0x7fffu;
+                    const bool second = j[q] >= wr.base2 && j[q] - wr.base2 <= 0x7fffu;
+                    if (valid && !first && !second) errBits |= ERR_DELTA_RANGE;
+                    code[q] = !valid ? 0u : first ? j[q] - wr.base : (0x8000u | (j[q] - wr.base2));
+                } else {
+                    code[q] = valid ? j[q] : 0u;
+                }
+            }
+            if (d16)
+                *reinterpret_cast<uint2*>(m.list16 + lin) = make_uint2(code[0] | (code[1] << 16), code[2] | (code[3] << 16));
+            else
+                *reinterpret_cast<uint4*>(m.list32 + lin) = make_uint4(code[0], code[1], code[2], code[3]);
+        }
     }
+    if (errBits) atomicOr(err, errBits);
+    wr.wr = cnt;  // every slot below the lane's count is written
 }
 
 // fill pass: scratch rows -> SELL32 (a chunk whose scratch overflowed walks its stencil again);
@@ -1089,9 +1130,9 @@ __global__ void __launch_bounds__(QUERY_THREADS, MB) KQueryFluidFill(QueryArgs a
     const uint32_t over = a.scrOver[chunk];
     LaneWriter wFF, wFB, wFR;
     wFF.init(mFF, chunk); wFB.init(mFB, chunk); wFR.init(mFR, chunk);
-    const uint32_t* sF = a.scrF + (uint64_t)chunk * a.ksF * SELL_W + lane;
-    const uint32_t* sB = a.scrB + (uint64_t)chunk * a.ksB * SELL_W + lane;
-    const uint32_t* sR = a.scrR + (uint64_t)chunk * a.ksR * SELL_W + lane;
+    const uint32_t* sF = a.scrF + (uint64_t)chunk * a.ksF * SELL_W;
+    const uint32_t* sB = a.scrB + (uint64_t)chunk * a.ksB * SELL_W;
+    const uint32_t* sR = a.scrR + (uint64_t)chunk * a.ksR * SELL_W;
     if (!(over & 1u)) EncodeFromScratch(mFF, wFF, sF, inRange ? mFF.counts[i] : 0u, lane, a.err);
     if (!(over & 2u)) EncodeFromScratch(mFB, wFB, sB, inRange ? mFB.counts[i] : 0u, lane, a.err);
     if (!(over & 4u)) EncodeFromScratch(mFR, wFR, sR, inRange ? mFR.counts[i] : 0u, lane, a.err);
