@@ -961,10 +961,12 @@ public:
         if (p.maxSolverIters > MAX_JACOBI_SWEEPS || p.minSolverIters > MAX_JACOBI_SWEEPS)
             throw Error(TSP_ERR_UNSUPPORTED, "solver iteration bounds above 100000");
         prm = p;
+        // the substep's device time includes the relayout of admissions and retirements (chunk
+        // moves, uploads of admitted scenes), batching work the one-scene path does not have
+        CK(cudaEventRecord(ev0, s));
         if (layoutDirty) Relayout();
         const uint32_t S = (uint32_t)order.size();
         if (S == 0 || nFtot == 0) return;
-        CK(cudaEventRecord(ev0, s));
         // ---- probe + host frame rule per scene
         hSc.resize(S);
         hGeom.resize(S);
