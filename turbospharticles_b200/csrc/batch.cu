@@ -285,6 +285,12 @@ public:
     uint64_t cap = 0;
     std::map<uint64_t, uint64_t> freeList;  // start -> length
     void reset(uint64_t c) { cap = c; freeList.clear(); if (c) freeList[0] = c; }
+    void extend(uint64_t c) {  // [cap, c) becomes free (merged with a free tail)
+        if (c <= cap) return;
+        const uint64_t old = cap;
+        cap = c;
+        release(old, c - old);
+    }
     bool alloc(uint64_t n, uint64_t& at) {
         if (n == 0) { at = 0; return true; }
         for (auto it = freeList.begin(); it != freeList.end(); ++it)
@@ -377,7 +383,7 @@ public:
     DBuf<uint64_t> idB, idBtmp;
     DBuf<uint64_t> uniqB, cidBtmp;
     DBuf<uint32_t> startB, permBtmp;
-    DBuf<uint32_t> gridB;
+    VBuf<uint32_t> gridB;  // grows in place: scenes keep their grid ranges when it grows
     DBuf<uint64_t> nCellsB;  // per slot
     // per-scene tables (by rank)
     std::vector<BatchSceneDev> hSc;
@@ -392,7 +398,8 @@ public:
     size_t hCap = 0;
     // neighbor build
     DBuf<uint64_t> keysA, keysB, cidF, uniqF, nCellsDev;
-    DBuf<uint32_t> valsA, valsB, tileHist, digitTotals, startF, gridF, err;
+    DBuf<uint32_t> valsA, valsB, tileHist, digitTotals, startF, err;
+    VBuf<uint32_t> gridF;  // grows in place (no free / allocation in the middle of a stream)
     DBuf<uint32_t> osAux, cellAux;  // one-pass sort and single-pass cell table (look-back words)
     DBuf<uint64_t> scanScratch;
     DBuf<U64x2> scanScratch2, sellTot;
@@ -438,6 +445,11 @@ public:
         CK(cudaMemset(dNActive.p, 0, 4));
         dLiveN.ensure(1);
         CK(cudaMemset(dLiveN.p, 0, 4));
+        // address reserves of the dense grids: admission charges 8 bytes per frame cell, so the
+        // budget bounds their total; twice that leaves room for the boundary arena's fragmentation
+        const uint64_t gridCells = std::max<uint64_t>(budget / 8, uint64_t(1) << 20);
+        gridB.reserveAddress(2 * gridCells);
+        gridF.reserveAddress(2 * gridCells);
         SetCellSize();
     }
     ~Batch() {
@@ -626,10 +638,12 @@ public:
         if (tot > 0x7fffffe0ull) throw Error(TSP_ERR_OVERFLOW, "batch fluid arena exceeds 2^31 particles");
         const uint32_t nNew = (uint32_t)tot, chunksNew = nNew / SELL_W;
         if (chunksNew > chunkCap) {
-            // doubling, but not past the chunks the memory budget can hold (each growth
-            // reallocates the arena and the scratch and re-captures the loop graph)
+            // the chunks the memory budget can hold, reserved at the first admission: a growth
+            // frees and reallocates the arena and its multi-GB row scratch and re-captures the
+            // loop graph, which took up to 0.7 s in the middle of a stream; the loop kernels
+            // iterate over the live chunks only, so the reserve costs no launch time
             const uint64_t budgetChunks = budget / (BatchSceneBytes(SELL_W, 0, 0) * 1ull);
-            const uint64_t want = std::max<uint64_t>(std::min<uint64_t>(2ull * chunkCap, budgetChunks), chunksNew);
+            const uint64_t want = std::max<uint64_t>(budgetChunks, chunksNew);
             chunkCap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(want, 64ull), 0x7fffffe0ull / SELL_W);
         }
         if (newOrder.size() > sceneCap) sceneCap = std::max<uint32_t>((uint32_t)newOrder.size(), std::max(2u * sceneCap, 16u));
@@ -798,7 +812,15 @@ public:
             allocGridB.release(sc.gridOffB, sc.gridVolB);
             sc.gridVolB = 0;
             sc.gridOffB = 0;
-            if (!allocGridB.alloc(vol, sc.gridOffB)) { regrown = true; break; }
+            if (!allocGridB.alloc(vol, sc.gridOffB)) {
+                // grow the arena in place when its address reserve allows (other scenes keep
+                // their ranges and sorts), else rebuild it below
+                const uint64_t capNew = std::max<uint64_t>(allocGridB.cap * 2, allocGridB.cap + vol + 4096);
+                if (capNew * sizeof(uint32_t) > gridB.reservedBytes) { regrown = true; break; }
+                gridB.ensure(capNew);
+                allocGridB.extend(gridB.cap);
+                if (!allocGridB.alloc(vol, sc.gridOffB)) { regrown = true; break; }
+            }
             sc.gridVolB = vol;
         }
         if (regrown) {
@@ -1005,7 +1027,7 @@ public:
         BuildBoundaries();
         for (uint32_t r = 0; r < S; r++) hGeom[r].gridOffB = slots[order[r]].gridOffB;
         gridCellsF = gOff;
-        gridF.grow(gridCellsF, 1.25);
+        gridF.grow(gridCellsF, 2.0);
         uint32_t rankBits = 1;
         while ((1u << rankBits) < S) rankBits++;
         const uint32_t shift = keyBitsMax;

@@ -152,6 +152,20 @@ struct VBuf {
         if (n <= cap && p) return;
         ensure((size_t)((double)n * slack) + 16);
     }
+    // reserves the virtual range for up to `elems` elements before anything is mapped, so that
+    // growth up to that size maps in place (addresses and contents kept); no physical memory
+    void reserveAddress(size_t elems) {
+        if (p) return;
+        const VmmApi& api = VmmApi::Get();
+        const CUmemAllocationProp prop = Prop();
+        size_t gran = 0;
+        CKD(api.granularity(&gran, &prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED));
+        const size_t want = std::max<size_t>(elems * sizeof(T), size_t(64) << 20);
+        reservedBytes = (want + gran - 1) / gran * gran;
+        CUdeviceptr va = 0;
+        CKD(api.reserve(&va, reservedBytes, gran, 0, 0));
+        p = reinterpret_cast<T*>(va);
+    }
     void release() {
         if (!p) return;
         cudaDeviceSynchronize();  // no kernel may still use the range (destruction / re-reservation only)
