@@ -384,7 +384,7 @@ def other_configs_measure(torch, dev):
     the neighbor-search-only case (Morton keys, sort, reorder, cell tables, SELL32 count + fill)
     at 1,048,576 and 4,194,304 points, uniform and clustered, 5 builds each after one warm-up
     build; algorithmic bytes of a build per point: keys 24 + sort 24 x passes + reorder of every
-    field 68 + cell table 8 + count 18 + fill 12 + list bytes (SURVEY 8(d))."""
+    field 68 + cell table 8 + count 18 + fill 12 + list bytes."""
     from turbospharticles_b200 import abi, scene as S
     from turbospharticles_b200.backend import SimBackendB200
     out = {}

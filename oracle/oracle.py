@@ -1,7 +1,7 @@
 """ctypes wrapper of the CPU oracle (TEST INFRASTRUCTURE ONLY).
 
-Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module,
-and only as the checker. It exposes the same method names as the product backend
+Only tests/ and __graft_entry__.smoke() import this module, to check results, and bench.py's
+CPU-baseline leg, which times it beside the GPU. It exposes the same method names as the product backend
 (turbospharticles_b200.backend.SimBackendB200) so parity tests drive both identically.
 """
 from __future__ import annotations
@@ -75,7 +75,7 @@ def _p(a):
 
 
 def sample_surface(mesh, sp):
-    """Sequential CPU restatement of SurfaceSampler::Sample (surface_oracle.cpp): the checker of
+    """Sequential CPU restatement of SurfaceSampler::Sample (surface_oracle.cpp): the oracle of
     turbospharticles_b200.mesh.sample_surface."""
     from turbospharticles_b200.mesh import _sample_with
     L = lib()

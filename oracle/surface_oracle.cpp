@@ -1,6 +1,6 @@
 // surface_oracle.cpp -- TEST INFRASTRUCTURE ONLY: sequential CPU restatement of the reference's
 // mesh surface sampler (Scene::SurfaceSampler, source/simulation/scene/geometry/
-// surface_sampling.cpp), the checker of tsp_b200_sample_surface. Compiled with
+// surface_sampling.cpp), the oracle of tsp_b200_sample_surface. Compiled with
 // -ffp-contract=off: every product and sum is rounded as written.
 //
 // The reference tests one cell phase group of a candidate round in parallel against the sample

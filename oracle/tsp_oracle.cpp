@@ -1,8 +1,8 @@
 // tsp_oracle.cpp -- CPU restatement of the reference IISPH step (TEST INFRASTRUCTURE ONLY).
 //
 // This file is the parity oracle of the B200 backend. It is never linked into, loaded by or
-// called from the product library; only tests/, __graft_entry__.smoke() and bench.py's CPU
-// baseline leg use it, and only as the checker.
+// called from the product library; only tests/ and __graft_entry__.smoke() use it, to check
+// results, and bench.py's CPU-baseline leg, which times it beside the GPU.
 //
 // It restates, scalar per particle and templated on the real type (float = the reference's
 // FP32 arithmetic, double = the "FP64 run" the reference does not have), the CPU path of

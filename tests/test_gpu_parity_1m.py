@@ -8,7 +8,7 @@ from the FP32 oracle before the stage) and its output is compared element by ele
 - against the FP32 oracle within the bound stated per field below (the GPU forms distances with
   the hardware reciprocal square root and sums in the same order; the rest is FP32 rounding);
 - against the FP64 oracle run on the same FP32 inputs: the FP32 error of the stage, asserted
-  against the north-star 1e-4 relative with the field's stated absolute floor.
+  against the 1e-4 relative bound on per-step field error with the field's stated absolute floor.
 
 Floors (atol): density, source term 1e-3 kg/m^3 (1e-6 of the rest density); pressure 1e-2 Pa;
 predicted velocity 1e-5 g dt; the diagonal a_ii and the pressure acceleration, sums of
@@ -51,7 +51,7 @@ def floors(diag_scale, acc_scale):
 # element-wise relative bound against the FP32 oracle, per field (floors above)
 RTOL_FP32 = {abi.FIELD_DENSITY: 2e-6, abi.FIELD_VEL_PRED: 2e-6, abi.FIELD_SOURCE: 1e-4, abi.FIELD_DIAG: 2e-5,
              abi.FIELD_PRESSURE: 1e-4, abi.FIELD_ACC_PRESS: 1e-4}
-RTOL_FP64 = 1e-4  # north star: per-step field error against FP64 <= 1e-4 relative
+RTOL_FP64 = 1e-4  # per-step field error against FP64 <= 1e-4 relative
 JACOBI_SWEEPS = (1, 3, 10)
 
 
