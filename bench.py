@@ -144,17 +144,18 @@ def profiled_traffic():
     return None
 
 
-def profiled_issue():
-    """Issue and L1 figures of the KJacobi launch from its committed ncu summary (lines
-    `issue_active_pct = X`, `l1_wavefronts_pct_of_peak = Y`): what bounds the sweep besides HBM."""
-    p = os.path.join(ROOT, "profiles", "KJacobi_iisph_dam_1M.md")
+def profiled_issue(name="KJacobi_iisph_dam_1M.md",
+                   keys=("issue_active_pct", "l1_wavefronts_pct_of_peak", "warp_instructions_per_pair_slot")):
+    """Issue and L1 figures of a kernel from its committed ncu summary (lines `key = value`):
+    what bounds it besides HBM."""
+    p = os.path.join(ROOT, "profiles", name)
     out = {}
     try:
         with open(p) as f:
             for line in f:
                 t = line.strip()
-                for key in ("issue_active_pct", "l1_wavefronts_pct_of_peak", "warp_instructions_per_pair_slot"):
-                    if t.startswith(key):
+                for key in keys:
+                    if t.startswith(key + " "):
                         out[key] = float(t.split("=")[1].strip().split()[0])
     except (OSError, ValueError, IndexError):
         pass
@@ -275,6 +276,21 @@ def run_b200(args):
             "bytes_per_particle": round(bytes_per_particle, 2), "list_bytes_per_particle": round(L, 2),
             "issue": profiled_issue(),
             "largest_phase_of_window": {"phase": largest, "p50_ms": round(phase_p50.get(largest, 0.0), 4)}}
+    # the neighbor build of a step (keys, sort, reorder, cell tables, count, finalize, fill) against
+    # the same peak: algorithmic bytes per particle keys 24 + sort 24 x passes + reorder 68 + cell
+    # table 8 + count 18 + fill 12 + list bytes, time = the build phases' p50 of the phase sample
+    nb_phases = ("sort_reorder_tables", "query_count", "finalize_readback", "query_fill")
+    if all(k in phase_p50 for k in nb_phases):
+        passes = (int(s.keyBits) + 7) // 8
+        nb_bpp = 24.0 + 24.0 * passes + 68.0 + 8.0 + 18.0 + 12.0 + L
+        nb_ms = sum(phase_p50[k] for k in nb_phases)
+        nb_gbs = nb_bpp * nF / (nb_ms * 1e-3) / 1e9
+        roof["neighbor_build"] = {
+            "phases_ms": {k: round(phase_p50[k], 4) for k in nb_phases}, "ms_per_build": round(nb_ms, 4),
+            "bytes_per_particle": round(nb_bpp, 2), "sort_passes": passes, "achieved": round(nb_gbs, 1),
+            "frac": round(nb_gbs / peak, 4), "bound": "SM issue (count pass: ~216 candidate tests per particle)",
+            "count_pass": profiled_issue("KQueryFluid_iisph_dam_1M.md",
+                                         ("count_issue_active_pct", "count_warps_active_pct"))}
     # ---- developed flow: the same run continued to step DEVELOPED_AT (the collapse under way,
     # more Jacobi sweeps per step), then DEVELOPED_STEPS steps timed the same way
     developed = None
