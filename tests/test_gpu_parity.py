@@ -143,6 +143,46 @@ def test_gpu_neighbor_lists_grow_between_builds():
     assert_neighbor_structures_equal(g, o, st.N_F, 0, 0)
 
 
+def test_gpu_neighbor_search_particles_outside_the_frame():
+    """Points over [0, 2]^3 with the unit cube as simulation domain: the frame is the bounds
+    clamped to the domain and widened by reach + 8 cells (neighbor_search.cpp:1902-2005), so
+    about half the points lie beyond it. They get the empty cell ID, sort last (stable) and
+    have no rows; every structure bit-exact with the oracle."""
+    st, dmin, dmax, p = S.neighbor_search_scene(50_000, "uniform", seed=13)
+    for a in (st.xPosF, st.yPosF, st.zPosF):
+        a *= np.float32(2.0)
+    g, o = pair(p)
+    load((g, o), st, p, dmin, dmax)
+    g.neighbor_search(p)
+    o.neighbor_search(p)
+    cid = g.cell_ids(abi.SPECIES_F)
+    empty = cid == np.uint64(0xFFFFFFFFFFFFFFFF)
+    assert empty.any() and not empty.all()
+    assert not empty[:int(np.argmax(empty))].any() and empty[int(np.argmax(empty)):].all(), "empty IDs sort last"
+    assert_neighbor_structures_equal(g, o, st.N_F, 0, 0, what="outside the frame")
+    off, _ = g.rows(abi.LIST_FF)
+    assert np.all(np.diff(off.astype(np.int64))[empty] == 0)
+
+
+def test_gpu_steps_without_fluid():
+    """A boundary-only scene steps like the reference's empty serial simulation
+    (cpu_backend.cpp:2309-2315): counters advance, no solve, the boundary is unchanged."""
+    p = K.ns_params()
+    st = K.make_particles(**K.NS_SCENES["boundary_only"])
+    g, o = pair(p)
+    load((g, o), st, p)
+    for _ in range(3):
+        g.step(p)
+        o.step(p)
+    sg, so = g.stats(), o.stats()
+    assert (sg.step, sg.solverIters) == (so.step, so.solverIters) == (3, 0)
+    assert sg.time == pytest.approx(so.time)
+    gs, os_ = g.push(), o.push()
+    assert gs.N_F == 0 and gs.N_B == os_.N_B
+    order = np.argsort(gs.idB)
+    assert np.array_equal(gs.xPosB[order], st.xPosB[np.argsort(st.idB)])
+
+
 def test_gpu_neighbor_search_4m_properties():
     """4,194,304 uniform points, another seed than the bit-exact case: size-independent
     properties -- FF rows ascending, self included exactly for in-frame particles, the FF
