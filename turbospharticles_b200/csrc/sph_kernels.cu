@@ -199,7 +199,9 @@ __global__ void __launch_bounds__(SPH_THREADS, MB) KNonPressure(Consts c, FluidD
             const float kg = GradFactor(d2, c);
             const float dot = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
             const float rhoJ = fmaxf(vj.w, 1e-7f);
-            const float a = ok ? (c.massF * dot) / (rhoJ * (d2 + c.hEps)) * kg : 0.0f;
+            // the quotient is formed in every lane (its denominator is positive) and the sums take
+            // a select, so no branch around the division splits the warp at a lane's last slot
+            const float a = (c.massF * dot) / (rhoJ * (d2 + c.hEps)) * kg;
             const float tx = fmaf(a, dx, fx), ty = fmaf(a, dy, fy), tz = fmaf(a, dz, fz);
             fx = ok ? tx : fx; fy = ok ? ty : fy; fz = ok ? tz : fz;
         });
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(SPH_THREADS, MB) KNonPressure(Consts c, FluidD
             const float dvx = vi.x - 0.0f, dvy = vi.y - 0.0f, dvz = vi.z - 0.0f;
             const float dot = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float a = ok ? (b.vol[j] * dot) / (d2 + c.hEps) : 0.0f;
+            const float a = (b.vol[j] * dot) / (d2 + c.hEps);
             const float tx = fmaf(a, gx, bx), ty = fmaf(a, gy, by), tz = fmaf(a, gz, bz);
             bx = ok ? tx : bx; by = ok ? ty : by; bz = ok ? tz : bz;
         });
@@ -223,7 +225,7 @@ __global__ void __launch_bounds__(SPH_THREADS, MB) KNonPressure(Consts c, FluidD
             const float dvx = vi.x - vj.x, dvy = vi.y - vj.y, dvz = vi.z - vj.z;
             const float dot = fmaf(dvx, dx, fmaf(dvy, dy, dvz * dz));
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float a = ok ? (vj.w * dot) / (d2 + c.hEps) : 0.0f;
+            const float a = (vj.w * dot) / (d2 + c.hEps);
             const float tx = fmaf(a, gx, rx), ty = fmaf(a, gy, ry), tz = fmaf(a, gz, rz);
             rx = ok ? tx : rx; ry = ok ? ty : ry; rz = ok ? tz : rz;
         });
